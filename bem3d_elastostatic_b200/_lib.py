@@ -1,0 +1,145 @@
+"""ctypes binding of libbem3d_b200.so (the C ABI in include/bem3d_b200.h).
+
+The library is built in-tree by ``bem3d_elastostatic_b200.build``.  There is no CPU
+fallback: if the shared library is missing or cannot be loaded, every entry point
+raises ``LibraryNotAvailable``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from . import build as _build
+
+LIB_PATH = _build.LIB
+
+BEM_OK = 0
+BEM_ERR_ARG = -1
+BEM_ERR_CUDA = -2
+BEM_ERR_OOM = -3
+BEM_ERR_TIMEOUT = -4
+BEM_ERR_STATE = -5
+BEM_ERR_MESH = -6
+BEM_ERR_NOCONV = -7
+
+BEM_PREC_FP64 = 0
+BEM_PREC_FP32_IR = 1
+BEM_PREC_BF16_IR = 2
+BEM_ASM_FP64 = 0
+BEM_ASM_FP32_FAR = 1
+BEM_IP_KELVIN_CONSISTENT = 1
+
+# every symbol the header declares, for the export check
+EXPORTS = [
+    "bem_ctx_create", "bem_ctx_destroy", "bem_last_error", "bem_sync", "bem_set_mesh",
+    "bem_set_material", "bem_set_bc", "bem_set_pins", "bem_precompute_geometry",
+    "bem_get_geometry", "bem_ghmat8", "bem_get_hg", "bem_solve", "bem_dgesv",
+    "bem_reorganize", "bem_internal_points", "bem_device_state",
+    "bem_internal_points_device",
+]
+
+
+class LibraryNotAvailable(RuntimeError):
+    pass
+
+
+class BemError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+class SolveInfo(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("restarts", C.c_int), ("rel_residual", C.c_double),
+                ("factor_seconds", C.c_double), ("refine_seconds", C.c_double),
+                ("gflops", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_vp = C.c_void_p
+_lib = None
+
+
+def load(build_if_needed: bool = True):
+    """Load the CUDA library (building it first when the sources are newer)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if build_if_needed and _build.needs_build():
+        try:
+            _build.build()
+        except Exception as exc:  # no nvcc where the library must already exist
+            if not os.path.exists(LIB_PATH):
+                raise LibraryNotAvailable(f"cannot build {LIB_PATH}: {exc}") from exc
+    if not os.path.exists(LIB_PATH):
+        raise LibraryNotAvailable(f"{LIB_PATH} is missing; run python -m bem3d_elastostatic_b200.build")
+    try:
+        L = C.CDLL(LIB_PATH)
+    except OSError as exc:
+        raise LibraryNotAvailable(str(exc)) from exc
+    ctxp = C.POINTER(C.c_void_p)
+    L.bem_ctx_create.argtypes = [ctxp, C.c_int]
+    L.bem_ctx_destroy.argtypes = [_vp]
+    L.bem_last_error.argtypes = [_vp]
+    L.bem_last_error.restype = C.c_char_p
+    L.bem_sync.argtypes = [_vp]
+    L.bem_set_mesh.argtypes = [_vp, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp]
+    L.bem_set_material.argtypes = [_vp, C.c_double, C.c_double]
+    L.bem_set_bc.argtypes = [_vp, _vp, _vp]
+    L.bem_set_pins.argtypes = [_vp, C.c_int, _vp]
+    L.bem_precompute_geometry.argtypes = [_vp]
+    L.bem_get_geometry.argtypes = [_vp] + [_vp] * 8
+    L.bem_ghmat8.argtypes = [_vp, C.c_int, _vp, C.c_int64, _vp]
+    L.bem_get_hg.argtypes = [_vp, C.c_int, C.c_int, _vp, C.c_int64, _vp, C.c_int64]
+    L.bem_solve.argtypes = [_vp, C.c_int, C.c_double, C.c_int, _vp, _ip, C.POINTER(SolveInfo)]
+    L.bem_dgesv.argtypes = [_vp, C.c_int, C.c_int, _vp, C.c_int, _vp, _vp, C.c_int, _ip]
+    L.bem_reorganize.argtypes = [_vp, _vp, _vp]
+    L.bem_internal_points.argtypes = [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int]
+    L.bem_device_state.argtypes = [_vp, C.POINTER(C.c_void_p), C.POINTER(C.c_int64),
+                                   C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]
+    L.bem_internal_points_device.argtypes = [_vp, C.c_int] + [_vp] * 7 + [C.c_int]
+    _lib = L
+    return L
+
+
+def ptr(a) -> int:
+    """Address of a numpy array (host) or an int device address."""
+    if a is None:
+        return None
+    if isinstance(a, int):
+        return a
+    return a.ctypes.data
+
+
+class Context:
+    """Owns one bem_ctx (one CUDA stream on one device)."""
+
+    def __init__(self, device: int = 0):
+        self.L = load()
+        h = C.c_void_p()
+        rc = self.L.bem_ctx_create(C.byref(h), device)
+        if rc != 0:
+            raise BemError(rc, f"bem_ctx_create(device={device}) failed")
+        self.h = h
+        self.device = device
+
+    def check(self, rc: int, what: str) -> int:
+        if rc < 0:
+            msg = self.L.bem_last_error(self.h)
+            raise BemError(rc, f"{what}: {msg.decode() if msg else ''}")
+        return rc
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.bem_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,614 @@
+// ghmat8 on the GPU: collocation assembly of A x = FI (assembly_mod.f90:53-223),
+// and the separate H/G products used for entrywise parity.
+//
+// Work split
+//   * regular pairs (collocation node not on the element; extin8, :339-384):
+//     one CTA owns 32 consecutive collocation nodes (96 rows of A) and walks the
+//     whole element list.  Its 8 warps take the 8 elements of one "batch" at a
+//     time; the elements of a batch share no node, so the 8 warps write disjoint
+//     columns of A and need no atomics, and a __syncthreads between batches orders
+//     the read-modify-writes of columns that neighbouring batches share.  Lane L of
+//     every warp integrates node (32*blockIdx + L) against the warp's element, so the
+//     element's quadrature table is a warp-uniform broadcast and the 3 rows of each
+//     lane make every column update one contiguous 768-byte segment.  FI and the
+//     rigid-body sums d1 stay in registers and are reduced across warps in a fixed
+//     order at the end (deterministic).
+//   * singular pairs (node on the element; locin8/triloc8, :386-616): one warp per
+//     collocation node, its <= 8 elements in sequence; lane (k, s) integrates the
+//     3x3 blocks of element node k over every third point of the sub-triangles, the
+//     partial sums meet in shared memory, and d2 = -sum_{k != nodo} h_k is a warp
+//     reduction.  Launched after the regular kernel on the same stream.
+// The column swap (:125-218) uses a per-(node, component) lookup built on the host
+// from the same node->element adjacency the reference scans (uknown / vp).
+#include "common.cuh"
+#include "shape.cuh"
+
+namespace bem {
+
+enum { kModeA = 0, kModeHG = 1 };
+
+struct AsmArgs {
+  int n, ne, nbatches;
+  int in0, nrows_nodes;  // collocation nodes [in0, in0 + nrows_nodes)
+  const int* batches;
+  const int* nconec;
+  const int* kconec;
+  const int* kode;
+  const double* bc;
+  const int* uknown;
+  const double* vp;
+  const int* nesim;
+  const int* ke;
+  const double* x;
+  const double* y;
+  const double* z;
+  const double* tab;
+  Material mat;
+  double* A;  // mode A: (3n, 3n); mode HG: H
+  int64_t lda;
+  double* FI;  // mode A only
+  double* G;   // mode HG only
+  int64_t ldg;
+};
+
+// symmetric 3x3 index (jj, ii) -> 0..5 : xx yy zz xy yz zx
+__device__ __forceinline__ int sym_idx(int a, int b) {
+  if (a == b) return a;
+  const int s = a + b;  // 1: xy, 3: yz, 2: zx
+  return s == 1 ? 3 : (s == 3 ? 4 : 5);
+}
+
+template <int NC, int MODE>
+__device__ __forceinline__ void regular_pair(const AsmArgs& P, int e, const int* kc, double xi0,
+                                             double xi1, double xi2, int64_t row,
+                                             double* fi, double* d1) {
+  constexpr int NG = (NC == 9) ? 36 : 16;
+  const double* T = P.tab + (int64_t)e * kTabStride;
+  const double c3 = P.mat.c3, c4 = P.mat.c4, c5 = P.mat.c5, c6 = P.mat.c6;
+
+  // ---- G: U* (symmetric, 6 values) x p12 -------------------------------------------
+  {
+    double g[NC][6];
+#pragma unroll
+    for (int k = 0; k < NC; ++k)
+#pragma unroll
+      for (int p = 0; p < 6; ++p) g[k][p] = 0.0;
+#pragma unroll 2
+    for (int q = 0; q < NG; ++q) {
+      const double r0 = __ldg(T + 6 * q + 0) - xi0;
+      const double r1 = __ldg(T + 6 * q + 1) - xi1;
+      const double r2 = __ldg(T + 6 * q + 2) - xi2;
+      const double ri = rsqrt(r0 * r0 + r1 * r1 + r2 * r2);
+      const double a0 = r0 * ri, a1 = r1 * ri, a2 = r2 * ri;
+      const double c3r = c3 * ri;
+      double u[6];
+      u[0] = (c4 + a0 * a0) * c3r;
+      u[1] = (c4 + a1 * a1) * c3r;
+      u[2] = (c4 + a2 * a2) * c3r;
+      u[3] = a0 * a1 * c3r;
+      u[4] = a1 * a2 * c3r;
+      u[5] = a2 * a0 * c3r;
+      const double* W = T + kTabGeo + 9 * q;
+#pragma unroll
+      for (int k = 0; k < NC; ++k) {
+        const double w = __ldg(W + k);
+#pragma unroll
+        for (int p = 0; p < 6; ++p) g[k][p] = fma(u[p], w, g[k][p]);
+      }
+    }
+    if (MODE == kModeA) {
+#pragma unroll
+      for (int ld = 0; ld < 3; ++ld) {
+        if (__ldg(P.kode + 3 * e + ld) == 0) {
+          const double mu = P.mat.mu;
+#pragma unroll
+          for (int k = 0; k < NC; ++k) {
+            double* col = P.A + (3 * (int64_t)kc[k] + ld) * P.lda + row;
+#pragma unroll
+            for (int jj = 0; jj < 3; ++jj) col[jj] = col[jj] - g[k][sym_idx(jj, ld)] * mu;
+          }
+        } else {
+#pragma unroll
+          for (int k = 0; k < NC; ++k) {
+            const double b = __ldg(P.bc + 3 * k + ld + 27 * e);
+#pragma unroll
+            for (int jj = 0; jj < 3; ++jj) fi[jj] = fma(g[k][sym_idx(jj, ld)], b, fi[jj]);
+          }
+        }
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < NC; ++k)
+#pragma unroll
+        for (int ii = 0; ii < 3; ++ii) {
+          double* col = P.G + (27 * (int64_t)e + 3 * k + ii) * P.ldg + row;
+#pragma unroll
+          for (int jj = 0; jj < 3; ++jj) col[jj] = g[k][sym_idx(jj, ii)];
+        }
+    }
+  }
+
+  // ---- H: T* (9 values) x p12 ------------------------------------------------------
+  {
+    double h[NC][9];  // h[k][jj + 3*ii]
+#pragma unroll
+    for (int k = 0; k < NC; ++k)
+#pragma unroll
+      for (int p = 0; p < 9; ++p) h[k][p] = 0.0;
+#pragma unroll 1
+    for (int q = 0; q < NG; ++q) {
+      const double r0 = __ldg(T + 6 * q + 0) - xi0;
+      const double r1 = __ldg(T + 6 * q + 1) - xi1;
+      const double r2 = __ldg(T + 6 * q + 2) - xi2;
+      const double n[3] = {__ldg(T + 6 * q + 3), __ldg(T + 6 * q + 4), __ldg(T + 6 * q + 5)};
+      const double ri = rsqrt(r0 * r0 + r1 * r1 + r2 * r2);
+      const double a[3] = {r0 * ri, r1 * ri, r2 * ri};
+      const double rdn = a[0] * n[0] + a[1] * n[1] + a[2] * n[2];
+      const double c5r2 = c5 * ri * ri;
+      double t[9];
+#pragma unroll
+      for (int ii = 0; ii < 3; ++ii)
+#pragma unroll
+        for (int jj = 0; jj < 3; ++jj) {
+          const double d = (ii == jj) ? c6 : 0.0;
+          t[jj + 3 * ii] =
+              c5r2 * (rdn * (d + 3.0 * a[ii] * a[jj]) + c6 * (n[jj] * a[ii] - n[ii] * a[jj]));
+        }
+      const double* W = T + kTabGeo + 9 * q;
+#pragma unroll
+      for (int k = 0; k < NC; ++k) {
+        const double w = __ldg(W + k);
+#pragma unroll
+        for (int p = 0; p < 9; ++p) h[k][p] = fma(t[p], w, h[k][p]);
+      }
+    }
+    // rigid-body partial sums d1(i, j) = -sum_k h(i, 3k + j) (assembly_mod.f90:103-111)
+#pragma unroll
+    for (int p = 0; p < 9; ++p) {
+      double s = 0.0;
+#pragma unroll
+      for (int k = 0; k < NC; ++k) s += h[k][p];
+      d1[p] -= s;
+    }
+    if (MODE == kModeA) {
+#pragma unroll
+      for (int ld = 0; ld < 3; ++ld) {
+        if (__ldg(P.kode + 3 * e + ld) == 0) {
+#pragma unroll
+          for (int k = 0; k < NC; ++k) {
+            const double b = __ldg(P.bc + 3 * k + ld + 27 * e);
+#pragma unroll
+            for (int jj = 0; jj < 3; ++jj) fi[jj] = fma(-h[k][jj + 3 * ld], b, fi[jj]);
+          }
+        } else {
+#pragma unroll
+          for (int k = 0; k < NC; ++k) {
+            const int64_t dof = 3 * (int64_t)kc[k] + ld;
+            if (__ldg(P.uknown + dof) == 0) {
+              double* col = P.A + dof * P.lda + row;
+#pragma unroll
+              for (int jj = 0; jj < 3; ++jj) col[jj] = col[jj] + h[k][jj + 3 * ld];
+            } else {
+              const double v = __ldg(P.vp + dof);
+#pragma unroll
+              for (int jj = 0; jj < 3; ++jj) fi[jj] = fma(-h[k][jj + 3 * ld], v, fi[jj]);
+            }
+          }
+        }
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < NC; ++k)
+#pragma unroll
+        for (int ii = 0; ii < 3; ++ii) {
+          double* col = P.A + (3 * (int64_t)kc[k] + ii) * P.lda + row;
+#pragma unroll
+          for (int jj = 0; jj < 3; ++jj) col[jj] = col[jj] + h[k][jj + 3 * ii];
+        }
+    }
+  }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(256, 1) ghmat_regular_kernel(AsmArgs P) {
+  __shared__ double s_red[kBatch][32][12];
+  const int w = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const int local = blockIdx.x * 32 + lane;  // node offset inside the row range
+  const bool active = local < P.nrows_nodes;
+  const int in = P.in0 + (active ? local : 0);
+  const double xi0 = P.x[in], xi1 = P.y[in], xi2 = P.z[in];
+  const int64_t row = 3 * (int64_t)local;
+  double fi[3] = {0.0, 0.0, 0.0};
+  double d1[9];
+#pragma unroll
+  for (int p = 0; p < 9; ++p) d1[p] = 0.0;
+
+  for (int b = 0; b < P.nbatches; ++b) {
+    const int e = __ldg(P.batches + kBatch * b + w);
+    if (e >= 0) {
+      const int ncone = __ldg(P.nconec + e);
+      int kc[9];
+      bool sing = false;
+#pragma unroll
+      for (int m = 0; m < 9; ++m) {
+        kc[m] = (m < ncone) ? __ldg(P.kconec + m + 9 * e) - 1 : 0;
+        sing |= (m < ncone) && (kc[m] == in);
+      }
+      if (active && !sing) {
+        if (ncone == 9)
+          regular_pair<9, MODE>(P, e, kc, xi0, xi1, xi2, row, fi, d1);
+        else
+          regular_pair<6, MODE>(P, e, kc, xi0, xi1, xi2, row, fi, d1);
+      }
+    }
+    __syncthreads();
+  }
+
+  for (int p = 0; p < 3; ++p) s_red[w][lane][p] = fi[p];
+  for (int p = 0; p < 9; ++p) s_red[w][lane][3 + p] = d1[p];
+  __syncthreads();
+  if (w == 0 && active) {
+    double F[3] = {0.0, 0.0, 0.0}, D[9];
+    for (int p = 0; p < 9; ++p) D[p] = 0.0;
+    for (int ww = 0; ww < kBatch; ++ww) {
+      for (int p = 0; p < 3; ++p) F[p] += s_red[ww][lane][p];
+      for (int p = 0; p < 9; ++p) D[p] += s_red[ww][lane][3 + p];
+    }
+    if (MODE == kModeA) {
+      // diagonal block from the non-singular elements (assembly_mod.f90:192-218)
+      for (int ld = 0; ld < 3; ++ld) {
+        const int64_t dof = 3 * (int64_t)in + ld;
+        if (P.uknown[dof] == 0) {
+          double* col = P.A + dof * P.lda + row;
+          for (int r = 0; r < 3; ++r) col[r] += D[r + 3 * ld];
+        } else {
+          const double v = P.vp[dof];
+          for (int r = 0; r < 3; ++r) F[r] -= D[r + 3 * ld] * v;
+        }
+      }
+      for (int r = 0; r < 3; ++r) P.FI[row + r] = F[r];
+    } else {
+      for (int ld = 0; ld < 3; ++ld) {
+        double* col = P.A + (3 * (int64_t)in + ld) * P.lda + row;
+        for (int r = 0; r < 3; ++r) col[r] += D[r + 3 * ld];
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------
+// singular elements
+// ---------------------------------------------------------------------------------
+
+__constant__ double s_gi[6];
+__constant__ double s_ome[6];
+
+// Sub-triangles of locin8 (assembly_mod.f90:399-489) for local node nodo (1-based):
+// returns the count and fills vertex parent coordinates (vertex 0 = the node).
+__device__ int sub_triangles(int ncone, int nodo, double v1[4][3], double v2[4][3],
+                             double area[4]) {
+  if (ncone == 9) {
+    const double gi1[9] = {-1.0, 0.0, 1.0, 1.0, 1.0, 0.0, -1.0, -1.0, 0.0};
+    const double gi2[9] = {-1.0, -1.0, -1.0, 0.0, 1.0, 1.0, 1.0, 0.0, 0.0};
+    // gii(p) = gi((p-1) mod 8 + 1) for p = 1..15
+    auto G1 = [&](int p) { return gi1[(p - 1) % 8]; };
+    auto G2 = [&](int p) { return gi2[(p - 1) % 8]; };
+    int cnt = 0;
+    if (nodo == 9) {
+      for (int k = 1; k <= 4; ++k) {
+        const int m = 2 * k - 1;
+        v1[cnt][0] = gi1[8];
+        v2[cnt][0] = gi2[8];
+        v1[cnt][1] = G1(m);
+        v2[cnt][1] = G2(m);
+        v1[cnt][2] = G1(m + 2);
+        v2[cnt][2] = G2(m + 2);
+        area[cnt] = 1.0;
+        ++cnt;
+      }
+    } else if (nodo & 1) {
+      for (int k = 1; k <= 2; ++k) {
+        const int m = 2 * k;
+        v1[cnt][0] = gi1[nodo - 1];
+        v2[cnt][0] = gi2[nodo - 1];
+        v1[cnt][1] = G1(nodo + m);
+        v2[cnt][1] = G2(nodo + m);
+        v1[cnt][2] = G1(nodo + m + 2);
+        v2[cnt][2] = G2(nodo + m + 2);
+        area[cnt] = 2.0;
+        ++cnt;
+      }
+    } else {
+      for (int k = 1; k <= 3; ++k) {
+        const int m = 2 * k - 1;
+        double a1[3] = {gi1[nodo - 1], G1(nodo + m), G1(nodo + m + 2)};
+        double a2[3] = {gi2[nodo - 1], G2(nodo + m), G2(nodo + m + 2)};
+        for (int t = 0; t < 3; ++t) {
+          v1[cnt][t] = a1[t];
+          v2[cnt][t] = a2[t];
+        }
+        area[cnt] = 0.5 * (a1[1] * a2[2] + a1[0] * a2[1] + a1[2] * a2[0] - a1[1] * a2[0] -
+                           a1[2] * a2[1] - a1[0] * a2[2]);
+        ++cnt;
+      }
+    }
+    return cnt;
+  }
+  const double gi1[6] = {1.0, 0.0, 0.0, 0.5, 0.0, 0.5};
+  const double gi2[6] = {0.0, 1.0, 0.0, 0.5, 0.5, 0.0};
+  int ta[2], tb[2], cnt;
+  double ar;
+  switch (nodo) {
+    case 1: cnt = 1; ta[0] = 2; tb[0] = 3; ar = 0.5; break;
+    case 2: cnt = 1; ta[0] = 3; tb[0] = 1; ar = 0.5; break;
+    case 3: cnt = 1; ta[0] = 1; tb[0] = 2; ar = 0.5; break;
+    case 4: cnt = 2; ta[0] = 2; tb[0] = 3; ta[1] = 3; tb[1] = 1; ar = 0.25; break;
+    case 5: cnt = 2; ta[0] = 3; tb[0] = 1; ta[1] = 1; tb[1] = 2; ar = 0.25; break;
+    default: cnt = 2; ta[0] = 1; tb[0] = 2; ta[1] = 2; tb[1] = 3; ar = 0.25; break;
+  }
+  for (int t = 0; t < cnt; ++t) {
+    v1[t][0] = gi1[nodo - 1];
+    v2[t][0] = gi2[nodo - 1];
+    v1[t][1] = gi1[ta[t] - 1];
+    v2[t][1] = gi2[ta[t] - 1];
+    v1[t][2] = gi1[tb[t] - 1];
+    v2[t][2] = gi2[tb[t] - 1];
+    area[t] = ar;
+  }
+  return cnt;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(128) ghmat_singular_kernel(AsmArgs P) {
+  __shared__ double s_part[4][27][18];
+  const int wib = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const int local = blockIdx.x * 4 + wib;
+  if (local >= P.nrows_nodes) return;  // warp-uniform
+  const int in = P.in0 + local;
+  const int64_t row = 3 * (int64_t)local;
+  const int k = lane % 9;
+  const int s = lane / 9;  // 0..2 active, 3 idle (lanes 27..31)
+  const double c3 = P.mat.c3, c4 = P.mat.c4, c5 = P.mat.c5, c6 = P.mat.c6;
+  const double xi[3] = {P.x[in], P.y[in], P.z[in]};
+  double fi[3] = {0.0, 0.0, 0.0};
+  double dsum[9];  // diagonal contributions for mode HG
+  for (int p = 0; p < 9; ++p) dsum[p] = 0.0;
+  const int cnt = min(P.nesim[in], 8);
+  for (int je = 0; je < cnt; ++je) {
+    const int e = P.ke[je + 8 * in] - 1;
+    const int ncone = P.nconec[e];
+    int kc[9];
+    int nodo = 0;
+    double xj1[9], xj2[9], xj3[9];
+    for (int m = 0; m < 9; ++m) {
+      kc[m] = (m < ncone) ? P.kconec[m + 9 * e] - 1 : 0;
+      xj1[m] = (m < ncone) ? P.x[kc[m]] : 0.0;
+      xj2[m] = (m < ncone) ? P.y[kc[m]] : 0.0;
+      xj3[m] = (m < ncone) ? P.z[kc[m]] : 0.0;
+      if (m < ncone && kc[m] == in && nodo == 0) nodo = m + 1;
+    }
+    double v1[4][3], v2[4][3], area[4];
+    const int ntri = sub_triangles(ncone, nodo, v1, v2, area);
+    double g[9], h[9];
+    for (int p = 0; p < 9; ++p) g[p] = h[p] = 0.0;
+    if (s < 3 && k < ncone) {
+      const int total = ntri * 36;
+      for (int t = s; t < total; t += 3) {
+        const int tri = t / 36, q = t % 36, i = q / 6, j = q % 6;
+        const double ss1 = 0.5 * (s_gi[i] + 1.0), ss2 = 0.5 * (s_gi[j] + 1.0);
+        const double g1 = (1.0 - ss1) * v1[tri][0] + ss1 * (1.0 - ss2) * v1[tri][1] +
+                          ss1 * ss2 * v1[tri][2];
+        const double g2 = (1.0 - ss1) * v2[tri][0] + ss1 * (1.0 - ss2) * v2[tri][1] +
+                          ss1 * ss2 * v2[tri][2];
+        double f[9], fd1[9], fd2[9];
+        shape_fn<double>(ncone, g1, g2, f, fd1, fd2);
+        double xp[3] = {0.0, 0.0, 0.0}, t1[3] = {0.0, 0.0, 0.0}, t2[3] = {0.0, 0.0, 0.0};
+        for (int m = 0; m < ncone; ++m) {
+          xp[0] += f[m] * xj1[m];
+          xp[1] += f[m] * xj2[m];
+          xp[2] += f[m] * xj3[m];
+          t1[0] += fd1[m] * xj1[m];
+          t1[1] += fd1[m] * xj2[m];
+          t1[2] += fd1[m] * xj3[m];
+          t2[0] += fd2[m] * xj1[m];
+          t2[1] += fd2[m] * xj2[m];
+          t2[2] += fd2[m] * xj3[m];
+        }
+        const double cr0 = t1[1] * t2[2] - t1[2] * t2[1];
+        const double cr1 = t1[2] * t2[0] - t1[0] * t2[2];
+        const double cr2 = t1[0] * t2[1] - t1[1] * t2[0];
+        const double J = sqrt(cr0 * cr0 + cr1 * cr1 + cr2 * cr2);
+        const double n[3] = {cr0 / J, cr1 / J, cr2 / J};
+        const double pk = f[k] * J * (s_gi[i] + 1.0) * area[tri] * 0.25 * s_ome[i] * s_ome[j];
+        const double r0 = xp[0] - xi[0], r1 = xp[1] - xi[1], r2 = xp[2] - xi[2];
+        const double ri = rsqrt(r0 * r0 + r1 * r1 + r2 * r2);
+        const double a[3] = {r0 * ri, r1 * ri, r2 * ri};
+        const double rdn = a[0] * n[0] + a[1] * n[1] + a[2] * n[2];
+        const double c3r = c3 * ri, c5r2 = c5 * ri * ri;
+        for (int ii = 0; ii < 3; ++ii)
+          for (int jj = 0; jj < 3; ++jj) {
+            const double dl = (ii == jj) ? 1.0 : 0.0;
+            const double u = (c4 * dl + a[ii] * a[jj]) * c3r;
+            const double tt = c5r2 * (rdn * (c6 * dl + 3.0 * a[ii] * a[jj]) +
+                                      c6 * (n[jj] * a[ii] - n[ii] * a[jj]));
+            g[jj + 3 * ii] += u * pk;
+            h[jj + 3 * ii] += tt * pk;
+          }
+      }
+    }
+    // combine the three point subsets of each node k
+    if (s < 3)
+      for (int p = 0; p < 9; ++p) {
+        s_part[wib][lane][p] = g[p];
+        s_part[wib][lane][9 + p] = h[p];
+      }
+    __syncwarp();
+    if (s == 0) {
+      for (int p = 0; p < 9; ++p) {
+        g[p] = s_part[wib][k][p] + s_part[wib][k + 9][p] + s_part[wib][k + 18][p];
+        h[p] = s_part[wib][k][9 + p] + s_part[wib][k + 9][9 + p] + s_part[wib][k + 18][9 + p];
+      }
+    }
+    __syncwarp();
+    // d2 = -sum_{k != nodo} h_k  (assembly_mod.f90:113-122)
+    double d2[9];
+    for (int p = 0; p < 9; ++p) {
+      double v = (s == 0 && k < ncone && k != nodo - 1) ? h[p] : 0.0;
+      for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+      d2[p] = -v;
+    }
+    if (s == 0 && k < ncone) {
+      const int ik = kc[k];
+      if (MODE == kModeA) {
+        for (int ld = 0; ld < 3; ++ld) {
+          const double bcv = P.bc[3 * k + ld + 27 * e];
+          const double* hk = (k == nodo - 1) ? d2 : h;  // entry at the node: rigid body
+          if (P.kode[3 * e + ld] == 0) {
+            double* col = P.A + (3 * (int64_t)ik + ld) * P.lda + row;
+            for (int jj = 0; jj < 3; ++jj) col[jj] -= g[jj + 3 * ld] * P.mat.mu;
+            for (int jj = 0; jj < 3; ++jj) fi[jj] -= hk[jj + 3 * ld] * bcv;
+          } else {
+            const int64_t dof = 3 * (int64_t)ik + ld;
+            if (P.uknown[dof] == 0) {
+              for (int jj = 0; jj < 3; ++jj) fi[jj] += g[jj + 3 * ld] * bcv;
+              double* col = P.A + dof * P.lda + row;
+              for (int jj = 0; jj < 3; ++jj) col[jj] += hk[jj + 3 * ld];
+            } else {
+              const double v = P.vp[dof];
+              for (int jj = 0; jj < 3; ++jj) fi[jj] += g[jj + 3 * ld] * bcv - hk[jj + 3 * ld] * v;
+            }
+          }
+        }
+      } else {
+        for (int ii = 0; ii < 3; ++ii) {
+          double* gc = P.G + (27 * (int64_t)e + 3 * k + ii) * P.ldg + row;
+          for (int jj = 0; jj < 3; ++jj) gc[jj] = g[jj + 3 * ii];
+          if (k != nodo - 1) {
+            double* hc = P.A + (3 * (int64_t)ik + ii) * P.lda + row;
+            for (int jj = 0; jj < 3; ++jj) hc[jj] += h[jj + 3 * ii];
+          }
+        }
+        if (k == 0)
+          for (int p = 0; p < 9; ++p) dsum[p] += d2[p];
+      }
+    }
+    __syncwarp();
+  }
+  if (MODE == kModeA) {
+    for (int p = 0; p < 3; ++p) {
+      double v = (s == 0) ? fi[p] : 0.0;
+      for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+      fi[p] = v;
+    }
+    if (lane == 0)
+      for (int r = 0; r < 3; ++r) P.FI[row + r] += fi[r];
+  } else if (lane == 0) {
+    for (int ld = 0; ld < 3; ++ld) {
+      double* col = P.A + (3 * (int64_t)in + ld) * P.lda + row;
+      for (int r = 0; r < 3; ++r) col[r] += dsum[r + 3 * ld];
+    }
+  }
+}
+
+// Pinned DOFs: row := unit row, rhs := 0.
+__global__ void pins_kernel(const int* pins, int npins, int64_t ncol, double* A, int64_t lda,
+                            double* FI) {
+  const int p = blockIdx.y;
+  if (p >= npins) return;
+  const int64_t r = pins[p];
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < ncol;
+       c += (int64_t)gridDim.x * blockDim.x)
+    A[r + c * lda] = (c == r) ? 1.0 : 0.0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) FI[r] = 0.0;
+}
+
+static AsmArgs make_args(bem_ctx* c) {
+  AsmArgs P{};
+  P.n = c->n;
+  P.ne = c->ne;
+  P.nbatches = c->nbatches;
+  P.in0 = 0;
+  P.nrows_nodes = c->n;
+  P.batches = c->batches.p;
+  P.nconec = c->nconec.p;
+  P.kconec = c->kconec.p;
+  P.kode = c->kode.p;
+  P.bc = c->bc.p;
+  P.uknown = c->uknown.p;
+  P.vp = c->vp.p;
+  P.nesim = c->nesim.p;
+  P.ke = c->ke.p;
+  P.x = c->x.p;
+  P.y = c->y.p;
+  P.z = c->z.p;
+  P.tab = c->tab.p;
+  P.mat = c->mat;
+  return P;
+}
+
+static int upload_singular_constants(bem_ctx* c) {
+  BEM_CUDA(c, cudaMemcpyToSymbol(s_gi, kGiQuad, sizeof(kGiQuad)));
+  BEM_CUDA(c, cudaMemcpyToSymbol(s_ome, kOmeQuad, sizeof(kOmeQuad)));
+  return BEM_OK;
+}
+
+int launch_ghmat8(bem_ctx* c, int precision) {
+  if (!c->have_geometry || !c->have_bc || !c->have_material)
+    return bem_fail(c, BEM_ERR_STATE, "ghmat8 needs mesh, material, bc and geometry");
+  if (precision != BEM_ASM_FP64 && precision != BEM_ASM_FP32_FAR)
+    return bem_fail(c, BEM_ERR_ARG, "unknown assembly precision");
+  int rc = upload_singular_constants(c);
+  if (rc) return rc;
+  const int64_t N = 3 * (int64_t)c->n;
+  const int64_t lda = (N + 31) / 32 * 32;
+  if (c->A.count != (size_t)(lda * N)) {
+    c->A.release();
+    cudaError_t e = c->A.alloc((size_t)(lda * N));
+    if (e != cudaSuccess) return bem_fail(c, BEM_ERR_OOM, "allocating the system matrix");
+  }
+  c->lda = lda;
+  BEM_CUDA(c, c->FI.alloc(N));
+  BEM_CUDA(c, cudaMemsetAsync(c->A.p, 0, c->A.bytes(), c->stream));
+  AsmArgs P = make_args(c);
+  P.A = c->A.p;
+  P.lda = lda;
+  P.FI = c->FI.p;
+  const int tiles = (c->n + 31) / 32;
+  ghmat_regular_kernel<kModeA><<<tiles, 256, 0, c->stream>>>(P);
+  BEM_LAUNCH_CHECK(c);
+  ghmat_singular_kernel<kModeA><<<(c->n + 3) / 4, 128, 0, c->stream>>>(P);
+  BEM_LAUNCH_CHECK(c);
+  if (c->npins > 0) {
+    dim3 grid(64, c->npins);
+    pins_kernel<<<grid, 256, 0, c->stream>>>(c->pins.p, c->npins, N, c->A.p, lda, c->FI.p);
+    BEM_LAUNCH_CHECK(c);
+  }
+  c->have_system = true;
+  c->have_solution = false;
+  c->factored_fp64 = false;
+  return BEM_OK;
+}
+
+int launch_hg(bem_ctx* c, int in0, int in1, double* dH, int64_t ldh, double* dG, int64_t ldg) {
+  if (!c->have_geometry || !c->have_material)
+    return bem_fail(c, BEM_ERR_STATE, "get_hg needs mesh, material and geometry");
+  int rc = upload_singular_constants(c);
+  if (rc) return rc;
+  AsmArgs P = make_args(c);
+  P.in0 = in0;
+  P.nrows_nodes = in1 - in0;
+  P.A = dH;
+  P.lda = ldh;
+  P.G = dG;
+  P.ldg = ldg;
+  const int tiles = (P.nrows_nodes + 31) / 32;
+  ghmat_regular_kernel<kModeHG><<<tiles, 256, 0, c->stream>>>(P);
+  BEM_LAUNCH_CHECK(c);
+  ghmat_singular_kernel<kModeHG><<<(P.nrows_nodes + 3) / 4, 128, 0, c->stream>>>(P);
+  BEM_LAUNCH_CHECK(c);
+  return BEM_OK;
+}
+
+}  // namespace bem

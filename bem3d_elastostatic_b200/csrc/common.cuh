@@ -1,0 +1,167 @@
+// Shared definitions of the B200 QUADESTH library: the context, status handling,
+// quadrature constants and device helpers (shape functions, Kelvin constants).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/bem3d_b200.h"
+
+namespace bem {
+
+// assembly_mod.f90:6-19 — the reference's literal quadrature constants (15 and 10
+// significant digits); parity needs these values, not freshly computed nodes.
+constexpr double kGiQuad[6] = {0.238619186083197, -0.238619186083197, 0.661209386466265,
+                               -0.661209386466265, 0.932469514203152, -0.932469514203152};
+constexpr double kOmeQuad[6] = {0.467913934572691, 0.467913934572691, 0.360761573048139,
+                                0.360761573048139, 0.171324492379170, 0.171324492379170};
+constexpr double kRrTri[4] = {0.0694318422, 0.3300094782, 0.6699905218, 0.9305681558};
+constexpr double kSsTri[4] = {0.0571041961, 0.2768430136, 0.5835904324, 0.8602401357};
+constexpr double kOmeiTri[4] = {0.1739274226, 0.3260725774, 0.3260725774, 0.1739274226};
+constexpr double kOmejTri[4] = {0.1355069134, 0.2034645680, 0.1298475476, 0.0311809709};
+// data_mod.f90:7
+constexpr double kPi = 3.14159265358979323846;
+
+// Per-element packed quadrature table used by the assembly kernels: 36 Gauss points
+// x {x, y, z, n1, n2, n3} followed by p12[36][9] = N_k * J * w_i * w_j
+// (assembly_mod.f90:363-369).  540 doubles = 4320 bytes per element.
+constexpr int kGp = 36;
+constexpr int kTabGeo = 6 * kGp;
+constexpr int kTabStride = kTabGeo + 9 * kGp;
+
+// Element schedule for the conflict-free assembly: batches of up to kBatch elements
+// that share no node.
+constexpr int kBatch = 8;
+
+struct Material {
+  double mu, nu;
+  double c3, c4, c5, c6;  // data_mod.f90:104-107
+};
+
+inline Material make_material(double mu, double nu) {
+  Material m;
+  m.mu = mu;
+  m.nu = nu;
+  m.c3 = 1.0 / (16.0 * kPi * (1.0 - nu) * mu);
+  m.c4 = 3.0 - 4.0 * nu;
+  m.c5 = -1.0 / (8.0 * kPi * (1.0 - nu));
+  m.c6 = 1.0 - 2.0 * nu;
+  return m;
+}
+
+// Device buffer with RAII release.
+template <typename T>
+struct DBuf {
+  T* p = nullptr;
+  size_t count = 0;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  ~DBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    count = 0;
+  }
+  cudaError_t alloc(size_t n) {
+    if (n == count && p) return cudaSuccess;
+    release();
+    if (n == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+    if (e != cudaSuccess) {
+      p = nullptr;
+      return e;
+    }
+    count = n;
+    return cudaSuccess;
+  }
+  size_t bytes() const { return count * sizeof(T); }
+};
+
+}  // namespace bem
+
+// The opaque context behind bem_ctx*.
+struct bem_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string last_error;
+  int sm_count = 148;
+
+  // mesh (host copies kept for the adjacency-derived tables)
+  int n = 0, ne = 0;
+  std::vector<int> h_nconec, h_kconec, h_kode;
+  std::vector<double> h_bc;
+  std::vector<int> h_nesim, h_ke;  // io_mod.f90:125-135
+  bool have_mesh = false, have_bc = false, have_material = false;
+  bem::Material mat{};
+
+  bem::DBuf<double> x, y, z;
+  bem::DBuf<int> nconec, kconec, kode;
+  bem::DBuf<double> bc;
+  bem::DBuf<int> ke;     // (8, n), 1-based element numbers, as the reference
+  bem::DBuf<int> nesim;  // (n)
+  // column-swap lookup (assembly_mod.f90:149-161, 194-206): per (node, ld) whether an
+  // adjacent element prescribes u there and the value it prescribes
+  bem::DBuf<int> uknown;
+  bem::DBuf<double> vp;
+  // conflict-free element schedule
+  bem::DBuf<int> batches;
+  int nbatches = 0;
+  bem::DBuf<int> pins;
+  int npins = 0;
+
+  // geometry (reference layout) and the packed assembly table
+  bem::DBuf<double> eta1, eta2, eta3, xja, xg1, xg2, xg3, ff, tab;
+  bool have_geometry = false;
+
+  // system
+  bem::DBuf<double> A, FI, X, U, DFI;  // FI: rhs; X: solution; U, DFI: reorganized u, t
+  int64_t lda = 0;
+  bool have_system = false, have_solution = false, factored_fp64 = false;
+
+  // LU / refinement workspace
+  bem::DBuf<float> A32;
+  bem::DBuf<int> piv;
+  bem::DBuf<double> work;
+  bem::DBuf<float> work32;
+  bem::DBuf<unsigned int> sync;
+  bem::DBuf<int> status;
+  bem::DBuf<double> rowscale, colscale;
+};
+
+// Status helpers (host).
+int bem_fail(bem_ctx* c, int code, const std::string& what);
+int bem_cuda_fail(bem_ctx* c, cudaError_t e, const char* where);
+
+#define BEM_CUDA(ctx, call)                                          \
+  do {                                                               \
+    cudaError_t _e = (call);                                         \
+    if (_e != cudaSuccess) return bem_cuda_fail((ctx), _e, #call);   \
+  } while (0)
+
+#define BEM_LAUNCH_CHECK(ctx)                                               \
+  do {                                                                      \
+    cudaError_t _e = cudaGetLastError();                                    \
+    if (_e != cudaSuccess) return bem_cuda_fail((ctx), _e, "kernel launch"); \
+  } while (0)
+
+// Internal (C++) entry points implemented in the .cu files.
+namespace bem {
+int launch_geometry(bem_ctx* c);
+int launch_ghmat8(bem_ctx* c, int precision);
+int launch_hg(bem_ctx* c, int in0, int in1, double* dH, int64_t ldh, double* dG,
+              int64_t ldg);
+int lu_factor_fp64(bem_ctx* c, double* A, int64_t lda, int n, int* d_piv, int* info,
+                   double* seconds);
+int lu_solve_fp64(bem_ctx* c, const double* LU, int64_t lda, int n, const int* d_piv,
+                  double* b);
+int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter,
+                bem_solve_info* stats, int* info);
+int launch_reorganize(bem_ctx* c);
+int launch_internal_points(bem_ctx* c, int l, const double* cx, const double* cy,
+                           const double* cz, double* u, double* s, double* pr, double* vm,
+                           int flags);
+}  // namespace bem

@@ -1,0 +1,671 @@
+// Blocked right-looking LU with partial pivoting (the DGESV replacement,
+// solver_mod.f90:28) and its triangular solves.  See lu.cuh for the layout and the
+// product form of the factors.
+//
+// One outer step factors an NB-wide panel of T = S^T (NB rows of S) and updates the
+// trailing matrix:
+//   for each 32-wide sub-panel:
+//     panel_kernel      cooperative launch over the SMs; every CTA holds a slice of
+//                       the sub-panel's S columns in shared memory; per pivot one
+//                       grid barrier (bounded spin) exchanges the per-CTA candidates;
+//                       the winner column and the diagonal column are swapped through
+//                       global copies, then each CTA scales and updates its slice
+//     swap_rows_kernel  applies the sub-panel's swaps to the other rows of the panel
+//                       and to the trailing rows (contiguous column segments)
+//     trsm_small + gemm update of the panel rows below the sub-panel
+//   inv_unit_upper + gemm (TRSM by inverse), then the trailing gemm update.
+#include <cfloat>
+#include <climits>
+#include <cmath>
+
+#include "lu.cuh"
+
+namespace bem {
+
+constexpr int kPitch = kPanelW + 1;  // shared-memory column pitch (conflict-free)
+constexpr long long kSpinLimit = 1ll << 24;
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void better(double& bv, int& bc, int& bg, double v, int cidx, int gidx) {
+  if (v > bv || (v == bv && cidx < bc)) {
+    bv = v;
+    bc = cidx;
+    bg = gidx;
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256, 1)
+    panel_kernel(T* S, int64_t lda, int n, int r0, int w, int chunk, int* piv, double* cand_val,
+                 int* cand_idx, T* cand_col, T* diag_col, unsigned* barrier, int* status) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* col = reinterpret_cast<T*>(smem_raw);  // [chunk][kPitch]
+  __shared__ T pvt[kPanelW];
+  __shared__ double red_v[8];
+  __shared__ int red_c[8], red_g[8];
+  __shared__ int s_local_c, s_win_g, s_win_c, s_abort;
+  const int G = gridDim.x, g = blockIdx.x, tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
+  const int c_beg = r0 + g * chunk;
+  const int c_end = min(n, c_beg + chunk);
+  const int ncols = max(0, c_end - c_beg);
+
+  for (int idx = tid; idx < ncols * kPanelW; idx += blockDim.x) {
+    const int cc = idx / kPanelW, j = idx % kPanelW;
+    col[cc * kPitch + j] = (j < w) ? S[(int64_t)(c_beg + cc) * lda + r0 + j] : T(0);
+  }
+  __syncthreads();
+
+  for (int t = 0; t < w; ++t) {
+    const int k = r0 + t;
+    const int par = t & 1;
+    // 1. local candidate: largest |S(k, c)| over owned c >= k, ties -> smallest c
+    double bv = -1.0;
+    int bc = INT_MAX, bg = g;
+    for (int cc = tid; cc < ncols; cc += blockDim.x) {
+      const int cgl = c_beg + cc;
+      if (cgl >= k) better(bv, bc, bg, fabs((double)col[cc * kPitch + t]), cgl, g);
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+      const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
+      const int oc = __shfl_xor_sync(0xffffffffu, bc, off);
+      better(bv, bc, bg, ov, oc, g);
+    }
+    if (lane == 0) {
+      red_v[wp] = bv;
+      red_c[wp] = bc;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      double v = red_v[0];
+      int cidx = red_c[0], gg = g;
+      for (int i = 1; i < (int)(blockDim.x >> 5); ++i) better(v, cidx, gg, red_v[i], red_c[i], g);
+      cand_val[par * G + g] = v;
+      cand_idx[par * G + g] = cidx;
+      s_local_c = cidx;
+    }
+    __syncthreads();
+    if (tid < w) {
+      const int lc = s_local_c;
+      if (lc != INT_MAX) cand_col[((int64_t)par * G + g) * kPanelW + tid] = col[(lc - c_beg) * kPitch + tid];
+      if (k >= c_beg && k < c_end) diag_col[par * kPanelW + tid] = col[(k - c_beg) * kPitch + tid];
+    }
+    __threadfence();
+    __syncthreads();
+    // 2. grid barrier (bounded)
+    if (tid == 0) {
+      atomicAdd(barrier, 1u);
+      const unsigned target = (unsigned)(t + 1) * (unsigned)G;
+      long long spins = 0;
+      int abort = 0;
+      while (ld_acquire_u32(barrier) < target) {
+        if (++spins > kSpinLimit || *((volatile int*)status) != 0) {
+          abort = 1;
+          break;
+        }
+        __nanosleep(64);
+      }
+      if (abort) atomicCAS(status, 0, BEM_ERR_TIMEOUT);
+      s_abort = abort;
+      __threadfence();
+    }
+    __syncthreads();
+    if (s_abort) return;
+    // 3. global pivot
+    if (wp == 0) {
+      double v = -1.0;
+      int cidx = INT_MAX, gg = 0;
+      for (int i = lane; i < G; i += 32) better(v, cidx, gg, __ldcg(cand_val + par * G + i), __ldcg(cand_idx + par * G + i), i);
+      for (int off = 16; off > 0; off >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, v, off);
+        const int oc = __shfl_xor_sync(0xffffffffu, cidx, off);
+        const int og = __shfl_xor_sync(0xffffffffu, gg, off);
+        better(v, cidx, gg, ov, oc, og);
+      }
+      if (lane == 0) {
+        s_win_g = gg;
+        s_win_c = cidx;
+      }
+    }
+    __syncthreads();
+    const int p = s_win_c;
+    if (tid < kPanelW)
+      pvt[tid] = (tid < w) ? __ldcg(cand_col + ((int64_t)par * G + s_win_g) * kPanelW + tid) : T(0);
+    __syncthreads();
+    const T pv = pvt[t];
+    if (g == 0 && tid == 0) {
+      piv[k] = p;
+      if (pv == T(0) && status[1] == 0) status[1] = k + 1;
+    }
+    if (tid < w) {
+      if (k >= c_beg && k < c_end) col[(k - c_beg) * kPitch + tid] = pvt[tid];
+      if (p != k && p >= c_beg && p < c_end) col[(p - c_beg) * kPitch + tid] = __ldcg(diag_col + par * kPanelW + tid);
+    }
+    __syncthreads();
+    // 4. scale the multipliers and update the rest of the sub-panel
+    if (pv != T(0)) {
+      for (int cc = tid; cc < ncols; cc += blockDim.x) {
+        if (c_beg + cc <= k) continue;
+        T* cp = col + cc * kPitch;
+        const T l = cp[t] / pv;
+        cp[t] = l;
+        for (int j = t + 1; j < w; ++j) cp[j] -= l * pvt[j];
+      }
+    }
+    __syncthreads();
+  }
+  for (int idx = tid; idx < ncols * kPanelW; idx += blockDim.x) {
+    const int cc = idx / kPanelW, j = idx % kPanelW;
+    if (j < w) S[(int64_t)(c_beg + cc) * lda + r0 + j] = col[cc * kPitch + j];
+  }
+}
+
+// Applies swaps k0+t <-> piv[k0+t] (t = 0..w-1 in order) to rows [a0,a1) and [b0,b1).
+template <typename T>
+__global__ void swap_rows_kernel(T* S, int64_t lda, const int* piv, int k0, int w, int a0, int a1, int b0,
+                                 int b1) {
+  __shared__ int sp[kPanelW];
+  if (threadIdx.x < w) sp[threadIdx.x] = piv[k0 + threadIdx.x];
+  __syncthreads();
+  const int na = a1 - a0;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (int64_t)na + (b1 - b0)) return;
+  const int64_t r = (i < na) ? a0 + i : b0 + (i - na);
+  for (int t = 0; t < w; ++t) {
+    const int p = sp[t];
+    if (p == k0 + t) continue;
+    T* x = S + r + (int64_t)(k0 + t) * lda;
+    T* y = S + r + (int64_t)p * lda;
+    const T a = *x;
+    *x = *y;
+    *y = a;
+  }
+}
+
+// Y := X * U^{-1} in place for rows [r_lo, r_hi), X = S(rows, k0..k0+w), U the unit
+// upper triangle of S(k0..k0+w, k0..k0+w).
+template <typename T>
+__global__ void trsm_small_kernel(T* S, int64_t lda, int k0, int w, int r_lo, int r_hi) {
+  __shared__ T U[kPanelW][kPanelW + 1];
+  for (int idx = threadIdx.x; idx < kPanelW * kPanelW; idx += blockDim.x) {
+    const int a = idx % kPanelW, b = idx / kPanelW;
+    U[a][b] = (a < w && b < w) ? S[(k0 + a) + (int64_t)(k0 + b) * lda] : T(0);
+  }
+  __syncthreads();
+  const int r = r_lo + blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= r_hi) return;
+  T y[kPanelW];
+#pragma unroll
+  for (int b = 0; b < kPanelW; ++b) {
+    if (b < w) {
+      T v = S[r + (int64_t)(k0 + b) * lda];
+#pragma unroll
+      for (int a = 0; a < b; ++a) v -= y[a] * U[a][b];
+      y[b] = v;
+      S[r + (int64_t)(k0 + b) * lda] = v;
+    }
+  }
+}
+
+// V = U^{-1} for the unit upper triangle U of S11 (jb x jb); V column-major (ldv).
+template <typename T>
+__global__ void inv_unit_upper_kernel(const T* S11, int64_t lda, int jb, T* V, int ldv) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* U = reinterpret_cast<T*>(smem_raw);  // [jb][jb] column-major
+  for (int idx = threadIdx.x; idx < jb * jb; idx += blockDim.x) {
+    const int a = idx % jb, b = idx / jb;
+    U[idx] = (a < b) ? S11[a + (int64_t)b * lda] : T(0);
+  }
+  __syncthreads();
+  const int j = threadIdx.x;
+  if (j >= jb) return;
+  T* v = V + (int64_t)j * ldv;
+  for (int i = jb - 1; i > j; --i) v[i] = T(0);
+  v[j] = T(1);
+  for (int i = j - 1; i >= 0; --i) {
+    T s = T(0);
+    for (int k = i + 1; k <= j; ++k) s += U[i + k * jb] * v[k];
+    v[i] = -s;
+  }
+}
+
+// ---------------------------------------------------------------------------------
+// GEMM (SIMT, register-tiled 128x128x8, 8x8 per thread)
+// ---------------------------------------------------------------------------------
+template <typename T, int MODE>
+__global__ void __launch_bounds__(256) gemm_simt_kernel(int M, int N, int K, const T* __restrict__ A, int64_t lda,
+                                                        const T* __restrict__ B, int64_t ldb, T* C, int64_t ldc) {
+  constexpr int BM = 128, BN = 128, BK = 8;
+  __shared__ T As[2][BK][BM];
+  __shared__ T Bs[2][BK][BN];
+  const int tid = threadIdx.x;
+  const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+  const int tx = tid % 16, ty = tid / 16;  // 16 x 16 threads, 8x8 each
+  T acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = T(0);
+  // loaders: A tile 128 x 8 (4 per thread), B tile 8 x 128 (4 per thread)
+  T ra[4], rb[4];
+  auto load = [&](int k0) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int idx = tid + 256 * i;
+      const int am = idx % BM, ak = idx / BM;
+      const int gm = m0 + am, gk = k0 + ak;
+      ra[i] = (gm < M && gk < K) ? A[gm + (int64_t)gk * lda] : T(0);
+      const int bk = idx % BK, bn = idx / BK;
+      const int gk2 = k0 + bk, gn = n0 + bn;
+      rb[i] = (gk2 < K && gn < N) ? B[gk2 + (int64_t)gn * ldb] : T(0);
+    }
+  };
+  auto store = [&](int buf) {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int idx = tid + 256 * i;
+      As[buf][idx / BM][idx % BM] = ra[i];
+      Bs[buf][idx % BK][idx / BK] = rb[i];
+    }
+  };
+  load(0);
+  store(0);
+  __syncthreads();
+  int buf = 0;
+  for (int k0 = 0; k0 < K; k0 += BK) {
+    const bool more = k0 + BK < K;
+    if (more) load(k0 + BK);
+#pragma unroll
+    for (int kk = 0; kk < BK; ++kk) {
+      T a[8], b[8];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        a[i] = As[buf][kk][ty * 4 + i];
+        a[4 + i] = As[buf][kk][64 + ty * 4 + i];
+        b[i] = Bs[buf][kk][tx * 4 + i];
+        b[4 + i] = Bs[buf][kk][64 + tx * 4 + i];
+      }
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+    if (more) {
+      store(buf ^ 1);
+      __syncthreads();
+      buf ^= 1;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int gm = m0 + ((i < 4) ? ty * 4 + i : 64 + ty * 4 + (i - 4));
+    if (gm >= M) continue;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int gn = n0 + ((j < 4) ? tx * 4 + j : 64 + tx * 4 + (j - 4));
+      if (gn >= N) continue;
+      T* cp = C + gm + (int64_t)gn * ldc;
+      if (MODE == 0)
+        *cp -= acc[i][j];
+      else
+        *cp = acc[i][j];
+    }
+  }
+}
+
+template <typename T>
+int gemm(bem_ctx* c, int M, int N, int K, const T* A, int64_t lda, const T* B, int64_t ldb, T* C, int64_t ldc,
+         int mode) {
+  if (M <= 0 || N <= 0 || K <= 0) return BEM_OK;
+  dim3 grid((N + 127) / 128, (M + 127) / 128);
+  if (grid.y > 65535) return bem_fail(c, BEM_ERR_ARG, "gemm: M too large");
+  if (mode == 0)
+    gemm_simt_kernel<T, 0><<<grid, 256, 0, c->stream>>>(M, N, K, A, lda, B, ldb, C, ldc);
+  else
+    gemm_simt_kernel<T, 1><<<grid, 256, 0, c->stream>>>(M, N, K, A, lda, B, ldb, C, ldc);
+  BEM_LAUNCH_CHECK(c);
+  return BEM_OK;
+}
+
+template int gemm<double>(bem_ctx*, int, int, int, const double*, int64_t, const double*, int64_t, double*,
+                          int64_t, int);
+template int gemm<float>(bem_ctx*, int, int, int, const float*, int64_t, const float*, int64_t, float*,
+                         int64_t, int);
+
+// ---------------------------------------------------------------------------------
+// factorisation driver
+// ---------------------------------------------------------------------------------
+namespace {
+
+struct PanelScratch {
+  DBuf<double> cand_val;
+  DBuf<int> cand_idx;
+  DBuf<unsigned char> cand_col, diag_col;
+  DBuf<unsigned> barrier;
+  DBuf<int> status;
+  DBuf<unsigned char> inv, ybuf;
+};
+
+template <typename T>
+int panel_launch(bem_ctx* c, PanelScratch& ps, T* S, int64_t lda, int n, int r0, int w, int* piv) {
+  static int max_smem_set = 0;
+  const int cols = n - r0;
+  int G = std::min(c->sm_count, std::max(1, (cols + 63) / 64));
+  int chunk = (cols + G - 1) / G;
+  size_t smem = (size_t)chunk * kPitch * sizeof(T);
+  if (smem > 200 * 1024) return bem_fail(c, BEM_ERR_ARG, "panel slice exceeds shared memory (matrix too large)");
+  if (!max_smem_set) {
+    cudaFuncSetAttribute(panel_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(panel_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    max_smem_set = 1;
+  }
+  int occ = 0;
+  BEM_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, panel_kernel<T>, 256, smem));
+  if (occ < 1) return bem_fail(c, BEM_ERR_CUDA, "panel kernel cannot be resident");
+  BEM_CUDA(c, cudaMemsetAsync(ps.barrier.p, 0, sizeof(unsigned), c->stream));
+  double* cv = ps.cand_val.p;
+  int* ci = ps.cand_idx.p;
+  T* cc = reinterpret_cast<T*>(ps.cand_col.p);
+  T* dc = reinterpret_cast<T*>(ps.diag_col.p);
+  unsigned* bar = ps.barrier.p;
+  int* st = ps.status.p;
+  void* args[] = {&S, &lda, &n, &r0, &w, &chunk, &piv, &cv, &ci, &cc, &dc, &bar, &st};
+  BEM_CUDA(c, cudaLaunchCooperativeKernel((void*)panel_kernel<T>, dim3(G), dim3(256), args, smem, c->stream));
+  return BEM_OK;
+}
+
+}  // namespace
+
+template <typename T>
+int lu_factor(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int nb, int* info) {
+  *info = 0;
+  PanelScratch ps;
+  const int Gmax = c->sm_count;
+  BEM_CUDA(c, ps.cand_val.alloc(2 * (size_t)Gmax));
+  BEM_CUDA(c, ps.cand_idx.alloc(2 * (size_t)Gmax));
+  BEM_CUDA(c, ps.cand_col.alloc(2 * (size_t)Gmax * kPanelW * sizeof(T)));
+  BEM_CUDA(c, ps.diag_col.alloc(2 * (size_t)kPanelW * sizeof(T)));
+  BEM_CUDA(c, ps.barrier.alloc(1));
+  BEM_CUDA(c, ps.status.alloc(2));
+  BEM_CUDA(c, ps.inv.alloc((size_t)nb * nb * sizeof(T)));
+  const int64_t ldy = ((int64_t)n + 31) / 32 * 32;
+  BEM_CUDA(c, ps.ybuf.alloc((size_t)ldy * nb * sizeof(T)));
+  BEM_CUDA(c, cudaMemsetAsync(ps.status.p, 0, 2 * sizeof(int), c->stream));
+  T* V = reinterpret_cast<T*>(ps.inv.p);
+  T* Y = reinterpret_cast<T*>(ps.ybuf.p);
+  const size_t inv_smem = (size_t)nb * nb * sizeof(T);
+  if (inv_smem > 200 * 1024) return bem_fail(c, BEM_ERR_ARG, "block size too large for the inverse kernel");
+  cudaFuncSetAttribute(inv_unit_upper_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inv_smem);
+  int rc;
+  for (int j0 = 0; j0 < n; j0 += nb) {
+    const int jb = std::min(nb, n - j0);
+    for (int r0 = j0; r0 < j0 + jb; r0 += kPanelW) {
+      const int w = std::min(kPanelW, j0 + jb - r0);
+      if ((rc = panel_launch<T>(c, ps, S, lda, n, r0, w, piv))) return rc;
+      // swaps on the other rows of the panel and on the trailing rows
+      const int a0 = j0, a1 = r0, b0 = r0 + w, b1 = n;
+      const int64_t rows = (int64_t)(a1 - a0) + (b1 - b0);
+      if (rows > 0) {
+        swap_rows_kernel<T><<<(unsigned)((rows + 255) / 256), 256, 0, c->stream>>>(S, lda, piv, r0, w, a0, a1, b0,
+                                                                                   b1);
+        BEM_LAUNCH_CHECK(c);
+      }
+      // update the panel rows below the sub-panel
+      const int q0 = r0 + w, q1 = j0 + jb;
+      if (q1 > q0) {
+        trsm_small_kernel<T><<<(q1 - q0 + 127) / 128, 128, 0, c->stream>>>(S, lda, r0, w, q0, q1);
+        BEM_LAUNCH_CHECK(c);
+        if ((rc = gemm<T>(c, q1 - q0, n - q0, w, S + q0 + (int64_t)r0 * lda, lda, S + r0 + (int64_t)q0 * lda, lda,
+                          S + q0 + (int64_t)q0 * lda, lda, 0)))
+          return rc;
+      }
+    }
+    const int t0 = j0 + jb;
+    if (t0 < n) {
+      const int m = n - t0;
+      inv_unit_upper_kernel<T><<<1, ((jb + 31) / 32) * 32, inv_smem, c->stream>>>(S + j0 + (int64_t)j0 * lda, lda, jb,
+                                                                                   V, nb);
+      BEM_LAUNCH_CHECK(c);
+      if ((rc = gemm<T>(c, m, jb, jb, S + t0 + (int64_t)j0 * lda, lda, V, nb, Y, ldy, 1))) return rc;
+      BEM_CUDA(c, cudaMemcpy2DAsync(S + t0 + (int64_t)j0 * lda, lda * sizeof(T), Y, ldy * sizeof(T), m * sizeof(T),
+                                    jb, cudaMemcpyDeviceToDevice, c->stream));
+      if ((rc = gemm<T>(c, m, m, jb, Y, ldy, S + j0 + (int64_t)t0 * lda, lda, S + t0 + (int64_t)t0 * lda, lda, 0)))
+        return rc;
+    }
+  }
+  int st[2];
+  BEM_CUDA(c, cudaMemcpyAsync(st, ps.status.p, sizeof(st), cudaMemcpyDeviceToHost, c->stream));
+  BEM_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (st[0] != 0) return bem_fail(c, st[0], "panel grid barrier timed out");
+  *info = st[1];
+  return BEM_OK;
+}
+
+template int lu_factor<double>(bem_ctx*, double*, int64_t, int, int*, int, int*);
+template int lu_factor<float>(bem_ctx*, float*, int64_t, int, int*, int, int*);
+
+// ---------------------------------------------------------------------------------
+// triangular solves
+// ---------------------------------------------------------------------------------
+
+// forward: solve U^T w = b on the diagonal block [j0, j0+jb) (lower triangle of S,
+// non-unit diagonal), b overwritten by w
+template <typename T>
+__global__ void fwd_diag_kernel(const T* S, int64_t lda, int j0, int jb, double* b) {
+  __shared__ double w[256];
+  const int t = threadIdx.x;
+  if (t < jb) w[t] = b[j0 + t];
+  __syncthreads();
+  for (int cidx = 0; cidx < jb; ++cidx) {
+    if (t == cidx) w[t] = w[t] / (double)S[(j0 + t) + (int64_t)(j0 + t) * lda];
+    __syncthreads();
+    if (t > cidx && t < jb) w[t] -= (double)S[(j0 + t) + (int64_t)(j0 + cidx) * lda] * w[cidx];
+    __syncthreads();
+  }
+  if (t < jb) b[j0 + t] = w[t];
+}
+
+// b[r] -= sum_c S(r, c) w[c] for r in [r0, n), c in [j0, j0+jb)
+template <typename T>
+__global__ void fwd_gemv_kernel(const T* S, int64_t lda, int n, int r0, int j0, int jb, double* b) {
+  __shared__ double w[256];
+  if (threadIdx.x < jb) w[threadIdx.x] = b[j0 + threadIdx.x];
+  __syncthreads();
+  const int64_t r = r0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  double acc = 0.0;
+  const T* p = S + r + (int64_t)j0 * lda;
+  for (int cidx = 0; cidx < jb; ++cidx) acc = fma((double)p[(int64_t)cidx * lda], w[cidx], acc);
+  b[r] -= acc;
+}
+
+// backward, off-panel part: part[blk][t] = sum_{c' in blk} S(j0+t, c') v[c']
+template <typename T>
+__global__ void bwd_dot_kernel(const T* S, int64_t lda, int n, int j0, int jb, int c0, const double* v,
+                               double* part) {
+  const int t = threadIdx.x;  // row of the panel
+  const int cs = c0 + blockIdx.x * 128;
+  const int ce = min(n, cs + 128);
+  double acc = 0.0;
+  if (t < jb)
+    for (int cc = cs; cc < ce; ++cc) acc = fma((double)S[(j0 + t) + (int64_t)cc * lda], v[cc], acc);
+  if (t < jb) part[(int64_t)blockIdx.x * 256 + t] = acc;
+}
+
+// backward, within-panel part and the panel's swaps (one CTA)
+template <typename T>
+__global__ void bwd_finish_kernel(const T* S, int64_t lda, int n, int j0, int jb, int nblk, const double* part,
+                                  const int* piv, double* v) {
+  __shared__ double w[256];
+  const int t = threadIdx.x;
+  if (t < jb) {
+    double s = 0.0;
+    for (int bb = 0; bb < nblk; ++bb) s += part[(int64_t)bb * 256 + t];
+    w[t] = v[j0 + t] - s;
+  }
+  __syncthreads();
+  for (int cidx = jb - 1; cidx >= 0; --cidx) {
+    // w[cidx] final; remove its contribution from the rows above
+    if (t < cidx) w[t] -= (double)S[(j0 + t) + (int64_t)(j0 + cidx) * lda] * w[cidx];
+    __syncthreads();
+  }
+  if (t < jb) v[j0 + t] = w[t];
+  __syncthreads();
+  if (t == 0)
+    for (int q = jb - 1; q >= 0; --q) {
+      const int p = piv[j0 + q];
+      if (p != j0 + q) {
+        const double a = v[j0 + q];
+        v[j0 + q] = v[p];
+        v[p] = a;
+      }
+    }
+}
+
+template <typename T>
+int lu_solve(bem_ctx* c, const T* S, int64_t lda, int n, const int* piv, int nb, double* b) {
+  if (nb > 256) return bem_fail(c, BEM_ERR_ARG, "lu_solve: block size > 256");
+  const int maxblk = (n + 127) / 128 + 1;
+  if (c->work.count < (size_t)maxblk * 256) BEM_CUDA(c, c->work.alloc((size_t)maxblk * 256));
+  for (int j0 = 0; j0 < n; j0 += nb) {
+    const int jb = std::min(nb, n - j0);
+    fwd_diag_kernel<T><<<1, 256, 0, c->stream>>>(S, lda, j0, jb, b);
+    BEM_LAUNCH_CHECK(c);
+    const int r0 = j0 + jb;
+    if (r0 < n) {
+      fwd_gemv_kernel<T><<<(n - r0 + 255) / 256, 256, 0, c->stream>>>(S, lda, n, r0, j0, jb, b);
+      BEM_LAUNCH_CHECK(c);
+    }
+  }
+  const int last = ((n - 1) / nb) * nb;
+  for (int j0 = last; j0 >= 0; j0 -= nb) {
+    const int jb = std::min(nb, n - j0);
+    const int c0 = j0 + jb;
+    const int nblk = (n - c0 + 127) / 128;
+    if (nblk > 0) {
+      bwd_dot_kernel<T><<<nblk, 256, 0, c->stream>>>(S, lda, n, j0, jb, c0, b, c->work.p);
+      BEM_LAUNCH_CHECK(c);
+    }
+    bwd_finish_kernel<T><<<1, 256, 0, c->stream>>>(S, lda, n, j0, jb, nblk, c->work.p, piv, b);
+    BEM_LAUNCH_CHECK(c);
+  }
+  return BEM_OK;
+}
+
+template int lu_solve<double>(bem_ctx*, const double*, int64_t, int, const int*, int, double*);
+template int lu_solve<float>(bem_ctx*, const float*, int64_t, int, const int*, int, double*);
+
+// ---------------------------------------------------------------------------------
+// residual r = b - A x (FP64) with infinity norms
+// ---------------------------------------------------------------------------------
+constexpr int kResCols = 512;
+
+__global__ void residual_part_kernel(const double* A, int64_t lda, int n, const double* x, double* part,
+                                     double* apart, int want_anorm) {
+  __shared__ double xs[kResCols];
+  const int cs = blockIdx.y * kResCols;
+  const int ce = min(n, cs + kResCols);
+  for (int i = threadIdx.x; i < ce - cs; i += blockDim.x) xs[i] = x[cs + i];
+  __syncthreads();
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  double acc = 0.0, aabs = 0.0;
+  const double* p = A + r + (int64_t)cs * lda;
+  for (int cc = 0; cc < ce - cs; ++cc) {
+    const double a = p[(int64_t)cc * lda];
+    acc = fma(a, xs[cc], acc);
+    if (want_anorm) aabs += fabs(a);
+  }
+  part[(int64_t)blockIdx.y * n + r] = acc;
+  if (want_anorm) apart[(int64_t)blockIdx.y * n + r] = aabs;
+}
+
+__device__ __forceinline__ void atomic_max_nonneg(double* addr, double v) {
+  // non-negative doubles order like their bit patterns
+  atomicMax(reinterpret_cast<unsigned long long*>(addr), __double_as_longlong(v));
+}
+
+__global__ void residual_finish_kernel(int n, int nchunk, const double* part, const double* apart, const double* b,
+                                       const double* x, double* r, double* norms, int want_anorm) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double rv = 0.0, xv = 0.0, bv = 0.0, av = 0.0;
+  if (i < n) {
+    double s = 0.0, sa = 0.0;
+    for (int k = 0; k < nchunk; ++k) {
+      s += part[(int64_t)k * n + i];
+      if (want_anorm) sa += apart[(int64_t)k * n + i];
+    }
+    const double ri = b[i] - s;
+    r[i] = ri;
+    rv = fabs(ri);
+    xv = fabs(x[i]);
+    bv = fabs(b[i]);
+    av = sa;
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    rv = fmax(rv, __shfl_xor_sync(0xffffffffu, rv, off));
+    xv = fmax(xv, __shfl_xor_sync(0xffffffffu, xv, off));
+    bv = fmax(bv, __shfl_xor_sync(0xffffffffu, bv, off));
+    av = fmax(av, __shfl_xor_sync(0xffffffffu, av, off));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomic_max_nonneg(norms + 0, rv);
+    atomic_max_nonneg(norms + 1, xv);
+    atomic_max_nonneg(norms + 2, bv);
+    if (want_anorm) atomic_max_nonneg(norms + 3, av);
+  }
+}
+
+int residual_fp64(bem_ctx* c, const double* A, int64_t lda, int n, const double* x, const double* b, double* r,
+                  double* norms, bool want_anorm) {
+  const int nchunk = (n + kResCols - 1) / kResCols;
+  const size_t need = (size_t)nchunk * n * (want_anorm ? 2 : 1) + 8;
+  if (c->work.count < need) {
+    c->work.release();
+    BEM_CUDA(c, c->work.alloc(need));
+  }
+  double* part = c->work.p + 8;
+  double* apart = part + (size_t)nchunk * n;
+  double* dn = c->work.p;
+  BEM_CUDA(c, cudaMemsetAsync(dn, 0, 4 * sizeof(double), c->stream));
+  dim3 grid((n + 255) / 256, nchunk);
+  residual_part_kernel<<<grid, 256, 0, c->stream>>>(A, lda, n, x, part, apart, want_anorm ? 1 : 0);
+  BEM_LAUNCH_CHECK(c);
+  residual_finish_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(n, nchunk, part, apart, b, x, r, dn,
+                                                                  want_anorm ? 1 : 0);
+  BEM_LAUNCH_CHECK(c);
+  BEM_CUDA(c, cudaMemcpyAsync(norms, dn, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  BEM_CUDA(c, cudaStreamSynchronize(c->stream));
+  return BEM_OK;
+}
+
+// ---------------------------------------------------------------------------------
+// FP64 entry points used by context.cu
+// ---------------------------------------------------------------------------------
+constexpr int kNbFp64 = 128;
+
+int lu_factor_fp64(bem_ctx* c, double* A, int64_t lda, int n, int* d_piv, int* info, double* seconds) {
+  cudaEvent_t e0, e1;
+  BEM_CUDA(c, cudaEventCreate(&e0));
+  BEM_CUDA(c, cudaEventCreate(&e1));
+  BEM_CUDA(c, cudaEventRecord(e0, c->stream));
+  int rc = lu_factor<double>(c, A, lda, n, d_piv, kNbFp64, info);
+  BEM_CUDA(c, cudaEventRecord(e1, c->stream));
+  BEM_CUDA(c, cudaEventSynchronize(e1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (seconds) *seconds = ms * 1e-3;
+  return rc;
+}
+
+int lu_solve_fp64(bem_ctx* c, const double* LU, int64_t lda, int n, const int* d_piv, double* b) {
+  return lu_solve<double>(c, LU, lda, n, d_piv, kNbFp64, b);
+}
+
+}  // namespace bem

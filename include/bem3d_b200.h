@@ -1,0 +1,142 @@
+/*
+ * bem3d_b200.h — C ABI of the B200-native (sm_100a) QUADESTH boundary-element hot path.
+ *
+ * Every entry point takes plain pointers and sizes and returns an int status.  The
+ * reference exposes its hot path as Fortran module procedures working on module
+ * globals (data_mod.f90:37-52); each function below names the procedure it stands
+ * in for.  A Fortran caller binds them with ISO_C_BINDING (INTEGRATION.md shows the
+ * interface block); Python binds them with ctypes (bem3d_elastostatic_b200/_lib.py).
+ *
+ * Data contract (identical to the reference's globals):
+ *   x, y, z       (n) node coordinates
+ *   nconec        (ne) nodes per element: 9 = quad9, 6 = tri6
+ *   kconec        (9, ne) column-major, 1-based node numbers
+ *   kode          (3*ne) per element and component: 0 = displacement prescribed,
+ *                 1 = traction prescribed
+ *   bc            (27, ne) column-major, value of component ld at local node k is
+ *                 bc(3*(k-1)+ld, e)
+ *   A             (3n, 3n) column-major, leading dimension lda
+ *   FI            (3n); DFI (27, ne)
+ *   u_int (3,l), sigma_int (6,l) ordered xx,yy,zz,xy,yz,zx, prin (3,l), vm (l)
+ *
+ * Status: 0 = success; > 0 = the LU met an exactly zero pivot at that 1-based step
+ * (the DGESV info convention); < 0 = one of the BEM_ERR_* codes.  Host pointers may be
+ * NULL where marked "nullable": the data then stays resident on the device.
+ * One CUDA stream per context; a context is not re-entrant.
+ */
+#ifndef BEM3D_B200_H
+#define BEM3D_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct bem_ctx bem_ctx;
+
+#define BEM_OK 0
+#define BEM_ERR_ARG (-1)      /* bad argument or size */
+#define BEM_ERR_CUDA (-2)     /* a CUDA call failed */
+#define BEM_ERR_OOM (-3)      /* device allocation failed */
+#define BEM_ERR_TIMEOUT (-4)  /* a bounded device wait ran out (grid barrier) */
+#define BEM_ERR_STATE (-5)    /* called out of order (e.g. solve before ghmat8) */
+#define BEM_ERR_MESH (-6)     /* a node lies in more than 8 elements, bad connectivity */
+#define BEM_ERR_NOCONV (-7)   /* refinement did not reach the requested tolerance */
+
+/* Solve precision modes (bem_solve). */
+#define BEM_PREC_FP64 0      /* FP64 LU with partial pivoting: the DGESV replacement */
+#define BEM_PREC_FP32_IR 1   /* FP32 LU (FP32 CUDA-core trailing update) + FP64 refinement */
+#define BEM_PREC_BF16_IR 2   /* scaled FP32 LU whose trailing update runs on the tensor
+                                cores with BF16 operands and FP32 accumulation,
+                                + FP64 refinement / GMRES-IR */
+
+/* Assembly precision modes (bem_ghmat8). */
+#define BEM_ASM_FP64 0  /* every element integral in FP64 (parity with the reference) */
+#define BEM_ASM_FP32_FAR 1 /* far-field integrals in FP32, near-singular and singular in FP64 */
+
+/* Internal-point flags (bem_internal_points). */
+#define BEM_IP_KELVIN_CONSISTENT 1 /* use T*_ij u_j in the displacement identity; clear =
+                                      the reference's stress_mod.f90:838-843 form */
+
+typedef struct {
+  int iterations;        /* refinement sweeps (IR) or GMRES iterations */
+  int restarts;          /* GMRES restarts */
+  double rel_residual;   /* ||b - A x|| / (||A||_inf ||x|| + ||b||), FP64 */
+  double factor_seconds; /* device time of the factorisation */
+  double refine_seconds; /* device time of the refinement */
+  double gflops;         /* 2/3 N^3 / factor_seconds */
+} bem_solve_info;
+
+/* Context ------------------------------------------------------------------------ */
+int bem_ctx_create(bem_ctx** ctx, int device);
+int bem_ctx_destroy(bem_ctx* ctx);
+const char* bem_last_error(const bem_ctx* ctx);
+/* sync the context's stream; returns a pending asynchronous error, if any */
+int bem_sync(bem_ctx* ctx);
+
+/* Input: replaces input_data (io_mod.f90:36-146) and update_material_constants
+ * (data_mod.f90:97-108).  Node -> element adjacency (io_mod.f90:125-135) is built here;
+ * a node in more than 8 elements is rejected (BEM_ERR_MESH). */
+int bem_set_mesh(bem_ctx* ctx, int n, int ne, const double* x, const double* y,
+                 const double* z, const int* nconec, const int* kconec);
+int bem_set_material(bem_ctx* ctx, double mu, double nu);
+int bem_set_bc(bem_ctx* ctx, const int* kode, const double* bc);
+/* Pinned displacement DOFs (0-based 3*(node-1)+comp) held at 0: row := unit row,
+ * rhs := 0 after assembly.  No counterpart in the reference (supports there are per
+ * element); used by the uniaxial-cube and sphere workloads. */
+int bem_set_pins(bem_ctx* ctx, int npins, const int* dofs);
+
+/* precompute_element_geometry (assembly_mod.f90:28-51) with etaxja (:225-337).
+ * Optional host copies of the tables in the reference's layout (nullable each):
+ * eta1..3, xja, xg1..3 as (36, ne), ff as (9, 36, ne). */
+int bem_precompute_geometry(bem_ctx* ctx);
+int bem_get_geometry(bem_ctx* ctx, double* eta1, double* eta2, double* eta3, double* xja,
+                     double* xg1, double* xg2, double* xg3, double* ff);
+
+/* ghmat8 (assembly_mod.f90:53-223): assembles A and FI on the device (column swap,
+ * rigid-body diagonal).  A_out/FI_out (nullable) receive host copies; lda >= 3n. */
+int bem_ghmat8(bem_ctx* ctx, int asm_precision, double* A_out, int64_t lda, double* FI_out);
+
+/* H (3n x 3n, rigid-body diagonal included) and G (3n x 27ne) for collocation nodes
+ * [in0, in1) — the two products ghmat8 combines, for entrywise parity checks. */
+int bem_get_hg(bem_ctx* ctx, int in0, int in1, double* H, int64_t ldh, double* G,
+               int64_t ldg);
+
+/* solve_linear_system (solver_mod.f90:17-36): solves A x = FI in place on the device.
+ * BEM_PREC_FP64 factors A itself (as DGESV overwrites it); the *_IR modes factor a
+ * lower-precision copy and refine against the FP64 A to rel_tol.  *info follows DGESV
+ * (0, or the 1-based step of an exactly zero pivot).  FI_inout (nullable) receives the
+ * solution on the host.  stats (nullable) receives iteration counts and timings. */
+int bem_solve(bem_ctx* ctx, int precision, double rel_tol, int max_iter, double* FI_inout,
+              int* info, bem_solve_info* stats);
+
+/* LAPACK dgesv drop-in on host buffers (solver_mod.f90:28): A (n x n, lda) is
+ * overwritten by its factors, B (n x nrhs, ldb) by the solution; ipiv receives the
+ * 1-based pivot sequence of the factorisation (pivoting over the rows of A^T: see the
+ * header of lu.cu).  Runs on the context's device. */
+int bem_dgesv(bem_ctx* ctx, int n, int nrhs, double* A, int lda, int* ipiv, double* B,
+              int ldb, int* info);
+
+/* reorganize_solution (io_mod.f90:148-183): FI -> nodal displacements u (3n),
+ * DFI (27, ne) element-nodal tractions.  Host outputs nullable. */
+int bem_reorganize(bem_ctx* ctx, double* FI_out, double* DFI_out);
+
+/* compute_internal_points (stress_mod.f90:511-886): Somigliana displacement and stress
+ * with calc_principal_and_vm (:299-359) at l points.  flags: BEM_IP_*. */
+int bem_internal_points(bem_ctx* ctx, int l, const double* cx, const double* cy,
+                        const double* cz, double* u_int, double* sigma_int, double* prin,
+                        double* vm, int flags);
+
+/* Device-resident variants for callers that keep data in HBM (the Python layer and
+ * the benchmark).  Pointers are device addresses. */
+int bem_device_state(bem_ctx* ctx, double** A, int64_t* lda, double** FI, double** DFI);
+int bem_internal_points_device(bem_ctx* ctx, int l, const double* d_cx, const double* d_cy,
+                               const double* d_cz, double* d_u_int, double* d_sigma_int,
+                               double* d_prin, double* d_vm, int flags);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BEM3D_B200_H */

@@ -1,0 +1,150 @@
+"""GPU parity against the CPU oracle, through the C ABI.
+
+Tolerances (FP64 throughout):
+  * geometry tables: bitwise (the geometry kernel is compiled without FMA contraction
+    and follows the reference's operation order);
+  * H, G, A, FI: |gpu - oracle| <= 1e-12 * |oracle| + 1e-14 * max|row| — the second
+    term covers entries that are sums of element integrals of opposite sign, where
+    reordering the (at most 8-term) sum legitimately changes the last bits;
+  * solution vector, internal displacements and stresses: relative 1e-10 in the
+    infinity norm (the north-star bound for boundary u/t and internal stresses).
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from bem3d_elastostatic_b200.mesh import cube_grid_points, uniaxial_cube
+
+pytestmark = pytest.mark.gpu
+
+
+def close_entrywise(got, ref, rel=1e-12, rowfloor=1e-14):
+    rowmax = np.abs(ref).max(axis=1, keepdims=True)
+    tol = rel * np.abs(ref) + rowfloor * rowmax + 1e-300
+    return float((np.abs(got - ref) / tol).max())
+
+
+@pytest.fixture(scope="module")
+def cube2():
+    return uniaxial_cube(2, young=1.0, nu=0.3, points=cube_grid_points([0.25, 0.5, 0.75]))
+
+
+@pytest.fixture(scope="module")
+def gpu_cube2(cube2):
+    from bem3d_elastostatic_b200.api import Quadesth
+
+    q = Quadesth(cube2)
+    q.precompute_element_geometry()
+    return q
+
+
+@pytest.fixture(scope="module")
+def gpu_cube8(cube8_mesh):
+    from bem3d_elastostatic_b200.api import Quadesth
+
+    q = Quadesth(cube8_mesh)
+    q.precompute_element_geometry()
+    return q
+
+
+@pytest.mark.parametrize("which", ["cube2", "cube8"])
+def test_geometry_bitwise(which, cube2, cube8_mesh, gpu_cube2, gpu_cube8):
+    mesh, q = (cube2, gpu_cube2) if which == "cube2" else (cube8_mesh, gpu_cube8)
+    ref = O.Oracle(mesh).geometry()
+    got = q.geometry_tables()
+    for k in ref:
+        assert np.array_equal(got[k], ref[k]), k
+
+
+@pytest.mark.parametrize("which", ["cube2", "cube8"])
+def test_hg_entrywise(which, cube2, cube8_mesh, gpu_cube2, gpu_cube8):
+    mesh, q = (cube2, gpu_cube2) if which == "cube2" else (cube8_mesh, gpu_cube8)
+    Hr, Gr = O.Oracle(mesh).hg()
+    H, G = q.hg()
+    assert close_entrywise(H, Hr) <= 1.0
+    assert close_entrywise(G, Gr) <= 1.0
+
+
+def test_hg_row_block(gpu_cube8, cube8_mesh):
+    Hr, Gr = O.Oracle(cube8_mesh).hg(100, 164)
+    H, G = gpu_cube8.hg(100, 164)
+    assert close_entrywise(H, Hr) <= 1.0
+    assert close_entrywise(G, Gr) <= 1.0
+
+
+@pytest.mark.parametrize("which", ["cube2", "cube8"])
+def test_ghmat8_entrywise(which, cube2, cube8_mesh, gpu_cube2, gpu_cube8):
+    mesh, q = (cube2, gpu_cube2) if which == "cube2" else (cube8_mesh, gpu_cube8)
+    Ar, Fr = O.Oracle(mesh).ghmat8()
+    A, F = q.ghmat8(return_system=True)
+    assert close_entrywise(A, Ar) <= 1.0
+    assert np.abs(F - Fr).max() <= 1e-12 * np.abs(Fr).max()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32-ir"])
+def test_solution_vs_oracle_cube8(precision, cube8_mesh):
+    from bem3d_elastostatic_b200.api import Quadesth
+
+    ref = O.Oracle(cube8_mesh).run()
+    q = Quadesth(cube8_mesh)
+    res = q.run(precision=precision)
+    for key in ("x", "u"):
+        err = np.abs(res[key] - ref[key]).max() / np.abs(ref[key]).max()
+        assert err <= 1e-10, (key, err)
+    terr = np.abs(res["t"] - ref["t"]).max() / np.abs(ref["t"]).max()
+    assert terr <= 1e-10
+    for key in ("u_int", "sigma", "prin", "vm"):
+        err = np.abs(res[key] - ref[key]).max() / np.abs(ref[key]).max()
+        assert err <= 1e-10, (key, err)
+
+
+def test_end_to_end_vs_reference_output(cube8_mesh, cube8_golden):
+    """The GPU path reproduces the reference's own internal_points.dat to its print."""
+    from bem3d_elastostatic_b200.api import Quadesth
+
+    res = Quadesth(cube8_mesh).run()
+    got = np.concatenate([res["u_int"].T, res["sigma"].T, res["vm"][:, None], res["prin"].T], 1)
+    ref = cube8_golden[:, 4:]
+    e = np.floor(np.log10(np.maximum(np.abs(ref), 1e-300))) + 1
+    half_ulp = 0.5 * 10.0 ** (e - 7)
+    scale = np.empty(13)
+    scale[:3] = np.abs(ref[:, :3]).max()
+    scale[3:] = np.abs(ref[:, 3:]).max()
+    tol = half_ulp + 1e-12 * scale[None, :]
+    assert (np.abs(got - ref) / tol).max() <= 1.0
+
+
+def test_kelvin_consistent_flag(cube2):
+    from bem3d_elastostatic_b200.api import Quadesth
+
+    orc = O.Oracle(cube2)
+    ref = orc.run()
+    fixed = orc.internal_points(ref["u"], ref["t"], kelvin_consistent=True)
+    q = Quadesth(cube2)
+    res = q.run(kelvin_consistent=True)
+    assert np.abs(res["u_int"] - fixed[0]).max() <= 1e-10 * np.abs(fixed[0]).max()
+    P = np.stack([cube2.cx, cube2.cy, cube2.cz], 1)
+    ua = np.stack([-0.3 * P[:, 0], -0.3 * P[:, 1], P[:, 2]], 1)
+    assert np.abs(res["u_int"].T - ua).max() < 1e-4
+
+
+def test_dgesv_dropin_random():
+    from bem3d_elastostatic_b200.api import dgesv
+
+    rng = np.random.default_rng(7)
+    for n in (1, 5, 33, 130, 300):
+        A = rng.standard_normal((n, n)) + n * np.eye(n) * 0.1
+        B = rng.standard_normal((n, 2))
+        _, ipiv, X, info = dgesv(A, B)
+        assert info == 0
+        res = np.abs(A @ X - B).max() / (np.abs(A).sum(1).max() * np.abs(X).max())
+        assert res < 1e-14, (n, res)
+        assert ipiv.min() >= 1 and ipiv.max() <= n
+
+
+def test_dgesv_singular_reports_info():
+    from bem3d_elastostatic_b200.api import dgesv
+
+    A = np.ones((40, 40))
+    _, _, _, info = dgesv(A, np.ones(40))
+    assert info > 0
