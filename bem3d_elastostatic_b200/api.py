@@ -88,10 +88,10 @@ class Quadesth:
         st = _lib.SolveInfo()
         rc = self.ctx.L.bem_solve(self.ctx.h, PRECISIONS[precision], tol, max_iter, _lib.ptr(x),
                                   _lib.C.byref(info), _lib.C.byref(st))
+        self.solve_info = st.as_dict()
         if rc > 0 or info.value != 0:
             raise SolverFailure(info.value or rc)
         self.ctx.check(rc, "solve")
-        self.solve_info = st.as_dict()
         return x
 
     # io_mod.f90:148

@@ -58,10 +58,13 @@ __device__ __forceinline__ int sym_idx(int a, int b) {
   return s == 1 ? 3 : (s == 3 ? 4 : 5);
 }
 
+// fi_acc (3) and d1_acc (9) are this lane's running sums over its elements, kept in
+// shared memory so the 9 x NC accumulators below have the register file to themselves.
 template <int NC, int MODE>
 __device__ __forceinline__ void regular_pair(const AsmArgs& P, int e, const int* kc, double xi0,
                                              double xi1, double xi2, int64_t row,
-                                             double* fi, double* d1) {
+                                             double* fi_acc, double* d1) {
+  double fi[3] = {0.0, 0.0, 0.0};
   constexpr int NG = (NC == 9) ? 36 : 16;
   const double* T = P.tab + (int64_t)e * kTabStride;
   const double c3 = P.mat.c3, c4 = P.mat.c4, c5 = P.mat.c5, c6 = P.mat.c6;
@@ -100,12 +103,27 @@ __device__ __forceinline__ void regular_pair(const AsmArgs& P, int e, const int*
 #pragma unroll
       for (int ld = 0; ld < 3; ++ld) {
         if (__ldg(P.kode + 3 * e + ld) == 0) {
+          // read-modify-write of the element's 3 x NC block: all loads first, so the
+          // update costs one memory round trip instead of one per entry
           const double mu = P.mat.mu;
+          constexpr int G1 = (NC + 2) / 3;
 #pragma unroll
-          for (int k = 0; k < NC; ++k) {
-            double* col = P.A + (3 * (int64_t)kc[k] + ld) * P.lda + row;
+          for (int k0 = 0; k0 < NC; k0 += G1) {
+            double old[G1][3];
 #pragma unroll
-            for (int jj = 0; jj < 3; ++jj) col[jj] = col[jj] - g[k][sym_idx(jj, ld)] * mu;
+            for (int kk = 0; kk < G1; ++kk)
+              if (k0 + kk < NC) {
+                const double* col = P.A + (3 * (int64_t)kc[k0 + kk] + ld) * P.lda + row;
+#pragma unroll
+                for (int jj = 0; jj < 3; ++jj) old[kk][jj] = col[jj];
+              }
+#pragma unroll
+            for (int kk = 0; kk < G1; ++kk)
+              if (k0 + kk < NC) {
+                double* col = P.A + (3 * (int64_t)kc[k0 + kk] + ld) * P.lda + row;
+#pragma unroll
+                for (int jj = 0; jj < 3; ++jj) col[jj] = old[kk][jj] - g[k0 + kk][sym_idx(jj, ld)] * mu;
+              }
           }
         } else {
 #pragma unroll
@@ -181,32 +199,64 @@ __device__ __forceinline__ void regular_pair(const AsmArgs& P, int e, const int*
             for (int jj = 0; jj < 3; ++jj) fi[jj] = fma(-h[k][jj + 3 * ld], b, fi[jj]);
           }
         } else {
+          // the same batched read-modify-write, in thirds of the element's nodes to
+          // bound the registers held next to the 9 x NC accumulators
+          constexpr int H1 = (NC + 2) / 3;
 #pragma unroll
-          for (int k = 0; k < NC; ++k) {
-            const int64_t dof = 3 * (int64_t)kc[k] + ld;
-            if (__ldg(P.uknown + dof) == 0) {
-              double* col = P.A + dof * P.lda + row;
+          for (int k0 = 0; k0 < NC; k0 += H1) {
+            double old[H1][3];
+            bool uk[H1];
 #pragma unroll
-              for (int jj = 0; jj < 3; ++jj) col[jj] = col[jj] + h[k][jj + 3 * ld];
-            } else {
-              const double v = __ldg(P.vp + dof);
+            for (int kk = 0; kk < H1; ++kk) {
+              const int k = k0 + kk;
+              if (k < NC) {
+                const int64_t dof = 3 * (int64_t)kc[k] + ld;
+                uk[kk] = __ldg(P.uknown + dof) != 0;
+                if (!uk[kk]) {
+                  const double* col = P.A + dof * P.lda + row;
 #pragma unroll
-              for (int jj = 0; jj < 3; ++jj) fi[jj] = fma(-h[k][jj + 3 * ld], v, fi[jj]);
+                  for (int jj = 0; jj < 3; ++jj) old[kk][jj] = col[jj];
+                }
+              }
+            }
+#pragma unroll
+            for (int kk = 0; kk < H1; ++kk) {
+              const int k = k0 + kk;
+              if (k < NC) {
+                const int64_t dof = 3 * (int64_t)kc[k] + ld;
+                if (!uk[kk]) {
+                  double* col = P.A + dof * P.lda + row;
+#pragma unroll
+                  for (int jj = 0; jj < 3; ++jj) col[jj] = old[kk][jj] + h[k][jj + 3 * ld];
+                } else {
+                  const double v = __ldg(P.vp + dof);
+#pragma unroll
+                  for (int jj = 0; jj < 3; ++jj) fi[jj] = fma(-h[k][jj + 3 * ld], v, fi[jj]);
+                }
+              }
             }
           }
         }
       }
     } else {
 #pragma unroll
-      for (int k = 0; k < NC; ++k)
+      for (int k = 0; k < NC; ++k) {
+        double old[3][3];
 #pragma unroll
-        for (int ii = 0; ii < 3; ++ii) {
-          double* col = P.A + (3 * (int64_t)kc[k] + ii) * P.lda + row;
+        for (int ii = 0; ii < 3; ++ii)
 #pragma unroll
-          for (int jj = 0; jj < 3; ++jj) col[jj] = col[jj] + h[k][jj + 3 * ii];
-        }
+          for (int jj = 0; jj < 3; ++jj) old[ii][jj] = P.A[(3 * (int64_t)kc[k] + ii) * P.lda + row + jj];
+#pragma unroll
+        for (int ii = 0; ii < 3; ++ii)
+#pragma unroll
+          for (int jj = 0; jj < 3; ++jj)
+            P.A[(3 * (int64_t)kc[k] + ii) * P.lda + row + jj] = old[ii][jj] + h[k][jj + 3 * ii];
+      }
     }
   }
+  if (MODE == kModeA)
+#pragma unroll
+    for (int jj = 0; jj < 3; ++jj) fi_acc[jj] += fi[jj];
 }
 
 template <int MODE>
@@ -219,10 +269,10 @@ __global__ void __launch_bounds__(256, 1) ghmat_regular_kernel(AsmArgs P) {
   const int in = P.in0 + (active ? local : 0);
   const double xi0 = P.x[in], xi1 = P.y[in], xi2 = P.z[in];
   const int64_t row = 3 * (int64_t)local;
-  double fi[3] = {0.0, 0.0, 0.0};
-  double d1[9];
+  double* fi = &s_red[w][lane][0];  // running FI sums of this lane
+  double* d1 = &s_red[w][lane][3];  // running rigid-body sums d1
 #pragma unroll
-  for (int p = 0; p < 9; ++p) d1[p] = 0.0;
+  for (int p = 0; p < 12; ++p) s_red[w][lane][p] = 0.0;
 
   for (int b = 0; b < P.nbatches; ++b) {
     const int e = __ldg(P.batches + kBatch * b + w);
@@ -245,8 +295,6 @@ __global__ void __launch_bounds__(256, 1) ghmat_regular_kernel(AsmArgs P) {
     __syncthreads();
   }
 
-  for (int p = 0; p < 3; ++p) s_red[w][lane][p] = fi[p];
-  for (int p = 0; p < 9; ++p) s_red[w][lane][3 + p] = d1[p];
   __syncthreads();
   if (w == 0 && active) {
     double F[3] = {0.0, 0.0, 0.0}, D[9];

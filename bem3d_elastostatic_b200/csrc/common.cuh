@@ -130,6 +130,11 @@ struct bem_ctx {
   bem::DBuf<unsigned int> sync;
   bem::DBuf<int> status;
   bem::DBuf<double> rowscale, colscale;
+  // GEMM flavour of the LU trailing update: f64_gemm 1 = DMMA tensor path, 0 = SIMT;
+  // f32_gemm 3 = BF16 x3 split, 1 = plain BF16 (tensor cores), 0 = SIMT FP32
+  int f64_gemm = 1;
+  int f32_gemm = 3;
+  int f32_gemm_override = -1;  // BEM_F32_GEMM environment override (0, 1, 3)
 };
 
 // Status helpers (host).

@@ -7,6 +7,7 @@
 // conflict-free element schedule of the assembly kernel.  All numerics run on the GPU.
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 
 #include "common.cuh"
@@ -116,6 +117,8 @@ int bem_ctx_create(bem_ctx** out, int device) {
     return BEM_ERR_CUDA;
   }
   cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
+  if (const char* v = getenv("BEM_F32_GEMM")) c->f32_gemm_override = atoi(v);
+  if (const char* v = getenv("BEM_F64_GEMM")) c->f64_gemm = atoi(v);
   *out = c;
   return BEM_OK;
 }
@@ -311,6 +314,7 @@ int bem_solve(bem_ctx* c, int precision, double rel_tol, int max_iter, double* F
   } else if (precision == BEM_PREC_FP32_IR || precision == BEM_PREC_BF16_IR) {
     rc = bem::solve_mixed(c, precision, rel_tol > 0 ? rel_tol : 1e-12, max_iter > 0 ? max_iter : 50, &st,
                           info);
+    if (stats) *stats = st;
     if (rc) return rc;
     if (*info != 0) return *info;
   } else {

@@ -17,6 +17,9 @@
 #include <cfloat>
 #include <climits>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <vector>
 
 #include "lu.cuh"
 
@@ -303,32 +306,55 @@ __global__ void __launch_bounds__(256) gemm_simt_kernel(int M, int N, int K, con
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
     const int gm = m0 + ((i < 4) ? ty * 4 + i : 64 + ty * 4 + (i - 4));
-    if (gm >= M) continue;
+    T old[8];
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
       const int gn = n0 + ((j < 4) ? tx * 4 + j : 64 + tx * 4 + (j - 4));
-      if (gn >= N) continue;
-      T* cp = C + gm + (int64_t)gn * ldc;
-      if (MODE == 0)
-        *cp -= acc[i][j];
-      else
-        *cp = acc[i][j];
+      old[j] = (MODE == 0 && gm < M && gn < N) ? C[gm + (int64_t)gn * ldc] : T(0);
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int gn = n0 + ((j < 4) ? tx * 4 + j : 64 + tx * 4 + (j - 4));
+      if (gm < M && gn < N) C[gm + (int64_t)gn * ldc] = (MODE == 0) ? old[j] - acc[i][j] : acc[i][j];
     }
   }
 }
 
+int gemm_dmma(bem_ctx* c, int M, int N, int K, const double* A, int64_t lda, const double* B, int64_t ldb, double* C,
+              int64_t ldc, int mode);
+int gemm_bf16(bem_ctx* c, int M, int N, int K, const float* A, int64_t lda, const float* B, int64_t ldb, float* C,
+              int64_t ldc, int mode, int split);
+bool gemm_tc_ok(const void* A, int64_t lda, const void* B, int64_t ldb, int elem);
+
 template <typename T>
-int gemm(bem_ctx* c, int M, int N, int K, const T* A, int64_t lda, const T* B, int64_t ldb, T* C, int64_t ldc,
-         int mode) {
-  if (M <= 0 || N <= 0 || K <= 0) return BEM_OK;
+static int gemm_simt(bem_ctx* c, int M, int N, int K, const T* A, int64_t lda, const T* B, int64_t ldb, T* C,
+                     int64_t ldc, int mode) {
   dim3 grid((N + 127) / 128, (M + 127) / 128);
-  if (grid.y > 65535) return bem_fail(c, BEM_ERR_ARG, "gemm: M too large");
   if (mode == 0)
     gemm_simt_kernel<T, 0><<<grid, 256, 0, c->stream>>>(M, N, K, A, lda, B, ldb, C, ldc);
   else
     gemm_simt_kernel<T, 1><<<grid, 256, 0, c->stream>>>(M, N, K, A, lda, B, ldb, C, ldc);
   BEM_LAUNCH_CHECK(c);
   return BEM_OK;
+}
+
+// FP64: DMMA tensor path; FP32: per-context choice (c->f32_gemm) of the BF16 tensor path
+// with 3 (FP32-grade) or 1 (plain BF16) terms, or SIMT FP32.  Misaligned operands take
+// the SIMT kernel.
+template <typename T>
+int gemm(bem_ctx* c, int M, int N, int K, const T* A, int64_t lda, const T* B, int64_t ldb, T* C, int64_t ldc,
+         int mode) {
+  if (M <= 0 || N <= 0 || K <= 0) return BEM_OK;
+  if ((M + 127) / 128 > 65535) return bem_fail(c, BEM_ERR_ARG, "gemm: M too large");
+  const bool tc = gemm_tc_ok(A, lda, B, ldb, (int)sizeof(T));
+  if (sizeof(T) == 8) {
+    if (tc && c->f64_gemm == 1)
+      return gemm_dmma(c, M, N, K, (const double*)A, lda, (const double*)B, ldb, (double*)C, ldc, mode);
+  } else {
+    if (tc && (c->f32_gemm == 1 || c->f32_gemm == 3))
+      return gemm_bf16(c, M, N, K, (const float*)A, lda, (const float*)B, ldb, (float*)C, ldc, mode, c->f32_gemm);
+  }
+  return gemm_simt<T>(c, M, N, K, A, lda, B, ldb, C, ldc, mode);
 }
 
 template int gemm<double>(bem_ctx*, int, int, int, const double*, int64_t, const double*, int64_t, double*,
@@ -380,6 +406,44 @@ int panel_launch(bem_ctx* c, PanelScratch& ps, T* S, int64_t lda, int n, int r0,
 
 }  // namespace
 
+// Optional phase timing of the factorisation (environment BEM_LU_PROFILE=1): CUDA
+// events around every phase, summed per phase and printed to stderr at the end.
+struct LUProfile {
+  bool on = false;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev;
+  int cur = -1;
+  cudaEvent_t start{};
+  void begin(int phase, cudaStream_t s) {
+    if (!on) return;
+    cudaEvent_t a;
+    cudaEventCreate(&a);
+    cudaEventRecord(a, s);
+    start = a;
+    cur = phase;
+  }
+  void end(cudaStream_t s) {
+    if (!on) return;
+    cudaEvent_t b;
+    cudaEventCreate(&b);
+    cudaEventRecord(b, s);
+    ev.push_back({cur, {start, b}});
+  }
+  void report(int n) {
+    if (!on) return;
+    double t[5] = {0, 0, 0, 0, 0};
+    for (auto& e : ev) {
+      float ms = 0.f;
+      cudaEventSynchronize(e.second.second);
+      cudaEventElapsedTime(&ms, e.second.first, e.second.second);
+      t[e.first] += ms;
+      cudaEventDestroy(e.second.first);
+      cudaEventDestroy(e.second.second);
+    }
+    fprintf(stderr, "[lu n=%d] panel %.1f ms  swaps %.1f ms  panel-update %.1f ms  trsm %.1f ms  trailing-gemm %.1f ms\n",
+            n, t[0], t[1], t[2], t[3], t[4]);
+  }
+};
+
 template <typename T>
 int lu_factor(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int nb, int* info) {
   *info = 0;
@@ -401,11 +465,16 @@ int lu_factor(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int nb, int* info)
   if (inv_smem > 200 * 1024) return bem_fail(c, BEM_ERR_ARG, "block size too large for the inverse kernel");
   cudaFuncSetAttribute(inv_unit_upper_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inv_smem);
   int rc;
+  LUProfile prof;
+  prof.on = getenv("BEM_LU_PROFILE") != nullptr;
   for (int j0 = 0; j0 < n; j0 += nb) {
     const int jb = std::min(nb, n - j0);
     for (int r0 = j0; r0 < j0 + jb; r0 += kPanelW) {
       const int w = std::min(kPanelW, j0 + jb - r0);
+      prof.begin(0, c->stream);
       if ((rc = panel_launch<T>(c, ps, S, lda, n, r0, w, piv))) return rc;
+      prof.end(c->stream);
+      prof.begin(1, c->stream);
       // swaps on the other rows of the panel and on the trailing rows
       const int a0 = j0, a1 = r0, b0 = r0 + w, b1 = n;
       const int64_t rows = (int64_t)(a1 - a0) + (b1 - b0);
@@ -414,8 +483,10 @@ int lu_factor(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int nb, int* info)
                                                                                    b1);
         BEM_LAUNCH_CHECK(c);
       }
+      prof.end(c->stream);
       // update the panel rows below the sub-panel
       const int q0 = r0 + w, q1 = j0 + jb;
+      prof.begin(2, c->stream);
       if (q1 > q0) {
         trsm_small_kernel<T><<<(q1 - q0 + 127) / 128, 128, 0, c->stream>>>(S, lda, r0, w, q0, q1);
         BEM_LAUNCH_CHECK(c);
@@ -423,20 +494,26 @@ int lu_factor(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int nb, int* info)
                           S + q0 + (int64_t)q0 * lda, lda, 0)))
           return rc;
       }
+      prof.end(c->stream);
     }
     const int t0 = j0 + jb;
     if (t0 < n) {
       const int m = n - t0;
+      prof.begin(3, c->stream);
       inv_unit_upper_kernel<T><<<1, ((jb + 31) / 32) * 32, inv_smem, c->stream>>>(S + j0 + (int64_t)j0 * lda, lda, jb,
                                                                                    V, nb);
       BEM_LAUNCH_CHECK(c);
       if ((rc = gemm<T>(c, m, jb, jb, S + t0 + (int64_t)j0 * lda, lda, V, nb, Y, ldy, 1))) return rc;
       BEM_CUDA(c, cudaMemcpy2DAsync(S + t0 + (int64_t)j0 * lda, lda * sizeof(T), Y, ldy * sizeof(T), m * sizeof(T),
                                     jb, cudaMemcpyDeviceToDevice, c->stream));
+      prof.end(c->stream);
+      prof.begin(4, c->stream);
       if ((rc = gemm<T>(c, m, m, jb, Y, ldy, S + j0 + (int64_t)t0 * lda, lda, S + t0 + (int64_t)t0 * lda, lda, 0)))
         return rc;
+      prof.end(c->stream);
     }
   }
+  prof.report(n);
   int st[2];
   BEM_CUDA(c, cudaMemcpyAsync(st, ps.status.p, sizeof(st), cudaMemcpyDeviceToHost, c->stream));
   BEM_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -453,17 +530,23 @@ template int lu_factor<float>(bem_ctx*, float*, int64_t, int, int*, int, int*);
 // ---------------------------------------------------------------------------------
 
 // forward: solve U^T w = b on the diagonal block [j0, j0+jb) (lower triangle of S,
-// non-unit diagonal), b overwritten by w
+// non-unit diagonal), b overwritten by w.  The block is staged in shared memory first.
 template <typename T>
 __global__ void fwd_diag_kernel(const T* S, int64_t lda, int j0, int jb, double* b) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* D = reinterpret_cast<T*>(smem_raw);  // [jb][jb] column-major
   __shared__ double w[256];
   const int t = threadIdx.x;
+  for (int idx = t; idx < jb * jb; idx += blockDim.x) {
+    const int r = idx % jb, cc = idx / jb;
+    D[idx] = (r >= cc) ? S[(j0 + r) + (int64_t)(j0 + cc) * lda] : T(0);
+  }
   if (t < jb) w[t] = b[j0 + t];
   __syncthreads();
   for (int cidx = 0; cidx < jb; ++cidx) {
-    if (t == cidx) w[t] = w[t] / (double)S[(j0 + t) + (int64_t)(j0 + t) * lda];
+    if (t == cidx) w[t] = w[t] / (double)D[t + t * jb];
     __syncthreads();
-    if (t > cidx && t < jb) w[t] -= (double)S[(j0 + t) + (int64_t)(j0 + cidx) * lda] * w[cidx];
+    if (t > cidx && t < jb) w[t] -= (double)D[t + cidx * jb] * w[cidx];
     __syncthreads();
   }
   if (t < jb) b[j0 + t] = w[t];
@@ -496,12 +579,19 @@ __global__ void bwd_dot_kernel(const T* S, int64_t lda, int n, int j0, int jb, i
   if (t < jb) part[(int64_t)blockIdx.x * 256 + t] = acc;
 }
 
-// backward, within-panel part and the panel's swaps (one CTA)
+// backward, within-panel part and the panel's swaps (one CTA); the panel's strict
+// upper block is staged in shared memory first
 template <typename T>
 __global__ void bwd_finish_kernel(const T* S, int64_t lda, int n, int j0, int jb, int nblk, const double* part,
                                   const int* piv, double* v) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* D = reinterpret_cast<T*>(smem_raw);  // [jb][jb] column-major
   __shared__ double w[256];
   const int t = threadIdx.x;
+  for (int idx = t; idx < jb * jb; idx += blockDim.x) {
+    const int r = idx % jb, cc = idx / jb;
+    D[idx] = (r < cc) ? S[(j0 + r) + (int64_t)(j0 + cc) * lda] : T(0);
+  }
   if (t < jb) {
     double s = 0.0;
     for (int bb = 0; bb < nblk; ++bb) s += part[(int64_t)bb * 256 + t];
@@ -510,7 +600,7 @@ __global__ void bwd_finish_kernel(const T* S, int64_t lda, int n, int j0, int jb
   __syncthreads();
   for (int cidx = jb - 1; cidx >= 0; --cidx) {
     // w[cidx] final; remove its contribution from the rows above
-    if (t < cidx) w[t] -= (double)S[(j0 + t) + (int64_t)(j0 + cidx) * lda] * w[cidx];
+    if (t < cidx) w[t] -= (double)D[t + cidx * jb] * w[cidx];
     __syncthreads();
   }
   if (t < jb) v[j0 + t] = w[t];
@@ -529,11 +619,15 @@ __global__ void bwd_finish_kernel(const T* S, int64_t lda, int n, int j0, int jb
 template <typename T>
 int lu_solve(bem_ctx* c, const T* S, int64_t lda, int n, const int* piv, int nb, double* b) {
   if (nb > 256) return bem_fail(c, BEM_ERR_ARG, "lu_solve: block size > 256");
+  const size_t dsm = (size_t)nb * nb * sizeof(T);
+  if (dsm > 200 * 1024) return bem_fail(c, BEM_ERR_ARG, "lu_solve: diagonal block exceeds shared memory");
+  cudaFuncSetAttribute(fwd_diag_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm);
+  cudaFuncSetAttribute(bwd_finish_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm);
   const int maxblk = (n + 127) / 128 + 1;
   if (c->work.count < (size_t)maxblk * 256) BEM_CUDA(c, c->work.alloc((size_t)maxblk * 256));
   for (int j0 = 0; j0 < n; j0 += nb) {
     const int jb = std::min(nb, n - j0);
-    fwd_diag_kernel<T><<<1, 256, 0, c->stream>>>(S, lda, j0, jb, b);
+    fwd_diag_kernel<T><<<1, 256, dsm, c->stream>>>(S, lda, j0, jb, b);
     BEM_LAUNCH_CHECK(c);
     const int r0 = j0 + jb;
     if (r0 < n) {
@@ -550,7 +644,7 @@ int lu_solve(bem_ctx* c, const T* S, int64_t lda, int n, const int* piv, int nb,
       bwd_dot_kernel<T><<<nblk, 256, 0, c->stream>>>(S, lda, n, j0, jb, c0, b, c->work.p);
       BEM_LAUNCH_CHECK(c);
     }
-    bwd_finish_kernel<T><<<1, 256, 0, c->stream>>>(S, lda, n, j0, jb, nblk, c->work.p, piv, b);
+    bwd_finish_kernel<T><<<1, 256, dsm, c->stream>>>(S, lda, n, j0, jb, nblk, c->work.p, piv, b);
     BEM_LAUNCH_CHECK(c);
   }
   return BEM_OK;

@@ -51,11 +51,16 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
   BEM_CUDA(c, cudaEventRecord(e0, c->stream));
   to_fp32_kernel<<<c->sm_count * 8, 256, 0, c->stream>>>(c->A.p, lda, n, c->A32.p);
   BEM_LAUNCH_CHECK(c);
+  const int saved = c->f32_gemm;
+  if (c->f32_gemm_override >= 0)
+    c->f32_gemm = c->f32_gemm_override;
+  else
+    c->f32_gemm = (precision == BEM_PREC_BF16_IR) ? 1 : 3;
   int rc = lu_factor<float>(c, c->A32.p, lda, n, c->piv.p, kNbMixed, info);
+  c->f32_gemm = saved;
   if (rc) return rc;
   BEM_CUDA(c, cudaEventRecord(e1, c->stream));
   if (*info != 0) return BEM_OK;
-  (void)precision;
   // x0 = LU^{-1} b, then x += LU^{-1} (b - A x)
   BEM_CUDA(c, cudaMemsetAsync(c->X.p, 0, n * sizeof(double), c->stream));
   BEM_CUDA(c, cudaMemcpyAsync(r.p, c->FI.p, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
