@@ -31,11 +31,12 @@ BEM_IP_KELVIN_CONSISTENT = 1
 
 # every symbol the header declares, for the export check
 EXPORTS = [
-    "bem_ctx_create", "bem_ctx_destroy", "bem_last_error", "bem_sync", "bem_set_mesh",
+    "bem_ctx_create", "bem_ctx_destroy", "bem_last_error", "bem_sync", "bem_get_stream",
+    "bem_set_mesh",
     "bem_set_material", "bem_set_bc", "bem_set_pins", "bem_precompute_geometry",
     "bem_get_geometry", "bem_ghmat8", "bem_get_hg", "bem_solve", "bem_dgesv",
     "bem_reorganize", "bem_internal_points", "bem_device_state",
-    "bem_internal_points_device",
+    "bem_internal_points_device", "bem_profile_begin", "bem_profile_end",
 ]
 
 
@@ -53,6 +54,17 @@ class SolveInfo(C.Structure):
     _fields_ = [("iterations", C.c_int), ("restarts", C.c_int), ("rel_residual", C.c_double),
                 ("factor_seconds", C.c_double), ("refine_seconds", C.c_double),
                 ("gflops", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Profile(C.Structure):
+    _fields_ = [("kernel_launches", C.c_longlong), ("lu_panel_ms", C.c_double),
+                ("lu_swap_ms", C.c_double), ("lu_panel_update_ms", C.c_double),
+                ("lu_trsm_ms", C.c_double), ("lu_trailing_ms", C.c_double),
+                ("lu_trailing_launches", C.c_longlong), ("lu_trailing_flops", C.c_double),
+                ("lu_trailing_bytes", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -87,6 +99,7 @@ def load(build_if_needed: bool = True):
     L.bem_last_error.argtypes = [_vp]
     L.bem_last_error.restype = C.c_char_p
     L.bem_sync.argtypes = [_vp]
+    L.bem_get_stream.argtypes = [_vp, C.POINTER(C.c_void_p)]
     L.bem_set_mesh.argtypes = [_vp, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp]
     L.bem_set_material.argtypes = [_vp, C.c_double, C.c_double]
     L.bem_set_bc.argtypes = [_vp, _vp, _vp]
@@ -102,6 +115,8 @@ def load(build_if_needed: bool = True):
     L.bem_device_state.argtypes = [_vp, C.POINTER(C.c_void_p), C.POINTER(C.c_int64),
                                    C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]
     L.bem_internal_points_device.argtypes = [_vp, C.c_int] + [_vp] * 7 + [C.c_int]
+    L.bem_profile_begin.argtypes = [_vp, C.c_int]
+    L.bem_profile_end.argtypes = [_vp, C.POINTER(Profile)]
     _lib = L
     return L
 
@@ -132,6 +147,23 @@ class Context:
             msg = self.L.bem_last_error(self.h)
             raise BemError(rc, f"{what}: {msg.decode() if msg else ''}")
         return rc
+
+    def stream(self) -> int:
+        """The context's cudaStream_t as an integer handle."""
+        s = C.c_void_p()
+        self.check(self.L.bem_get_stream(self.h, C.byref(s)), "get_stream")
+        return int(s.value or 0)
+
+    def sync(self):
+        self.check(self.L.bem_sync(self.h), "sync")
+
+    def profile_begin(self, timing: bool = True):
+        self.check(self.L.bem_profile_begin(self.h, 1 if timing else 0), "profile_begin")
+
+    def profile_end(self) -> dict:
+        p = Profile()
+        self.check(self.L.bem_profile_end(self.h, C.byref(p)), "profile_end")
+        return p.as_dict()
 
     def close(self):
         if getattr(self, "h", None):

@@ -135,6 +135,10 @@ struct bem_ctx {
   int f64_gemm = 1;
   int f32_gemm = 3;
   int f32_gemm_override = -1;  // BEM_F32_GEMM environment override (0, 1, 3)
+  // profiling (bem_profile_begin/end)
+  long long launches = 0;
+  int prof_timing = 0;
+  bem_profile prof{};
 };
 
 // Status helpers (host).
@@ -149,6 +153,7 @@ int bem_cuda_fail(bem_ctx* c, cudaError_t e, const char* where);
 
 #define BEM_LAUNCH_CHECK(ctx)                                               \
   do {                                                                      \
+    ++(ctx)->launches;                                                      \
     cudaError_t _e = cudaGetLastError();                                    \
     if (_e != cudaSuccess) return bem_cuda_fail((ctx), _e, "kernel launch"); \
   } while (0)

@@ -140,6 +140,12 @@ int bem_sync(bem_ctx* c) {
   return BEM_OK;
 }
 
+int bem_get_stream(bem_ctx* c, void** stream) {
+  if (!c || !stream) return BEM_ERR_ARG;
+  *stream = (void*)c->stream;
+  return BEM_OK;
+}
+
 int bem_set_mesh(bem_ctx* c, int n, int ne, const double* x, const double* y, const double* z,
                  const int* nconec, const int* kconec) {
   if (!c || n <= 0 || ne <= 0 || !x || !y || !z || !nconec || !kconec)
@@ -408,6 +414,23 @@ int bem_internal_points(bem_ctx* c, int l, const double* cx, const double* cy, c
   BEM_CUDA(c, cudaMemcpyAsync(pr, dp, 3 * (size_t)l * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   BEM_CUDA(c, cudaMemcpyAsync(vm, dv, (size_t)l * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   BEM_CUDA(c, cudaStreamSynchronize(c->stream));
+  return BEM_OK;
+}
+
+int bem_profile_begin(bem_ctx* c, int timing) {
+  if (!c) return BEM_ERR_ARG;
+  c->launches = 0;
+  c->prof = bem_profile{};
+  c->prof_timing = timing ? 1 : 0;
+  return BEM_OK;
+}
+
+int bem_profile_end(bem_ctx* c, bem_profile* out) {
+  if (!c) return BEM_ERR_ARG;
+  BEM_CUDA(c, cudaStreamSynchronize(c->stream));
+  c->prof.kernel_launches = c->launches;
+  if (out) *out = c->prof;
+  c->prof_timing = 0;
   return BEM_OK;
 }
 

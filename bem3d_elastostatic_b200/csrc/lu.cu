@@ -410,37 +410,57 @@ int panel_launch(bem_ctx* c, PanelScratch& ps, T* S, int64_t lda, int n, int r0,
 // events around every phase, summed per phase and printed to stderr at the end.
 struct LUProfile {
   bool on = false;
-  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev;
+  struct Ev {
+    int phase;
+    cudaEvent_t a, b;
+    double flops, bytes;
+  };
+  std::vector<Ev> ev;
   int cur = -1;
   cudaEvent_t start{};
   void begin(int phase, cudaStream_t s) {
     if (!on) return;
-    cudaEvent_t a;
-    cudaEventCreate(&a);
-    cudaEventRecord(a, s);
-    start = a;
+    cudaEventCreate(&start);
+    cudaEventRecord(start, s);
     cur = phase;
   }
-  void end(cudaStream_t s) {
+  void end(cudaStream_t s, double flops = 0.0, double bytes = 0.0) {
     if (!on) return;
     cudaEvent_t b;
     cudaEventCreate(&b);
     cudaEventRecord(b, s);
-    ev.push_back({cur, {start, b}});
+    ev.push_back({cur, start, b, flops, bytes});
   }
-  void report(int n) {
+  void report(bem_ctx* c, int n) {
     if (!on) return;
-    double t[5] = {0, 0, 0, 0, 0};
+    double t[5] = {0, 0, 0, 0, 0}, fl = 0, by = 0;
+    long long cnt = 0;
     for (auto& e : ev) {
       float ms = 0.f;
-      cudaEventSynchronize(e.second.second);
-      cudaEventElapsedTime(&ms, e.second.first, e.second.second);
-      t[e.first] += ms;
-      cudaEventDestroy(e.second.first);
-      cudaEventDestroy(e.second.second);
+      cudaEventSynchronize(e.b);
+      cudaEventElapsedTime(&ms, e.a, e.b);
+      t[e.phase] += ms;
+      if (e.phase == 4) {
+        ++cnt;
+        fl += e.flops;
+        by += e.bytes;
+      }
+      cudaEventDestroy(e.a);
+      cudaEventDestroy(e.b);
     }
-    fprintf(stderr, "[lu n=%d] panel %.1f ms  swaps %.1f ms  panel-update %.1f ms  trsm %.1f ms  trailing-gemm %.1f ms\n",
-            n, t[0], t[1], t[2], t[3], t[4]);
+    if (c->prof_timing) {
+      c->prof.lu_panel_ms += t[0];
+      c->prof.lu_swap_ms += t[1];
+      c->prof.lu_panel_update_ms += t[2];
+      c->prof.lu_trsm_ms += t[3];
+      c->prof.lu_trailing_ms += t[4];
+      c->prof.lu_trailing_launches += cnt;
+      c->prof.lu_trailing_flops += fl;
+      c->prof.lu_trailing_bytes += by;
+    }
+    if (getenv("BEM_LU_PROFILE"))
+      fprintf(stderr, "[lu n=%d] panel %.1f ms  swaps %.1f ms  panel-update %.1f ms  trsm %.1f ms  trailing-gemm %.1f ms\n",
+              n, t[0], t[1], t[2], t[3], t[4]);
   }
 };
 
@@ -466,7 +486,7 @@ int lu_factor(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int nb, int* info)
   cudaFuncSetAttribute(inv_unit_upper_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inv_smem);
   int rc;
   LUProfile prof;
-  prof.on = getenv("BEM_LU_PROFILE") != nullptr;
+  prof.on = getenv("BEM_LU_PROFILE") != nullptr || c->prof_timing;
   for (int j0 = 0; j0 < n; j0 += nb) {
     const int jb = std::min(nb, n - j0);
     for (int r0 = j0; r0 < j0 + jb; r0 += kPanelW) {
@@ -510,10 +530,10 @@ int lu_factor(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int nb, int* info)
       prof.begin(4, c->stream);
       if ((rc = gemm<T>(c, m, m, jb, Y, ldy, S + j0 + (int64_t)t0 * lda, lda, S + t0 + (int64_t)t0 * lda, lda, 0)))
         return rc;
-      prof.end(c->stream);
+      prof.end(c->stream, 2.0 * m * (double)m * jb, (2.0 * m * (double)m + 2.0 * m * (double)jb) * sizeof(T));
     }
   }
-  prof.report(n);
+  prof.report(c, n);
   int st[2];
   BEM_CUDA(c, cudaMemcpyAsync(st, ps.status.p, sizeof(st), cudaMemcpyDeviceToHost, c->stream));
   BEM_CUDA(c, cudaStreamSynchronize(c->stream));

@@ -46,7 +46,9 @@ typedef struct bem_ctx bem_ctx;
 
 /* Solve precision modes (bem_solve). */
 #define BEM_PREC_FP64 0      /* FP64 LU with partial pivoting: the DGESV replacement */
-#define BEM_PREC_FP32_IR 1   /* FP32 LU (FP32 CUDA-core trailing update) + FP64 refinement */
+#define BEM_PREC_FP32_IR 1   /* FP32 LU whose trailing update runs on the tensor cores as a
+                                three-term BF16 split (FP32-grade products, FP32
+                                accumulation) + FP64 iterative refinement */
 #define BEM_PREC_BF16_IR 2   /* scaled FP32 LU whose trailing update runs on the tensor
                                 cores with BF16 operands and FP32 accumulation,
                                 + FP64 refinement / GMRES-IR */
@@ -74,6 +76,8 @@ int bem_ctx_destroy(bem_ctx* ctx);
 const char* bem_last_error(const bem_ctx* ctx);
 /* sync the context's stream; returns a pending asynchronous error, if any */
 int bem_sync(bem_ctx* ctx);
+/* the context's CUDA stream (a cudaStream_t), for callers that time or order work */
+int bem_get_stream(bem_ctx* ctx, void** stream);
 
 /* Input: replaces input_data (io_mod.f90:36-146) and update_material_constants
  * (data_mod.f90:97-108).  Node -> element adjacency (io_mod.f90:125-135) is built here;
@@ -127,6 +131,25 @@ int bem_reorganize(bem_ctx* ctx, double* FI_out, double* DFI_out);
 int bem_internal_points(bem_ctx* ctx, int l, const double* cx, const double* cy,
                         const double* cz, double* u_int, double* sigma_int, double* prin,
                         double* vm, int flags);
+
+/* Profiling of the library's own kernels.  bem_profile_begin zeroes the counters;
+ * with timing != 0 the LU phases are bracketed by CUDA events on the context's stream
+ * (the stream every kernel of the context runs on).  bem_profile_end syncs the stream
+ * and reports.  Trailing flops/bytes are the algorithmic work of the trailing-update
+ * GEMMs: 2*m*m*nb flops and the C read+write plus one read of each operand. */
+typedef struct {
+  long long kernel_launches;    /* kernels this context launched */
+  double lu_panel_ms;           /* cooperative panel factorisation */
+  double lu_swap_ms;            /* row interchanges outside the panel */
+  double lu_panel_update_ms;    /* TRSM + GEMM inside the panel */
+  double lu_trsm_ms;            /* TRSM of the block row (inverse + GEMM) */
+  double lu_trailing_ms;        /* trailing-matrix GEMM */
+  long long lu_trailing_launches;
+  double lu_trailing_flops;
+  double lu_trailing_bytes;
+} bem_profile;
+int bem_profile_begin(bem_ctx* ctx, int timing);
+int bem_profile_end(bem_ctx* ctx, bem_profile* out);
 
 /* Device-resident variants for callers that keep data in HBM (the Python layer and
  * the benchmark).  Pointers are device addresses. */
