@@ -367,20 +367,11 @@ template int gemm<float>(bem_ctx*, int, int, int, const float*, int64_t, const f
 // ---------------------------------------------------------------------------------
 namespace {
 
-struct PanelScratch {
-  DBuf<double> cand_val;
-  DBuf<int> cand_idx;
-  DBuf<unsigned char> cand_col, diag_col;
-  DBuf<unsigned> barrier;
-  DBuf<int> status;
-  DBuf<unsigned char> inv, ybuf;
-};
-
 template <typename T>
-int panel_launch(bem_ctx* c, PanelScratch& ps, T* S, int64_t lda, int n, int r0, int w, int* piv) {
+int panel_launch(bem_ctx* c, const LUWorkspace& ws, T* S, int64_t lda, int n, int r0, int w, int* piv) {
   static int max_smem_set = 0;
   const int cols = n - r0;
-  int G = std::min(c->sm_count, std::max(1, (cols + 63) / 64));
+  int G = std::min(std::min(c->sm_count, ws.gmax), std::max(1, (cols + 63) / 64));
   int chunk = (cols + G - 1) / G;
   size_t smem = (size_t)chunk * kPitch * sizeof(T);
   if (smem > 200 * 1024) return bem_fail(c, BEM_ERR_ARG, "panel slice exceeds shared memory (matrix too large)");
@@ -392,15 +383,16 @@ int panel_launch(bem_ctx* c, PanelScratch& ps, T* S, int64_t lda, int n, int r0,
   int occ = 0;
   BEM_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, panel_kernel<T>, 256, smem));
   if (occ < 1) return bem_fail(c, BEM_ERR_CUDA, "panel kernel cannot be resident");
-  BEM_CUDA(c, cudaMemsetAsync(ps.barrier.p, 0, sizeof(unsigned), c->stream));
-  double* cv = ps.cand_val.p;
-  int* ci = ps.cand_idx.p;
-  T* cc = reinterpret_cast<T*>(ps.cand_col.p);
-  T* dc = reinterpret_cast<T*>(ps.diag_col.p);
-  unsigned* bar = ps.barrier.p;
-  int* st = ps.status.p;
+  BEM_CUDA(c, cudaMemsetAsync(ws.barrier, 0, sizeof(unsigned), c->stream));
+  double* cv = ws.cand_val;
+  int* ci = ws.cand_idx;
+  T* cc = reinterpret_cast<T*>(ws.cand_col);
+  T* dc = reinterpret_cast<T*>(ws.diag_col);
+  unsigned* bar = ws.barrier;
+  int* st = ws.status;
   void* args[] = {&S, &lda, &n, &r0, &w, &chunk, &piv, &cv, &ci, &cc, &dc, &bar, &st};
   BEM_CUDA(c, cudaLaunchCooperativeKernel((void*)panel_kernel<T>, dim3(G), dim3(256), args, smem, c->stream));
+  ++c->launches;
   return BEM_OK;
 }
 
@@ -464,23 +456,55 @@ struct LUProfile {
   }
 };
 
+static size_t up256(size_t b) { return (b + 255) / 256 * 256; }
+
+size_t lu_workspace_bytes(int n, int nb, int gmax, int elem) {
+  const size_t ldy = ((size_t)n + 31) / 32 * 32;
+  return up256(2 * (size_t)gmax * sizeof(double)) + up256(2 * (size_t)gmax * sizeof(int)) +
+         up256(2 * (size_t)gmax * kPanelW * elem) + up256(2 * (size_t)kPanelW * elem) + up256(16) +
+         up256((size_t)nb * nb * elem) + up256(ldy * nb * elem);
+}
+
+LUWorkspace lu_workspace_carve(void* base, int n, int nb, int gmax, int elem) {
+  unsigned char* p = static_cast<unsigned char*>(base);
+  LUWorkspace w{};
+  w.gmax = gmax;
+  w.ldy = ((int64_t)n + 31) / 32 * 32;
+  w.cand_val = reinterpret_cast<double*>(p);
+  p += up256(2 * (size_t)gmax * sizeof(double));
+  w.cand_idx = reinterpret_cast<int*>(p);
+  p += up256(2 * (size_t)gmax * sizeof(int));
+  w.cand_col = p;
+  p += up256(2 * (size_t)gmax * kPanelW * elem);
+  w.diag_col = p;
+  p += up256(2 * (size_t)kPanelW * elem);
+  w.barrier = reinterpret_cast<unsigned*>(p);
+  w.status = reinterpret_cast<int*>(p + 8);
+  p += up256(16);
+  w.inv = p;
+  p += up256((size_t)nb * nb * elem);
+  w.ybuf = p;
+  return w;
+}
+
+size_t lu_solve_work_count(int n) { return ((size_t)n + 127) / 128 * 256 + 256; }
+
 template <typename T>
 int lu_factor(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int nb, int* info) {
+  DBuf<unsigned char> scratch;
+  const int gmax = c->sm_count;
+  BEM_CUDA(c, scratch.alloc(lu_workspace_bytes(n, nb, gmax, sizeof(T))));
+  const LUWorkspace ws = lu_workspace_carve(scratch.p, n, nb, gmax, sizeof(T));
+  return lu_factor_ws<T>(c, S, lda, n, piv, nb, info, ws);
+}
+
+template <typename T>
+int lu_factor_ws(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int nb, int* info, const LUWorkspace& ws) {
   *info = 0;
-  PanelScratch ps;
-  const int Gmax = c->sm_count;
-  BEM_CUDA(c, ps.cand_val.alloc(2 * (size_t)Gmax));
-  BEM_CUDA(c, ps.cand_idx.alloc(2 * (size_t)Gmax));
-  BEM_CUDA(c, ps.cand_col.alloc(2 * (size_t)Gmax * kPanelW * sizeof(T)));
-  BEM_CUDA(c, ps.diag_col.alloc(2 * (size_t)kPanelW * sizeof(T)));
-  BEM_CUDA(c, ps.barrier.alloc(1));
-  BEM_CUDA(c, ps.status.alloc(2));
-  BEM_CUDA(c, ps.inv.alloc((size_t)nb * nb * sizeof(T)));
-  const int64_t ldy = ((int64_t)n + 31) / 32 * 32;
-  BEM_CUDA(c, ps.ybuf.alloc((size_t)ldy * nb * sizeof(T)));
-  BEM_CUDA(c, cudaMemsetAsync(ps.status.p, 0, 2 * sizeof(int), c->stream));
-  T* V = reinterpret_cast<T*>(ps.inv.p);
-  T* Y = reinterpret_cast<T*>(ps.ybuf.p);
+  BEM_CUDA(c, cudaMemsetAsync(ws.status, 0, 2 * sizeof(int), c->stream));
+  T* V = reinterpret_cast<T*>(ws.inv);
+  T* Y = reinterpret_cast<T*>(ws.ybuf);
+  const int64_t ldy = ws.ldy;
   const size_t inv_smem = (size_t)nb * nb * sizeof(T);
   if (inv_smem > 200 * 1024) return bem_fail(c, BEM_ERR_ARG, "block size too large for the inverse kernel");
   cudaFuncSetAttribute(inv_unit_upper_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inv_smem);
@@ -492,7 +516,7 @@ int lu_factor(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int nb, int* info)
     for (int r0 = j0; r0 < j0 + jb; r0 += kPanelW) {
       const int w = std::min(kPanelW, j0 + jb - r0);
       prof.begin(0, c->stream);
-      if ((rc = panel_launch<T>(c, ps, S, lda, n, r0, w, piv))) return rc;
+      if ((rc = panel_launch<T>(c, ws, S, lda, n, r0, w, piv))) return rc;
       prof.end(c->stream);
       prof.begin(1, c->stream);
       // swaps on the other rows of the panel and on the trailing rows
@@ -535,7 +559,7 @@ int lu_factor(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int nb, int* info)
   }
   prof.report(c, n);
   int st[2];
-  BEM_CUDA(c, cudaMemcpyAsync(st, ps.status.p, sizeof(st), cudaMemcpyDeviceToHost, c->stream));
+  BEM_CUDA(c, cudaMemcpyAsync(st, ws.status, sizeof(st), cudaMemcpyDeviceToHost, c->stream));
   BEM_CUDA(c, cudaStreamSynchronize(c->stream));
   if (st[0] != 0) return bem_fail(c, st[0], "panel grid barrier timed out");
   *info = st[1];
@@ -543,6 +567,8 @@ int lu_factor(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int nb, int* info)
 }
 
 template int lu_factor<double>(bem_ctx*, double*, int64_t, int, int*, int, int*);
+template int lu_factor_ws<double>(bem_ctx*, double*, int64_t, int, int*, int, int*, const LUWorkspace&);
+template int lu_factor_ws<float>(bem_ctx*, float*, int64_t, int, int*, int, int*, const LUWorkspace&);
 template int lu_factor<float>(bem_ctx*, float*, int64_t, int, int*, int, int*);
 
 // ---------------------------------------------------------------------------------
@@ -637,14 +663,12 @@ __global__ void bwd_finish_kernel(const T* S, int64_t lda, int n, int j0, int jb
 }
 
 template <typename T>
-int lu_solve(bem_ctx* c, const T* S, int64_t lda, int n, const int* piv, int nb, double* b) {
+int lu_solve_ws(bem_ctx* c, const T* S, int64_t lda, int n, const int* piv, int nb, double* b, double* work) {
   if (nb > 256) return bem_fail(c, BEM_ERR_ARG, "lu_solve: block size > 256");
   const size_t dsm = (size_t)nb * nb * sizeof(T);
   if (dsm > 200 * 1024) return bem_fail(c, BEM_ERR_ARG, "lu_solve: diagonal block exceeds shared memory");
   cudaFuncSetAttribute(fwd_diag_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm);
   cudaFuncSetAttribute(bwd_finish_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm);
-  const int maxblk = (n + 127) / 128 + 1;
-  if (c->work.count < (size_t)maxblk * 256) BEM_CUDA(c, c->work.alloc((size_t)maxblk * 256));
   for (int j0 = 0; j0 < n; j0 += nb) {
     const int jb = std::min(nb, n - j0);
     fwd_diag_kernel<T><<<1, 256, dsm, c->stream>>>(S, lda, j0, jb, b);
@@ -661,16 +685,27 @@ int lu_solve(bem_ctx* c, const T* S, int64_t lda, int n, const int* piv, int nb,
     const int c0 = j0 + jb;
     const int nblk = (n - c0 + 127) / 128;
     if (nblk > 0) {
-      bwd_dot_kernel<T><<<nblk, 256, 0, c->stream>>>(S, lda, n, j0, jb, c0, b, c->work.p);
+      bwd_dot_kernel<T><<<nblk, 256, 0, c->stream>>>(S, lda, n, j0, jb, c0, b, work);
       BEM_LAUNCH_CHECK(c);
     }
-    bwd_finish_kernel<T><<<1, 256, dsm, c->stream>>>(S, lda, n, j0, jb, nblk, c->work.p, piv, b);
+    bwd_finish_kernel<T><<<1, 256, dsm, c->stream>>>(S, lda, n, j0, jb, nblk, work, piv, b);
     BEM_LAUNCH_CHECK(c);
   }
   return BEM_OK;
 }
 
+template <typename T>
+int lu_solve(bem_ctx* c, const T* S, int64_t lda, int n, const int* piv, int nb, double* b) {
+  const size_t need = lu_solve_work_count(n);
+  if (c->work.count < need) {
+    c->work.release();
+    BEM_CUDA(c, c->work.alloc(need));
+  }
+  return lu_solve_ws<T>(c, S, lda, n, piv, nb, b, c->work.p);
+}
+
 template int lu_solve<double>(bem_ctx*, const double*, int64_t, int, const int*, int, double*);
+template int lu_solve_ws<double>(bem_ctx*, const double*, int64_t, int, const int*, int, double*, double*);
 template int lu_solve<float>(bem_ctx*, const float*, int64_t, int, const int*, int, double*);
 
 // ---------------------------------------------------------------------------------

@@ -21,20 +21,34 @@ namespace bem {
 
 constexpr int kPanelW = 32;  // columns of T factored by one cooperative panel launch
 
-struct LUScratch {
-  // cooperative panel kernel
-  double* cand_val;   // [2][grid]
-  int* cand_idx;      // [2][grid]
-  void* cand_col;     // [2][grid][kPanelW] of T
+// Device scratch of one factorisation: the cooperative panel kernel's candidate
+// exchange (double-buffered per-CTA candidates, the diagonal column, the grid-barrier
+// counter and the status words) and the TRSM-by-inverse buffers.  lu_factor()
+// allocates it per call; lu_factor_ws() takes it from the caller.
+struct LUWorkspace {
+  double* cand_val;   // [2][gmax]
+  int* cand_idx;      // [2][gmax]
+  void* cand_col;     // [2][gmax][kPanelW] of T
   void* diag_col;     // [2][kPanelW] of T
-  unsigned* barrier;  // grid barrier counter
-  int* status;        // [0] error code, [1] info
-  // TRSM by inverse
-  void* inv;          // NB x NB
-  void* ybuf;         // n x NB
-  // solve
-  double* partial;    // GEMV / dot partial sums
+  unsigned* barrier;  // grid-barrier counter (zeroed before every panel launch)
+  int* status;        // [0] error code, [1] info (zeroed at the start of a factorisation)
+  void* inv;          // nb x nb of T
+  void* ybuf;         // ldy x nb of T
+  int64_t ldy;
+  int gmax;           // most CTAs a panel launch may use
 };
+
+// bytes of an LUWorkspace for order n (rounded up per region to 256 bytes); carve()
+// lays the regions out from base in that order
+size_t lu_workspace_bytes(int n, int nb, int gmax, int elem);
+LUWorkspace lu_workspace_carve(void* base, int n, int nb, int gmax, int elem);
+// doubles of triangular-solve scratch for order n
+size_t lu_solve_work_count(int n);
+
+template <typename T>
+int lu_factor_ws(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int nb, int* info, const LUWorkspace& ws);
+template <typename T>
+int lu_solve_ws(bem_ctx* c, const T* S, int64_t lda, int n, const int* piv, int nb, double* b, double* work);
 
 template <typename T>
 int lu_factor(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int nb, int* info);
