@@ -21,6 +21,8 @@ BEM_ERR_TIMEOUT = -4
 BEM_ERR_STATE = -5
 BEM_ERR_MESH = -6
 BEM_ERR_NOCONV = -7
+BEM_ERR_TOO_LARGE = -8
+NOALLOC_MAX_N = 4096
 
 BEM_PREC_FP64 = 0
 BEM_PREC_FP32_IR = 1
@@ -37,6 +39,7 @@ EXPORTS = [
     "bem_get_geometry", "bem_ghmat8", "bem_get_hg", "bem_solve", "bem_dgesv",
     "bem_reorganize", "bem_internal_points", "bem_device_state",
     "bem_internal_points_device", "bem_profile_begin", "bem_profile_end",
+    "bem_dgesv_noalloc",
 ]
 
 
@@ -110,6 +113,7 @@ def load(build_if_needed: bool = True):
     L.bem_get_hg.argtypes = [_vp, C.c_int, C.c_int, _vp, C.c_int64, _vp, C.c_int64]
     L.bem_solve.argtypes = [_vp, C.c_int, C.c_double, C.c_int, _vp, _ip, C.POINTER(SolveInfo)]
     L.bem_dgesv.argtypes = [_vp, C.c_int, C.c_int, _vp, C.c_int, _vp, _vp, C.c_int, _ip]
+    L.bem_dgesv_noalloc.argtypes = [C.c_int, C.c_int, _vp, C.c_int, _vp, _vp, C.c_int, _ip, _vp]
     L.bem_reorganize.argtypes = [_vp, _vp, _vp]
     L.bem_internal_points.argtypes = [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int]
     L.bem_device_state.argtypes = [_vp, C.POINTER(C.c_void_p), C.POINTER(C.c_int64),

@@ -43,6 +43,7 @@ typedef struct bem_ctx bem_ctx;
 #define BEM_ERR_STATE (-5)    /* called out of order (e.g. solve before ghmat8) */
 #define BEM_ERR_MESH (-6)     /* a node lies in more than 8 elements, bad connectivity */
 #define BEM_ERR_NOCONV (-7)   /* refinement did not reach the requested tolerance */
+#define BEM_ERR_TOO_LARGE (-8) /* order above the limit of bem_dgesv_noalloc (4096) */
 
 /* Solve precision modes (bem_solve). */
 #define BEM_PREC_FP64 0      /* FP64 LU with partial pivoting: the DGESV replacement */
@@ -121,6 +122,21 @@ int bem_solve(bem_ctx* ctx, int precision, double rel_tol, int max_iter, double*
  * header of lu.cu).  Runs on the context's device. */
 int bem_dgesv(bem_ctx* ctx, int n, int nrhs, double* A, int lda, int* ipiv, double* B,
               int ldb, int* info);
+
+/* No counterpart in the reference.  The dgesv solve on caller-owned DEVICE buffers
+ * that performs no device allocation, for callers that cannot allocate at the point
+ * of the solve (a host that owns all device memory through its own pool, a loop that
+ * must not pay for cudaMalloc/cudaFree synchronisation, a fixed memory budget).  Its
+ * scratch is one static 4.5 MiB device array per GPU, which limits n to 4096
+ * (larger n returns BEM_ERR_TOO_LARGE).  dA (n x n, lda) is overwritten by the factors,
+ * dB (n x nrhs, ldb) by the solution, d_ipiv (n ints) by the 1-based pivots; *info
+ * (host) follows DGESV.  Work is queued on `stream` (a cudaStream_t, 0 = legacy
+ * default stream); the call returns after the factorisation's status is known, the
+ * solution is complete once the stream has been synchronised.  The first call on a
+ * device sets up the array's device address: make it before any stream capture.  All
+ * calls share the array: calls that overlap on the GPU race and must be serialised. */
+int bem_dgesv_noalloc(int n, int nrhs, double* dA, int lda, int* d_ipiv, double* dB, int ldb,
+                      int* info, void* stream);
 
 /* reorganize_solution (io_mod.f90:148-183): FI -> nodal displacements u (3n),
  * DFI (27, ne) element-nodal tractions.  Host outputs nullable. */
