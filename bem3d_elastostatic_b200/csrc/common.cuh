@@ -131,10 +131,14 @@ struct bem_ctx {
   bem::DBuf<int> status;
   bem::DBuf<double> rowscale, colscale;
   // GEMM flavour of the LU trailing update: f64_gemm 1 = DMMA tensor path, 0 = SIMT;
-  // f32_gemm 3 = BF16 x3 split, 1 = plain BF16 (tensor cores), 0 = SIMT FP32
+  // f32_gemm 4 = BF16 x3 split on tcgen05 for the trailing update (mma.sync elsewhere),
+  // 3 = BF16 x3 split on mma.sync, 1 = plain BF16 (mma.sync), 0 = SIMT FP32
   int f64_gemm = 1;
-  int f32_gemm = 3;
+  int f32_gemm = 4;
   int f32_gemm_override = -1;  // BEM_F32_GEMM environment override (0, 1, 3)
+  // tcgen05 trailing update: BF16 hi/lo operand copies and its error word
+  bem::DBuf<unsigned char> umma_buf;
+  bem::DBuf<int> umma_err;
   // profiling (bem_profile_begin/end)
   long long launches = 0;
   int prof_timing = 0;

@@ -325,6 +325,9 @@ int gemm_dmma(bem_ctx* c, int M, int N, int K, const double* A, int64_t lda, con
 int gemm_bf16(bem_ctx* c, int M, int N, int K, const float* A, int64_t lda, const float* B, int64_t ldb, float* C,
               int64_t ldc, int mode, int split);
 bool gemm_tc_ok(const void* A, int64_t lda, const void* B, int64_t ldb, int elem);
+bool umma_supported(int K);
+int gemm_umma_bf16x3(bem_ctx* c, int M, int N, int K, const float* A, int64_t lda, const float* B, int64_t ldb,
+                     float* C, int64_t ldc);
 
 template <typename T>
 static int gemm_simt(bem_ctx* c, int M, int N, int K, const T* A, int64_t lda, const T* B, int64_t ldb, T* C,
@@ -351,8 +354,11 @@ int gemm(bem_ctx* c, int M, int N, int K, const T* A, int64_t lda, const T* B, i
     if (tc && c->f64_gemm == 1)
       return gemm_dmma(c, M, N, K, (const double*)A, lda, (const double*)B, ldb, (double*)C, ldc, mode);
   } else {
-    if (tc && (c->f32_gemm == 1 || c->f32_gemm == 3))
-      return gemm_bf16(c, M, N, K, (const float*)A, lda, (const float*)B, ldb, (float*)C, ldc, mode, c->f32_gemm);
+    if (c->f32_gemm == 4 && mode == 0 && umma_supported(K) && M >= 128 && N >= 256)
+      return gemm_umma_bf16x3(c, M, N, K, (const float*)A, lda, (const float*)B, ldb, (float*)C, ldc);
+    if (tc && (c->f32_gemm == 1 || c->f32_gemm == 3 || c->f32_gemm == 4))
+      return gemm_bf16(c, M, N, K, (const float*)A, lda, (const float*)B, ldb, (float*)C, ldc, mode,
+                       c->f32_gemm == 1 ? 1 : 3);
   }
   return gemm_simt<T>(c, M, N, K, A, lda, B, ldb, C, ldc, mode);
 }
@@ -502,6 +508,10 @@ template <typename T>
 int lu_factor_ws(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int nb, int* info, const LUWorkspace& ws) {
   *info = 0;
   BEM_CUDA(c, cudaMemsetAsync(ws.status, 0, 2 * sizeof(int), c->stream));
+  if (sizeof(T) == 4 && c->f32_gemm == 4) {
+    if (c->umma_err.count < 1) BEM_CUDA(c, c->umma_err.alloc(1));
+    BEM_CUDA(c, cudaMemsetAsync(c->umma_err.p, 0, sizeof(int), c->stream));
+  }
   T* V = reinterpret_cast<T*>(ws.inv);
   T* Y = reinterpret_cast<T*>(ws.ybuf);
   const int64_t ldy = ws.ldy;
@@ -562,6 +572,11 @@ int lu_factor_ws(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int nb, int* in
   BEM_CUDA(c, cudaMemcpyAsync(st, ws.status, sizeof(st), cudaMemcpyDeviceToHost, c->stream));
   BEM_CUDA(c, cudaStreamSynchronize(c->stream));
   if (st[0] != 0) return bem_fail(c, st[0], "panel grid barrier timed out");
+  if (sizeof(T) == 4 && c->f32_gemm == 4) {
+    int ue = 0;
+    BEM_CUDA(c, cudaMemcpy(&ue, c->umma_err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (ue != 0) return bem_fail(c, ue, "tcgen05 trailing update: an mbarrier wait timed out");
+  }
   *info = st[1];
   return BEM_OK;
 }

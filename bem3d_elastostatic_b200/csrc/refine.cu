@@ -55,7 +55,7 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
   if (c->f32_gemm_override >= 0)
     c->f32_gemm = c->f32_gemm_override;
   else
-    c->f32_gemm = (precision == BEM_PREC_BF16_IR) ? 1 : 3;
+    c->f32_gemm = (precision == BEM_PREC_BF16_IR) ? 1 : 4;
   int rc = lu_factor<float>(c, c->A32.p, lda, n, c->piv.p, kNbMixed, info);
   c->f32_gemm = saved;
   if (rc) return rc;

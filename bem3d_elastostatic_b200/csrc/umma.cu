@@ -1,0 +1,299 @@
+// Trailing update of the FP32 LU on the 5th-generation tensor cores (tcgen05).
+//
+//   C (m x n, FP32, column-major, ldc) -= A (m x K) * B (K x n),  K = the panel width
+//
+// FP32 operands are split once per call into BF16 hi + lo parts (split_a_kernel /
+// split_b_kernel), stored K-major so the Tensor Memory Accelerator can bring 64-wide
+// K chunks into 128-byte-swizzled shared memory.  One thread issues, per K chunk and
+// per 16-wide K step, the three products hi*hi + hi*lo + lo*hi as tcgen05.mma
+// (kind::f16, BF16 inputs, FP32 accumulation in tensor memory, M = 128, N = 256); a
+// tcgen05.commit signals an mbarrier when they are done, and four warps drain the
+// 128 x 256 accumulator with tcgen05.ld (one TMEM lane = one row of C) into a
+// coalesced read-modify-write of C.
+//
+// Every mbarrier wait is bounded: on timeout the kernel records an error word, skips
+// the rest of its work, waits (bounded) for its own copies and frees its tensor memory.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cudaTypedefs.h>
+
+#include "lu.cuh"
+
+namespace bem {
+
+namespace {
+
+constexpr int UM = 128;                 // tile rows (UMMA M)
+constexpr int UN = 256;                 // tile columns (UMMA N)
+constexpr int UK = 64;                  // K chunk per TMA box (128 bytes of BF16)
+constexpr int kMaxK = 128;              // K handled without a ring (2 chunks resident)
+constexpr int kChunks = kMaxK / UK;
+constexpr int A_TILE = UM * UK * 2;     // 16 KB
+constexpr int B_TILE = UN * UK * 2;     // 32 KB
+constexpr int STAGE = 2 * A_TILE + 2 * B_TILE;  // hi + lo of A and B: 96 KB
+constexpr int kSmem = kChunks * STAGE + 1024 + 256;
+constexpr unsigned kTmemCols = 256;
+constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s bound on every mbarrier wait
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ unsigned long long globaltimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
+  const unsigned long long t0 = globaltimer();
+  while (true) {
+    unsigned done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (globaltimer() - t0 > kWaitNs) return false;
+  }
+}
+
+__device__ __forceinline__ uint64_t sw128_desc(unsigned saddr) {
+  // K-major, 128-byte swizzle: SBO = 1024 B between 8-row groups, LBO = 16 B,
+  // descriptor version 1, layout type 2
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | (1ull << 16) | (64ull << 32) | (1ull << 46) | (2ull << 61);
+}
+
+__global__ void __launch_bounds__(128, 1)
+    umma_update_kernel(const __grid_constant__ CUtensorMap tAh, const __grid_constant__ CUtensorMap tAl,
+                       const __grid_constant__ CUtensorMap tBh, const __grid_constant__ CUtensorMap tBl, int M,
+                       int N, int K, float* C, int64_t ldc, int* err) {
+  extern __shared__ __align__(16) unsigned char umma_smem[];
+  const unsigned raw = smem_u32(umma_smem);
+  const unsigned base = (raw + 1023u) & ~1023u;  // 1024-byte aligned operand tiles
+  unsigned char* gbase = umma_smem + (base - raw);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(gbase + kChunks * STAGE);  // full[kChunks], done
+  unsigned* tmem_slot = reinterpret_cast<unsigned*>(gbase + kChunks * STAGE + 128);
+  __shared__ int s_fail;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m0 = blockIdx.x * UM, n0 = blockIdx.y * UN;
+  const int nchunk = (K + UK - 1) / UK;
+
+  if (threadIdx.x == 0) {
+    s_fail = 0;
+    for (int c = 0; c <= kChunks; ++c)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&bars[c])), "r"(1) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const unsigned tmem = *tmem_slot;
+
+  if (threadIdx.x == 0) {
+    // producer: every K chunk of A (hi, lo) and B (hi, lo) at once
+    for (int c = 0; c < nchunk; ++c) {
+      const unsigned st = base + c * STAGE;
+      const unsigned bar = smem_u32(&bars[c]);
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"((unsigned)STAGE)
+                   : "memory");
+      const int kx = c * UK;
+      const CUtensorMap* maps[4] = {&tAh, &tAl, &tBh, &tBl};
+      const unsigned dst[4] = {st, st + A_TILE, st + 2 * A_TILE, st + 2 * A_TILE + B_TILE};
+      const int row[4] = {m0, m0, n0, n0};
+      for (int t = 0; t < 4; ++t)
+        asm volatile(
+            "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+            "[%4];" ::"r"(dst[t]),
+            "l"(reinterpret_cast<uint64_t>(maps[t])), "r"(kx), "r"(row[t]), "r"(bar)
+            : "memory");
+    }
+    // MMA issue: D (TMEM) = sum over chunks, K steps and the three split products
+    // instruction descriptor: F32 accumulate, BF16 A and B, K-major both, N = 256, M = 128
+    const unsigned idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(UN >> 3) << 17) | ((unsigned)(UM >> 4) << 24);
+    int acc = 0;
+    bool ok = true;
+    for (int c = 0; c < nchunk && ok; ++c) {
+      if (!mbar_wait(smem_u32(&bars[c]), 0)) {
+        ok = false;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const unsigned st = base + c * STAGE;
+      const unsigned ah = st, al = st + A_TILE, bh = st + 2 * A_TILE, bl = st + 2 * A_TILE + B_TILE;
+      for (int kk = 0; kk < UK / 16; ++kk) {
+        const unsigned off = kk * 32;  // 16 BF16 = 32 bytes along K inside the swizzle atom
+        const uint64_t a_h = sw128_desc(ah + off), a_l = sw128_desc(al + off);
+        const uint64_t b_h = sw128_desc(bh + off), b_l = sw128_desc(bl + off);
+        const uint64_t pa[3] = {a_h, a_h, a_l}, pb[3] = {b_h, b_l, b_h};
+        for (int t = 0; t < 3; ++t) {
+          asm volatile(
+              "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+              "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+              "l"(pa[t]), "l"(pb[t]), "r"(idesc), "r"(acc)
+              : "memory");
+          acc = 1;
+        }
+      }
+    }
+    if (ok) {
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                       smem_u32(&bars[kChunks]))
+                   : "memory");
+    } else {
+      s_fail = 1;
+      atomicCAS(err, 0, BEM_ERR_TIMEOUT);
+      // let this CTA's own copies land (bounded) before the shared memory is released
+      for (int c = 0; c < nchunk; ++c) mbar_wait(smem_u32(&bars[c]), 0);
+    }
+  }
+  __syncwarp();
+  // epilogue: wait for the MMAs, then 32 columns at a time TMEM -> registers -> C
+  bool ok = true;
+  if (!s_fail) ok = mbar_wait(smem_u32(&bars[kChunks]), 0);
+  __syncthreads();
+  if (!ok || s_fail) {
+    if (threadIdx.x == 0) atomicCAS(err, 0, BEM_ERR_TIMEOUT);
+  } else {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const int row = m0 + warp * 32 + lane;
+    for (int j0 = 0; j0 < UN; j0 += 32) {
+      unsigned r[32];
+      const unsigned taddr = tmem + ((unsigned)(warp * 32) << 16) + (unsigned)j0;
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+          "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+            "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]),
+            "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]),
+            "=r"(r[30]), "=r"(r[31])
+          : "r"(taddr)
+          : "memory");
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (row < M) {
+        float old[32];
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+          const int col = n0 + j0 + j;
+          old[j] = (col < N) ? C[row + (int64_t)col * ldc] : 0.f;
+        }
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+          const int col = n0 + j0 + j;
+          if (col < N) C[row + (int64_t)col * ldc] = old[j] - __uint_as_float(r[j]);
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+  }
+}
+
+// A (m x K, FP32, column-major lda) -> hi/lo BF16 [m][K] (K contiguous)
+__global__ void split_a_kernel(int m, int K, const float* __restrict__ A, int64_t lda, __nv_bfloat16* hi,
+                               __nv_bfloat16* lo) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int groups = K / 8;
+  if (t >= (int64_t)m * groups) return;
+  const int r = (int)(t % m), g = (int)(t / m);
+  __align__(16) __nv_bfloat16 h[8], l[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const float v = A[r + (int64_t)(8 * g + q) * lda];
+    h[q] = __float2bfloat16_rn(v);
+    l[q] = __float2bfloat16_rn(v - __bfloat162float(h[q]));
+  }
+  *reinterpret_cast<uint4*>(hi + (int64_t)r * K + 8 * g) = *reinterpret_cast<uint4*>(h);
+  *reinterpret_cast<uint4*>(lo + (int64_t)r * K + 8 * g) = *reinterpret_cast<uint4*>(l);
+}
+
+// B (K x n, FP32, column-major ldb) -> hi/lo BF16 [n][K]
+__global__ void split_b_kernel(int n, int K, const float* __restrict__ B, int64_t ldb, __nv_bfloat16* hi,
+                               __nv_bfloat16* lo) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int groups = K / 8;
+  if (t >= (int64_t)n * groups) return;
+  const int g = (int)(t % groups), col = (int)(t / groups);
+  __align__(16) __nv_bfloat16 h[8], l[8];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const float v = B[8 * g + q + (int64_t)col * ldb];
+    h[q] = __float2bfloat16_rn(v);
+    l[q] = __float2bfloat16_rn(v - __bfloat162float(h[q]));
+  }
+  *reinterpret_cast<uint4*>(hi + (int64_t)col * K + 8 * g) = *reinterpret_cast<uint4*>(h);
+  *reinterpret_cast<uint4*>(lo + (int64_t)col * K + 8 * g) = *reinterpret_cast<uint4*>(l);
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+
+bool make_map(CUtensorMap* map, const void* ptr, int rows, int K, int box_rows) {
+  cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)K * 2};
+  cuuint32_t box[2] = {(cuuint32_t)UK, (cuuint32_t)box_rows};
+  cuuint32_t estr[2] = {1, 1};
+  return g_encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+}  // namespace
+
+bool umma_supported(int K) { return K > 0 && K <= kMaxK && K % UK == 0; }
+
+// C (M x N) -= A (M x K) * B (K x N) on tcgen05 with the three-term BF16 split.
+int gemm_umma_bf16x3(bem_ctx* c, int M, int N, int K, const float* A, int64_t lda, const float* B, int64_t ldb,
+                     float* C, int64_t ldc) {
+  if (!umma_supported(K)) return bem_fail(c, BEM_ERR_ARG, "umma: K must be a multiple of 64 up to 128");
+  if (!g_encode) {
+    cudaDriverEntryPointQueryResult q;
+    void* fn = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess || !fn)
+      return bem_fail(c, BEM_ERR_CUDA, "cuTensorMapEncodeTiled not available");
+    g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    cudaFuncSetAttribute(umma_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem);
+  }
+  const size_t na = (size_t)M * K, nb_ = (size_t)N * K;
+  const size_t need = 2 * (na + nb_) * sizeof(__nv_bfloat16) + 256;
+  if (c->umma_buf.count < need) {
+    c->umma_buf.release();
+    BEM_CUDA(c, c->umma_buf.alloc(need));
+  }
+  if (c->umma_err.count < 1) BEM_CUDA(c, c->umma_err.alloc(1));
+  __nv_bfloat16* ah = reinterpret_cast<__nv_bfloat16*>(c->umma_buf.p);
+  __nv_bfloat16* al = ah + na;
+  __nv_bfloat16* bh = al + na;
+  __nv_bfloat16* bl = bh + nb_;
+  const int64_t ta = (int64_t)M * (K / 8), tb = (int64_t)N * (K / 8);
+  split_a_kernel<<<(unsigned)((ta + 255) / 256), 256, 0, c->stream>>>(M, K, A, lda, ah, al);
+  BEM_LAUNCH_CHECK(c);
+  split_b_kernel<<<(unsigned)((tb + 255) / 256), 256, 0, c->stream>>>(N, K, B, ldb, bh, bl);
+  BEM_LAUNCH_CHECK(c);
+  CUtensorMap mAh, mAl, mBh, mBl;
+  if (!make_map(&mAh, ah, M, K, UM) || !make_map(&mAl, al, M, K, UM) || !make_map(&mBh, bh, N, K, UN) ||
+      !make_map(&mBl, bl, N, K, UN))
+    return bem_fail(c, BEM_ERR_CUDA, "umma: tensor map encoding failed");
+  dim3 grid((M + UM - 1) / UM, (N + UN - 1) / UN);
+  if (grid.y > 65535) return bem_fail(c, BEM_ERR_ARG, "umma: N too large");
+  umma_update_kernel<<<grid, 128, kSmem, c->stream>>>(mAh, mAl, mBh, mBl, M, N, K, C, ldc, c->umma_err.p);
+  BEM_LAUNCH_CHECK(c);
+  return BEM_OK;
+}
+
+}  // namespace bem
