@@ -26,6 +26,9 @@
 namespace bem {
 
 constexpr int kPitch = kPanelW + 1;  // shared-memory column pitch (conflict-free)
+constexpr int kInvBlock = 128;       // unit-triangle inverse block of the block-row TRSM
+constexpr int kSolveBlock = 128;     // diagonal block of the triangular solves
+constexpr int kPanelSmemMax = 200 * 1024;
 constexpr long long kSpinLimit = 1ll << 24;
 
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
@@ -42,10 +45,34 @@ __device__ __forceinline__ void better(double& bv, int& bc, int& bg, double v, i
   }
 }
 
+// Copies the rows x cols block at src (column-major, lda) into shared memory dst
+// (column-major, leading dimension ldd), zero outside [0,rows) x [0,cols) up to
+// (full_rows x full_cols) and outside the mask; 16 loads per thread are issued before
+// their shared stores so a block costs a few memory round trips, not one per element.
+template <typename T, typename Mask>
+__device__ __forceinline__ void stage_block(T* dst, int ldd, const T* src, int64_t lda, int rows, int cols,
+                                            int full_rows, int full_cols, Mask mask) {
+  const int total = full_rows * full_cols;
+  for (int base = 0; base < total; base += 16 * blockDim.x) {
+    T v[16];
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+      const int idx = base + u * blockDim.x + threadIdx.x;
+      const int r = idx % full_rows, cc = idx / full_rows;
+      v[u] = (idx < total && r < rows && cc < cols && mask(r, cc)) ? src[r + (int64_t)cc * lda] : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+      const int idx = base + u * blockDim.x + threadIdx.x;
+      if (idx < total) dst[(idx % full_rows) + (idx / full_rows) * ldd] = v[u];
+    }
+  }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256, 1)
     panel_kernel(T* S, int64_t lda, int n, int r0, int w, int chunk, int* piv, double* cand_val,
-                 int* cand_idx, T* cand_col, T* diag_col, unsigned* barrier, int* status) {
+                 int* cand_idx, T* cand_col, T* diag_col, unsigned* barrier, unsigned bar_base, int* status) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* col = reinterpret_cast<T*>(smem_raw);  // [chunk][kPitch]
   __shared__ T pvt[kPanelW];
@@ -57,10 +84,8 @@ __global__ void __launch_bounds__(256, 1)
   const int c_end = min(n, c_beg + chunk);
   const int ncols = max(0, c_end - c_beg);
 
-  for (int idx = tid; idx < ncols * kPanelW; idx += blockDim.x) {
-    const int cc = idx / kPanelW, j = idx % kPanelW;
-    col[cc * kPitch + j] = (j < w) ? S[(int64_t)(c_beg + cc) * lda + r0 + j] : T(0);
-  }
+  stage_block<T>(col, kPitch, S + r0 + (int64_t)c_beg * lda, lda, w, ncols, kPanelW, ncols,
+                 [](int, int) { return true; });
   __syncthreads();
 
   for (int t = 0; t < w; ++t) {
@@ -102,7 +127,7 @@ __global__ void __launch_bounds__(256, 1)
     // 2. grid barrier (bounded)
     if (tid == 0) {
       atomicAdd(barrier, 1u);
-      const unsigned target = (unsigned)(t + 1) * (unsigned)G;
+      const unsigned target = bar_base + (unsigned)(t + 1) * (unsigned)G;
       long long spins = 0;
       int abort = 0;
       while (ld_acquire_u32(barrier) < target) {
@@ -193,12 +218,11 @@ __global__ void swap_rows_kernel(T* S, int64_t lda, const int* piv, int k0, int 
 // upper triangle of S(k0..k0+w, k0..k0+w).
 template <typename T>
 __global__ void trsm_small_kernel(T* S, int64_t lda, int k0, int w, int r_lo, int r_hi) {
-  __shared__ T U[kPanelW][kPanelW + 1];
-  for (int idx = threadIdx.x; idx < kPanelW * kPanelW; idx += blockDim.x) {
-    const int a = idx % kPanelW, b = idx / kPanelW;
-    U[a][b] = (a < w && b < w) ? S[(k0 + a) + (int64_t)(k0 + b) * lda] : T(0);
-  }
+  __shared__ T Ucm[kPanelW * (kPanelW + 1)];  // column-major, leading dimension kPanelW + 1
+  stage_block<T>(Ucm, kPanelW + 1, S + k0 + (int64_t)k0 * lda, lda, w, w, kPanelW, kPanelW,
+                 [](int, int) { return true; });
   __syncthreads();
+  auto U = [&](int a, int b) { return Ucm[a + b * (kPanelW + 1)]; };
   const int r = r_lo + blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= r_hi) return;
   T y[kPanelW];
@@ -207,33 +231,75 @@ __global__ void trsm_small_kernel(T* S, int64_t lda, int k0, int w, int r_lo, in
     if (b < w) {
       T v = S[r + (int64_t)(k0 + b) * lda];
 #pragma unroll
-      for (int a = 0; a < b; ++a) v -= y[a] * U[a][b];
+      for (int a = 0; a < b; ++a) v -= y[a] * U(a, b);
       y[b] = v;
       S[r + (int64_t)(k0 + b) * lda] = v;
     }
   }
 }
 
-// V = U^{-1} for the unit upper triangle U of S11 (jb x jb); V column-major (ldv).
+// V = U^{-1} for the unit upper triangle U of S11 (jb x jb, jb <= 128); V column-major
+// (ldv).  Blocked by 32: four warps invert the diagonal blocks (lane j holds column j
+// of its block in registers and back-substitutes), then the off-diagonal blocks follow
+// in order of their distance from the diagonal,
+//   V_ij = -V_ii * sum_{k=i+1..j} U_ik V_kj,
+// each a 32 x 32 product spread over all 256 threads.  U is staged in shared memory,
+// V is written to (and re-read from) global memory by this CTA only.
 template <typename T>
-__global__ void inv_unit_upper_kernel(const T* S11, int64_t lda, int jb, T* V, int ldv) {
+__global__ void __launch_bounds__(256) inv_unit_upper_kernel(const T* S11, int64_t lda, int jb, T* V, int ldv) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* U = reinterpret_cast<T*>(smem_raw);  // [jb][jb] column-major
-  for (int idx = threadIdx.x; idx < jb * jb; idx += blockDim.x) {
-    const int a = idx % jb, b = idx / jb;
-    U[idx] = (a < b) ? S11[a + (int64_t)b * lda] : T(0);
+  T* U = reinterpret_cast<T*>(smem_raw);  // [128][128] column-major, zero outside the strict upper part
+  __shared__ T tmp[32 * 33];
+  constexpr int B = 32, NB = 128;
+  stage_block<T>(U, NB, S11, lda, jb, jb, NB, NB, [](int a, int b) { return a < b; });
+  __syncthreads();
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nblk = (jb + B - 1) / B;
+  // diagonal blocks
+  if (warp < nblk) {
+    const int o = warp * B;
+    T x[B];
+#pragma unroll
+    for (int i = 0; i < B; ++i) x[i] = (i == lane) ? T(1) : T(0);
+#pragma unroll
+    for (int i = B - 2; i >= 0; --i) {
+      T sacc = x[i];
+#pragma unroll
+      for (int k = i + 1; k < B; ++k) sacc -= U[(o + i) + (o + k) * NB] * x[k];
+      x[i] = (i < lane) ? sacc : x[i];
+    }
+#pragma unroll
+    for (int i = 0; i < B; ++i)
+      if (o + i < jb && o + lane < jb) V[(o + i) + (int64_t)(o + lane) * ldv] = x[i];
+  }
+  // zero the strict lower blocks of V
+  for (int idx = tid; idx < jb * jb; idx += blockDim.x) {
+    const int r = idx % jb, cc = idx / jb;
+    if (r / B > cc / B) V[r + (int64_t)cc * ldv] = T(0);
   }
   __syncthreads();
-  const int j = threadIdx.x;
-  if (j >= jb) return;
-  T* v = V + (int64_t)j * ldv;
-  for (int i = jb - 1; i > j; --i) v[i] = T(0);
-  v[j] = T(1);
-  for (int i = j - 1; i >= 0; --i) {
-    T s = T(0);
-    for (int k = i + 1; k <= j; ++k) s += U[i + k * jb] * v[k];
-    v[i] = -s;
-  }
+  for (int d = 1; d < nblk; ++d)
+    for (int bi = 0; bi + d < nblk; ++bi) {
+      const int bj = bi + d;
+      const int oi = bi * B, oj = bj * B;
+      // tmp = sum_{k=bi+1..bj} U_{bi,k} V_{k,bj}   (32 x 32)
+      for (int e = tid; e < B * B; e += blockDim.x) {
+        const int r = e % B, cc = e / B;
+        T acc = T(0);
+        for (int k = oi + B; k <= oj + B - 1 && k < jb; ++k) acc += U[(oi + r) + k * NB] * V[k + (int64_t)(oj + cc) * ldv];
+        tmp[r + cc * 33] = acc;
+      }
+      __syncthreads();
+      // V_{bi,bj} = -V_{bi,bi} tmp
+      for (int e = tid; e < B * B; e += blockDim.x) {
+        const int r = e % B, cc = e / B;
+        T acc = T(0);
+#pragma unroll 8
+        for (int k = 0; k < B; ++k) acc += V[(oi + r) + (int64_t)(oi + k) * ldv] * tmp[k + cc * 33];
+        if (oi + r < jb && oj + cc < jb) V[(oi + r) + (int64_t)(oj + cc) * ldv] = -acc;
+      }
+      __syncthreads();
+    }
 }
 
 // ---------------------------------------------------------------------------------
@@ -373,32 +439,37 @@ template int gemm<float>(bem_ctx*, int, int, int, const float*, int64_t, const f
 // ---------------------------------------------------------------------------------
 namespace {
 
+// The barrier counter grows monotonically over a factorisation (zeroed once with the
+// status words); each launch waits for its own arrivals on top of bar_base.
 template <typename T>
-int panel_launch(bem_ctx* c, const LUWorkspace& ws, T* S, int64_t lda, int n, int r0, int w, int* piv) {
-  static int max_smem_set = 0;
+int panel_launch(bem_ctx* c, const LUWorkspace& ws, T* S, int64_t lda, int n, int r0, int w, int* piv,
+                 unsigned& bar_base) {
+  static int checked = 0;  // bit 0: double, bit 1: float
   const int cols = n - r0;
   int G = std::min(std::min(c->sm_count, ws.gmax), std::max(1, (cols + 63) / 64));
   int chunk = (cols + G - 1) / G;
   size_t smem = (size_t)chunk * kPitch * sizeof(T);
-  if (smem > 200 * 1024) return bem_fail(c, BEM_ERR_ARG, "panel slice exceeds shared memory (matrix too large)");
-  if (!max_smem_set) {
-    cudaFuncSetAttribute(panel_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(panel_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    max_smem_set = 1;
+  if (smem > kPanelSmemMax) return bem_fail(c, BEM_ERR_ARG, "panel slice exceeds shared memory (matrix too large)");
+  const int bit = sizeof(T) == 8 ? 1 : 2;
+  if (!(checked & bit)) {
+    // one CTA per SM at the largest slice guarantees co-residency of every launch
+    BEM_CUDA(c, cudaFuncSetAttribute(panel_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, kPanelSmemMax));
+    int occ = 0;
+    BEM_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, panel_kernel<T>, 256, kPanelSmemMax));
+    if (occ < 1) return bem_fail(c, BEM_ERR_CUDA, "panel kernel cannot be resident");
+    checked |= bit;
   }
-  int occ = 0;
-  BEM_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, panel_kernel<T>, 256, smem));
-  if (occ < 1) return bem_fail(c, BEM_ERR_CUDA, "panel kernel cannot be resident");
-  BEM_CUDA(c, cudaMemsetAsync(ws.barrier, 0, sizeof(unsigned), c->stream));
   double* cv = ws.cand_val;
   int* ci = ws.cand_idx;
   T* cc = reinterpret_cast<T*>(ws.cand_col);
   T* dc = reinterpret_cast<T*>(ws.diag_col);
   unsigned* bar = ws.barrier;
   int* st = ws.status;
-  void* args[] = {&S, &lda, &n, &r0, &w, &chunk, &piv, &cv, &ci, &cc, &dc, &bar, &st};
+  unsigned bb = bar_base;
+  void* args[] = {&S, &lda, &n, &r0, &w, &chunk, &piv, &cv, &ci, &cc, &dc, &bar, &bb, &st};
   BEM_CUDA(c, cudaLaunchCooperativeKernel((void*)panel_kernel<T>, dim3(G), dim3(256), args, smem, c->stream));
   ++c->launches;
+  bar_base += (unsigned)w * (unsigned)G;
   return BEM_OK;
 }
 
@@ -468,7 +539,7 @@ size_t lu_workspace_bytes(int n, int nb, int gmax, int elem) {
   const size_t ldy = ((size_t)n + 31) / 32 * 32;
   return up256(2 * (size_t)gmax * sizeof(double)) + up256(2 * (size_t)gmax * sizeof(int)) +
          up256(2 * (size_t)gmax * kPanelW * elem) + up256(2 * (size_t)kPanelW * elem) + up256(16) +
-         up256((size_t)nb * nb * elem) + up256(ldy * nb * elem);
+         up256((size_t)kInvBlock * kInvBlock * elem) + up256(ldy * nb * elem);
 }
 
 LUWorkspace lu_workspace_carve(void* base, int n, int nb, int gmax, int elem) {
@@ -488,7 +559,7 @@ LUWorkspace lu_workspace_carve(void* base, int n, int nb, int gmax, int elem) {
   w.status = reinterpret_cast<int*>(p + 8);
   p += up256(16);
   w.inv = p;
-  p += up256((size_t)nb * nb * elem);
+  p += up256((size_t)kInvBlock * kInvBlock * elem);
   w.ybuf = p;
   return w;
 }
@@ -507,7 +578,9 @@ int lu_factor(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int nb, int* info)
 template <typename T>
 int lu_factor_ws(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int nb, int* info, const LUWorkspace& ws) {
   *info = 0;
-  BEM_CUDA(c, cudaMemsetAsync(ws.status, 0, 2 * sizeof(int), c->stream));
+  // barrier counter (offset 0) and status words (offset 8) of the workspace's sync slot
+  BEM_CUDA(c, cudaMemsetAsync(ws.barrier, 0, 16, c->stream));
+  unsigned bar_base = 0;
   if (sizeof(T) == 4 && c->f32_gemm == 4) {
     if (c->umma_err.count < 1) BEM_CUDA(c, c->umma_err.alloc(1));
     BEM_CUDA(c, cudaMemsetAsync(c->umma_err.p, 0, sizeof(int), c->stream));
@@ -515,8 +588,7 @@ int lu_factor_ws(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int nb, int* in
   T* V = reinterpret_cast<T*>(ws.inv);
   T* Y = reinterpret_cast<T*>(ws.ybuf);
   const int64_t ldy = ws.ldy;
-  const size_t inv_smem = (size_t)nb * nb * sizeof(T);
-  if (inv_smem > 200 * 1024) return bem_fail(c, BEM_ERR_ARG, "block size too large for the inverse kernel");
+  const size_t inv_smem = (size_t)kInvBlock * kInvBlock * sizeof(T);
   cudaFuncSetAttribute(inv_unit_upper_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inv_smem);
   int rc;
   LUProfile prof;
@@ -526,7 +598,7 @@ int lu_factor_ws(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int nb, int* in
     for (int r0 = j0; r0 < j0 + jb; r0 += kPanelW) {
       const int w = std::min(kPanelW, j0 + jb - r0);
       prof.begin(0, c->stream);
-      if ((rc = panel_launch<T>(c, ws, S, lda, n, r0, w, piv))) return rc;
+      if ((rc = panel_launch<T>(c, ws, S, lda, n, r0, w, piv, bar_base))) return rc;
       prof.end(c->stream);
       prof.begin(1, c->stream);
       // swaps on the other rows of the panel and on the trailing rows
@@ -554,10 +626,19 @@ int lu_factor_ws(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int nb, int* in
     if (t0 < n) {
       const int m = n - t0;
       prof.begin(3, c->stream);
-      inv_unit_upper_kernel<T><<<1, ((jb + 31) / 32) * 32, inv_smem, c->stream>>>(S + j0 + (int64_t)j0 * lda, lda, jb,
-                                                                                   V, nb);
-      BEM_LAUNCH_CHECK(c);
-      if ((rc = gemm<T>(c, m, jb, jb, S + t0 + (int64_t)j0 * lda, lda, V, nb, Y, ldy, 1))) return rc;
+      // TRSM of the block row, Y = X U^{-1} with U the unit upper triangle of the panel's
+      // diagonal block, in 128-wide column blocks: X_b -= Y_{<b} U_{<b,b}, Y_b = X_b inv(U_bb)
+      for (int b0 = 0; b0 < jb; b0 += kInvBlock) {
+        const int bb = std::min(kInvBlock, jb - b0);
+        T* Xb = S + t0 + (int64_t)(j0 + b0) * lda;
+        if (b0 > 0 &&
+            (rc = gemm<T>(c, m, bb, b0, Y, ldy, S + j0 + (int64_t)(j0 + b0) * lda, lda, Xb, lda, 0)))
+          return rc;
+        inv_unit_upper_kernel<T><<<1, 256, inv_smem, c->stream>>>(
+            S + (j0 + b0) + (int64_t)(j0 + b0) * lda, lda, bb, V, kInvBlock);
+        BEM_LAUNCH_CHECK(c);
+        if ((rc = gemm<T>(c, m, bb, bb, Xb, lda, V, kInvBlock, Y + (int64_t)b0 * ldy, ldy, 1))) return rc;
+      }
       BEM_CUDA(c, cudaMemcpy2DAsync(S + t0 + (int64_t)j0 * lda, lda * sizeof(T), Y, ldy * sizeof(T), m * sizeof(T),
                                     jb, cudaMemcpyDeviceToDevice, c->stream));
       prof.end(c->stream);
@@ -590,121 +671,257 @@ template int lu_factor<float>(bem_ctx*, float*, int64_t, int, int*, int, int*);
 // triangular solves
 // ---------------------------------------------------------------------------------
 
-// forward: solve U^T w = b on the diagonal block [j0, j0+jb) (lower triangle of S,
-// non-unit diagonal), b overwritten by w.  The block is staged in shared memory first.
+// Triangular solves of the factors (see lu.cuh): forward with the lower triangle of S
+// (non-unit diagonal), backward with the panels' multipliers and their interchanges.
+// Diagonal blocks are solved by one warp from a shared-memory copy of the block: each
+// lane holds 4 of the 128 unknowns, each step broadcasts the newest unknown with a
+// shuffle, so a block costs ~128 dependent FMA+shuffle steps instead of 128 barriers.
+
+// Solve the jb x jb lower (non-unit) block of S at (j0, j0) in shared memory D
+// (column-major, leading dimension kSolveBlock) for the unknowns w (in/out, shared);
+// rdiag holds the reciprocals of the diagonal, so the dependent chain of each step is
+// a shuffle and a multiply-add.
 template <typename T>
-__global__ void fwd_diag_kernel(const T* S, int64_t lda, int j0, int jb, double* b) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* D = reinterpret_cast<T*>(smem_raw);  // [jb][jb] column-major
-  __shared__ double w[256];
-  const int t = threadIdx.x;
-  for (int idx = t; idx < jb * jb; idx += blockDim.x) {
-    const int r = idx % jb, cc = idx / jb;
-    D[idx] = (r >= cc) ? S[(j0 + r) + (int64_t)(j0 + cc) * lda] : T(0);
-  }
-  if (t < jb) w[t] = b[j0 + t];
-  __syncthreads();
+__device__ void warp_lower_solve(const T* D, const double* rdiag, int jb, double* w) {
+  const int lane = threadIdx.x & 31;
+  double x[kSolveBlock / 32];
+#pragma unroll
+  for (int q = 0; q < kSolveBlock / 32; ++q) x[q] = (lane + 32 * q < jb) ? w[lane + 32 * q] : 0.0;
+#pragma unroll 4
   for (int cidx = 0; cidx < jb; ++cidx) {
-    if (t == cidx) w[t] = w[t] / (double)D[t + t * jb];
-    __syncthreads();
-    if (t > cidx && t < jb) w[t] -= (double)D[t + cidx * jb] * w[cidx];
-    __syncthreads();
+    double dcol[kSolveBlock / 32];
+#pragma unroll
+    for (int q = 0; q < kSolveBlock / 32; ++q) dcol[q] = (double)D[lane + 32 * q + cidx * kSolveBlock];
+    const int owner = cidx & 31, slot = cidx >> 5;
+    double xc = x[0];
+#pragma unroll
+    for (int q = 1; q < kSolveBlock / 32; ++q)
+      if (q == slot) xc = x[q];
+    xc = __shfl_sync(0xffffffffu, xc, owner) * rdiag[cidx];
+#pragma unroll
+    for (int q = 0; q < kSolveBlock / 32; ++q) {
+      const int r = lane + 32 * q;
+      if (r == cidx) x[q] = xc;
+      else if (r > cidx) x[q] = fma(-dcol[q], xc, x[q]);
+    }
   }
-  if (t < jb) b[j0 + t] = w[t];
+#pragma unroll
+  for (int q = 0; q < kSolveBlock / 32; ++q)
+    if (lane + 32 * q < jb) w[lane + 32 * q] = x[q];
 }
 
-// b[r] -= sum_c S(r, c) w[c] for r in [r0, n), c in [j0, j0+jb)
+// the same for the strict upper (unit diagonal) block, from the last unknown down
 template <typename T>
-__global__ void fwd_gemv_kernel(const T* S, int64_t lda, int n, int r0, int j0, int jb, double* b) {
-  __shared__ double w[256];
-  if (threadIdx.x < jb) w[threadIdx.x] = b[j0 + threadIdx.x];
-  __syncthreads();
-  const int64_t r = r0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= n) return;
-  double acc = 0.0;
-  const T* p = S + r + (int64_t)j0 * lda;
-  for (int cidx = 0; cidx < jb; ++cidx) acc = fma((double)p[(int64_t)cidx * lda], w[cidx], acc);
-  b[r] -= acc;
-}
-
-// backward, off-panel part: part[blk][t] = sum_{c' in blk} S(j0+t, c') v[c']
-template <typename T>
-__global__ void bwd_dot_kernel(const T* S, int64_t lda, int n, int j0, int jb, int c0, const double* v,
-                               double* part) {
-  const int t = threadIdx.x;  // row of the panel
-  const int cs = c0 + blockIdx.x * 128;
-  const int ce = min(n, cs + 128);
-  double acc = 0.0;
-  if (t < jb)
-    for (int cc = cs; cc < ce; ++cc) acc = fma((double)S[(j0 + t) + (int64_t)cc * lda], v[cc], acc);
-  if (t < jb) part[(int64_t)blockIdx.x * 256 + t] = acc;
-}
-
-// backward, within-panel part and the panel's swaps (one CTA); the panel's strict
-// upper block is staged in shared memory first
-template <typename T>
-__global__ void bwd_finish_kernel(const T* S, int64_t lda, int n, int j0, int jb, int nblk, const double* part,
-                                  const int* piv, double* v) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* D = reinterpret_cast<T*>(smem_raw);  // [jb][jb] column-major
-  __shared__ double w[256];
-  const int t = threadIdx.x;
-  for (int idx = t; idx < jb * jb; idx += blockDim.x) {
-    const int r = idx % jb, cc = idx / jb;
-    D[idx] = (r < cc) ? S[(j0 + r) + (int64_t)(j0 + cc) * lda] : T(0);
-  }
-  if (t < jb) {
-    double s = 0.0;
-    for (int bb = 0; bb < nblk; ++bb) s += part[(int64_t)bb * 256 + t];
-    w[t] = v[j0 + t] - s;
-  }
-  __syncthreads();
+__device__ void warp_upper_unit_solve(const T* D, int jb, double* w) {
+  const int lane = threadIdx.x & 31;
+  double x[kSolveBlock / 32];
+#pragma unroll
+  for (int q = 0; q < kSolveBlock / 32; ++q) x[q] = (lane + 32 * q < jb) ? w[lane + 32 * q] : 0.0;
+#pragma unroll 4
   for (int cidx = jb - 1; cidx >= 0; --cidx) {
-    // w[cidx] final; remove its contribution from the rows above
-    if (t < cidx) w[t] -= (double)D[t + cidx * jb] * w[cidx];
-    __syncthreads();
+    double dcol[kSolveBlock / 32];
+#pragma unroll
+    for (int q = 0; q < kSolveBlock / 32; ++q) dcol[q] = (double)D[lane + 32 * q + cidx * kSolveBlock];
+    const int owner = cidx & 31, slot = cidx >> 5;
+    double xc = x[0];
+#pragma unroll
+    for (int q = 1; q < kSolveBlock / 32; ++q)
+      if (q == slot) xc = x[q];
+    xc = __shfl_sync(0xffffffffu, xc, owner);
+#pragma unroll
+    for (int q = 0; q < kSolveBlock / 32; ++q) {
+      const int r = lane + 32 * q;
+      if (r < cidx) x[q] = fma(-dcol[q], xc, x[q]);
+    }
   }
-  if (t < jb) v[j0 + t] = w[t];
+#pragma unroll
+  for (int q = 0; q < kSolveBlock / 32; ++q)
+    if (lane + 32 * q < jb) w[lane + 32 * q] = x[q];
+}
+
+// Forward step: every CTA subtracts the (final) unknowns of block [j0, j0+jb) from its
+// 256 rows of b below the block; CTA 0, whose first rows are the next block
+// [jn, jn+jnb), then solves that block.  jb = 0 skips the update (first block).
+template <typename T>
+__global__ void __launch_bounds__(256) fwd_step_kernel(const T* __restrict__ S, int64_t lda, int n, int j0, int jb,
+                                                       int jn, int jnb, double* b) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* D = reinterpret_cast<T*>(smem_raw);  // [kSolveBlock][kSolveBlock] column-major
+  __shared__ double wb[kSolveBlock];
+  __shared__ double wn[kSolveBlock];
+  __shared__ double rdiag[kSolveBlock];
+  const int t = threadIdx.x;
+  if (jb > 0) {
+    if (t < jb) wb[t] = b[j0 + t];
+    __syncthreads();
+    const int64_t r = (int64_t)j0 + jb + (int64_t)blockIdx.x * blockDim.x + t;
+    if (r < n) {
+      const T* p = S + r + (int64_t)j0 * lda;
+      double acc0 = 0.0, acc1 = 0.0;
+      int cidx = 0;
+#pragma unroll 8
+      for (; cidx + 1 < jb; cidx += 2) {
+        acc0 = fma((double)p[(int64_t)cidx * lda], wb[cidx], acc0);
+        acc1 = fma((double)p[(int64_t)(cidx + 1) * lda], wb[cidx + 1], acc1);
+      }
+      if (cidx < jb) acc0 = fma((double)p[(int64_t)cidx * lda], wb[cidx], acc0);
+      b[r] -= acc0 + acc1;
+    }
+  }
+  if (blockIdx.x != 0 || jnb <= 0) return;
+  __syncthreads();  // this CTA's updates of rows [jn, jn+jnb) are visible to the block
+  stage_block<T>(D, kSolveBlock, S + jn + (int64_t)jn * lda, lda, jnb, jnb, kSolveBlock, kSolveBlock,
+                 [](int r, int cc) { return r >= cc; });
+  if (t < jnb) wn[t] = b[jn + t];
   __syncthreads();
-  if (t == 0)
-    for (int q = jb - 1; q >= 0; --q) {
-      const int p = piv[j0 + q];
-      if (p != j0 + q) {
-        const double a = v[j0 + q];
-        v[j0 + q] = v[p];
+  if (t < kSolveBlock) rdiag[t] = (t < jnb) ? 1.0 / (double)D[t + t * kSolveBlock] : 0.0;
+  __syncthreads();
+  if (t < 32) warp_lower_solve<T>(D, rdiag, jnb, wn);
+  __syncthreads();
+  if (t < jnb) b[jn + t] = wn[t];
+}
+
+// Backward, off-block part: part[chunk][t] = sum over the chunk's 512 columns c' >= c0
+// of S(j0+t, c') v[c'] for the block's rows t < jb.  A warp reads one column's rows
+// with 16-byte loads (each lane 16 bytes of rows), the 8 warps of a CTA take columns
+// 8 apart, and their per-row partials meet in shared memory.
+template <typename T>
+__global__ void __launch_bounds__(256) bwd_dot_kernel(const T* __restrict__ S, int64_t lda, int n, int j0, int jb,
+                                                      int c0, const double* v, double* part) {
+  constexpr int RPL = 16 / sizeof(T);            // rows per lane per 16-byte load
+  constexpr int LANES = kSolveBlock / RPL;       // lanes that cover the 128 rows
+  __shared__ double red[8][kSolveBlock];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int cs = c0 + blockIdx.x * 512;
+  const int ce = min(n, cs + 512);
+  double acc[RPL];
+#pragma unroll
+  for (int q = 0; q < RPL; ++q) acc[q] = 0.0;
+  // 16-byte loads need the block's rows aligned; jb is the full 128 except for the
+  // very last (partial) block, which takes the scalar path
+  const bool vec = (jb == kSolveBlock) && ((((uintptr_t)(S + j0)) & 15) == 0) && ((lda * sizeof(T)) % 16 == 0);
+  for (int g = 0; g < 2; ++g) {
+    // lanes [0, LANES) cover the rows; with FP32 (LANES = 32) one column per warp, with
+    // FP64 (LANES = 64) a column spans two passes g
+    const int lane_row = lane + 32 * g;
+    if (lane_row >= LANES) break;
+    const int r0 = lane_row * RPL;
+#pragma unroll 4
+    for (int cc = cs + warp; cc < ce; cc += 8) {
+      const double vc = v[cc];
+      const T* p = S + (j0 + r0) + (int64_t)cc * lda;
+      if (vec) {
+        if (sizeof(T) == 4) {
+          const float4 a = *reinterpret_cast<const float4*>(p);
+          acc[0] = fma((double)a.x, vc, acc[0]);
+          acc[1 % RPL] = fma((double)a.y, vc, acc[1 % RPL]);
+          acc[2 % RPL] = fma((double)a.z, vc, acc[2 % RPL]);
+          acc[3 % RPL] = fma((double)a.w, vc, acc[3 % RPL]);
+        } else {
+          const double2 a = *reinterpret_cast<const double2*>(p);
+          acc[0] = fma(a.x, vc, acc[0]);
+          acc[1 % RPL] = fma(a.y, vc, acc[1 % RPL]);
+        }
+      } else {
+#pragma unroll
+        for (int q = 0; q < RPL; ++q)
+          if (r0 + q < jb) acc[q] = fma((double)p[q], vc, acc[q]);
+      }
+    }
+    if (sizeof(T) == 8 || g == 0) {
+#pragma unroll
+      for (int q = 0; q < RPL; ++q) red[warp][r0 + q] = acc[q];
+#pragma unroll
+      for (int q = 0; q < RPL; ++q) acc[q] = 0.0;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < kSolveBlock) {
+    double s0 = 0.0;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) s0 += red[w][threadIdx.x];
+    part[(int64_t)blockIdx.x * kSolveBlock + threadIdx.x] = s0;
+  }
+}
+
+// Backward, block part: reduce the partial sums, solve the block's unit upper part with
+// one warp, and after the panel's first block apply the panel's interchanges
+// (in reverse order) when do_swaps is set.
+template <typename T>
+__global__ void __launch_bounds__(256) bwd_finish_kernel(const T* __restrict__ S, int64_t lda, int j0, int jb,
+                                                         int nchunk, const double* part, const int* piv,
+                                                         int do_swaps, int p0, int pb, double* v) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* D = reinterpret_cast<T*>(smem_raw);
+  __shared__ double w[kSolveBlock];
+  const int t = threadIdx.x;
+  stage_block<T>(D, kSolveBlock, S + j0 + (int64_t)j0 * lda, lda, jb, jb, kSolveBlock, kSolveBlock,
+                 [](int r, int cc) { return r < cc; });
+  if (t < jb) {
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int k = 0;
+    for (; k + 8 <= nchunk; k += 8) {
+#pragma unroll
+      for (int u = 0; u < 8; ++u) acc[u] += part[(int64_t)(k + u) * kSolveBlock + t];
+    }
+    for (; k < nchunk; ++k) acc[0] += part[(int64_t)k * kSolveBlock + t];
+    w[t] = v[j0 + t] - (((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7])));
+  }
+  __syncthreads();
+  if (t < 32) warp_upper_unit_solve<T>(D, jb, w);
+  __syncthreads();
+  if (t < jb) v[j0 + t] = w[t];
+  if (!do_swaps) return;
+  __syncthreads();
+  if (t == 0) {
+    __threadfence_block();
+    for (int q = pb - 1; q >= 0; --q) {
+      const int p = piv[p0 + q];
+      if (p != p0 + q) {
+        const double a = v[p0 + q];
+        v[p0 + q] = v[p];
         v[p] = a;
       }
     }
+  }
 }
 
 template <typename T>
 int lu_solve_ws(bem_ctx* c, const T* S, int64_t lda, int n, const int* piv, int nb, double* b, double* work) {
-  if (nb > 256) return bem_fail(c, BEM_ERR_ARG, "lu_solve: block size > 256");
-  const size_t dsm = (size_t)nb * nb * sizeof(T);
-  if (dsm > 200 * 1024) return bem_fail(c, BEM_ERR_ARG, "lu_solve: diagonal block exceeds shared memory");
-  cudaFuncSetAttribute(fwd_diag_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm);
-  cudaFuncSetAttribute(bwd_finish_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm);
-  for (int j0 = 0; j0 < n; j0 += nb) {
-    const int jb = std::min(nb, n - j0);
-    fwd_diag_kernel<T><<<1, 256, dsm, c->stream>>>(S, lda, j0, jb, b);
-    BEM_LAUNCH_CHECK(c);
-    const int r0 = j0 + jb;
-    if (r0 < n) {
-      fwd_gemv_kernel<T><<<(n - r0 + 255) / 256, 256, 0, c->stream>>>(S, lda, n, r0, j0, jb, b);
-      BEM_LAUNCH_CHECK(c);
-    }
+  // triangular blocks of kSolveBlock; the interchanges are applied per factorisation
+  // panel of width nb (the product form of the factors)
+  const int db = kSolveBlock;
+  const size_t dsm = (size_t)db * db * sizeof(T);
+  static int attr = 0;
+  const int bit = sizeof(T) == 8 ? 1 : 2;
+  if (!(attr & bit)) {
+    cudaFuncSetAttribute(fwd_step_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm);
+    cudaFuncSetAttribute(bwd_finish_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm);
+    attr |= bit;
   }
-  const int last = ((n - 1) / nb) * nb;
-  for (int j0 = last; j0 >= 0; j0 -= nb) {
-    const int jb = std::min(nb, n - j0);
-    const int c0 = j0 + jb;
-    const int nblk = (n - c0 + 127) / 128;
-    if (nblk > 0) {
-      bwd_dot_kernel<T><<<nblk, 256, 0, c->stream>>>(S, lda, n, j0, jb, c0, b, work);
+  // forward: launch k updates with block k-1 and solves block k
+  for (int jn = 0, j0 = 0, jb = 0; jn < n; j0 = jn, jn += db) {
+    const int jnb = std::min(db, n - jn);
+    jb = (jn == 0) ? 0 : std::min(db, n - j0);
+    const int rows = n - jn;
+    fwd_step_kernel<T><<<(rows + 255) / 256, 256, dsm, c->stream>>>(S, lda, n, j0, jb, jn, jnb, b);
+    BEM_LAUNCH_CHECK(c);
+  }
+  const int last_panel = ((n - 1) / nb) * nb;
+  for (int p0 = last_panel; p0 >= 0; p0 -= nb) {
+    const int pb = std::min(nb, n - p0);
+    const int last_blk = p0 + ((pb - 1) / db) * db;
+    for (int j0 = last_blk; j0 >= p0; j0 -= db) {
+      const int jb = std::min(db, p0 + pb - j0);
+      const int c0 = j0 + jb;
+      const int nchunk = (n - c0 + 511) / 512;
+      if (nchunk > 0) {
+        bwd_dot_kernel<T><<<nchunk, 256, 0, c->stream>>>(S, lda, n, j0, jb, c0, b, work);
+        BEM_LAUNCH_CHECK(c);
+      }
+      bwd_finish_kernel<T><<<1, 256, dsm, c->stream>>>(S, lda, j0, jb, nchunk, work, piv, j0 == p0 ? 1 : 0, p0, pb, b);
       BEM_LAUNCH_CHECK(c);
     }
-    bwd_finish_kernel<T><<<1, 256, dsm, c->stream>>>(S, lda, n, j0, jb, nblk, work, piv, b);
-    BEM_LAUNCH_CHECK(c);
   }
   return BEM_OK;
 }
@@ -737,14 +954,26 @@ __global__ void residual_part_kernel(const double* A, int64_t lda, int n, const 
   __syncthreads();
   const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= n) return;
-  double acc = 0.0, aabs = 0.0;
+  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0}, aabs = 0.0;
   const double* p = A + r + (int64_t)cs * lda;
-  for (int cc = 0; cc < ce - cs; ++cc) {
+  const int cnt = ce - cs;
+  int cc = 0;
+  for (; cc + 8 <= cnt; cc += 8) {
+    double a[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) a[u] = p[(int64_t)(cc + u) * lda];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      acc[u] = fma(a[u], xs[cc + u], acc[u]);
+      if (want_anorm) aabs += fabs(a[u]);
+    }
+  }
+  for (; cc < cnt; ++cc) {
     const double a = p[(int64_t)cc * lda];
-    acc = fma(a, xs[cc], acc);
+    acc[0] = fma(a, xs[cc], acc[0]);
     if (want_anorm) aabs += fabs(a);
   }
-  part[(int64_t)blockIdx.y * n + r] = acc;
+  part[(int64_t)blockIdx.y * n + r] = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
   if (want_anorm) apart[(int64_t)blockIdx.y * n + r] = aabs;
 }
 

@@ -66,6 +66,7 @@ extern "C" int bem_dgesv_noalloc(int n, int nrhs, double* dA, int lda, int* d_ip
     g_scratch_addr[dev] = p;
   }
   unsigned char* base = static_cast<unsigned char*>(g_scratch_addr[dev]);
+  if (bem::lu_workspace_bytes(n, kNoAllocNb, kNoAllocGmax, sizeof(double)) > kFactorBytes) return BEM_ERR_TOO_LARGE;
 
   // a context on the stack: no device memory of its own (its buffers stay empty)
   bem_ctx c;

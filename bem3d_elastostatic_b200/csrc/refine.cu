@@ -1,6 +1,8 @@
 // Mixed-precision solve (FP32 factors + FP64 iterative refinement against the FP64
 // A) and reorganize_solution (io_mod.f90:148-183).
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <algorithm>
 #include <vector>
 
@@ -8,7 +10,7 @@
 
 namespace bem {
 
-constexpr int kNbMixed = 128;
+constexpr int kNbMixed = 256;  // panel width of the FP32 factorisation (halves the trailing C traffic)
 
 __global__ void to_fp32_kernel(const double* A, int64_t lda, int n, float* A32) {
   const int64_t total = (int64_t)lda * n;
@@ -67,12 +69,29 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
   double norms[4] = {0, 0, 0, 0};
   double anorm = -1.0, berr = 1.0, prev = 1e300;
   int it = 0;
+  const bool ir_prof = getenv("BEM_IR_PROFILE") != nullptr;
+  cudaEvent_t q0, q1, q2;
+  if (ir_prof) {
+    cudaEventCreate(&q0);
+    cudaEventCreate(&q1);
+    cudaEventCreate(&q2);
+  }
   for (it = 1; it <= max_iter; ++it) {
+    if (ir_prof) cudaEventRecord(q0, c->stream);
     BEM_CUDA(c, cudaMemcpyAsync(d.p, r.p, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
     if ((rc = lu_solve<float>(c, c->A32.p, lda, n, c->piv.p, kNbMixed, d.p))) return rc;
     axpy_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(n, d.p, c->X.p);
     BEM_LAUNCH_CHECK(c);
+    if (ir_prof) cudaEventRecord(q1, c->stream);
     if ((rc = residual_fp64(c, c->A.p, lda, n, c->X.p, c->FI.p, r.p, norms, anorm < 0))) return rc;
+    if (ir_prof) {
+      cudaEventRecord(q2, c->stream);
+      cudaEventSynchronize(q2);
+      float a = 0.f, b2 = 0.f;
+      cudaEventElapsedTime(&a, q0, q1);
+      cudaEventElapsedTime(&b2, q1, q2);
+      fprintf(stderr, "[ir it=%d] lu-solve %.2f ms residual %.2f ms\n", it, a, b2);
+    }
     if (anorm < 0) anorm = norms[3];
     berr = norms[0] / (anorm * norms[1] + norms[2]);
     if (!(berr == berr)) break;  // NaN: diverged

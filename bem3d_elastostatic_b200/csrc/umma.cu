@@ -11,11 +11,15 @@
 // 128 x 256 accumulator with tcgen05.ld (one TMEM lane = one row of C) into a
 // coalesced read-modify-write of C.
 //
-// Every mbarrier wait is bounded: on timeout the kernel records an error word, skips
-// the rest of its work, waits (bounded) for its own copies and frees its tensor memory.
+// Every mbarrier wait is bounded: on timeout the kernel records an error word, the
+// other roles stop at their next wait, the producer waits (bounded) for its own copies
+// and the MMA warp for its own MMAs, and the tensor memory is freed.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cstdint>
 
 #include "lu.cuh"
 
@@ -26,13 +30,15 @@ namespace {
 constexpr int UM = 128;                 // tile rows (UMMA M)
 constexpr int UN = 256;                 // tile columns (UMMA N)
 constexpr int UK = 64;                  // K chunk per TMA box (128 bytes of BF16)
-constexpr int kMaxK = 128;              // K handled without a ring (2 chunks resident)
-constexpr int kChunks = kMaxK / UK;
+constexpr int kMaxK = 256;              // largest panel width
+constexpr int kStages = 2;              // shared-memory ring of K chunks
 constexpr int A_TILE = UM * UK * 2;     // 16 KB
 constexpr int B_TILE = UN * UK * 2;     // 32 KB
 constexpr int STAGE = 2 * A_TILE + 2 * B_TILE;  // hi + lo of A and B: 96 KB
-constexpr int kSmem = kChunks * STAGE + 1024 + 256;
-constexpr unsigned kTmemCols = 256;
+constexpr int kSmem = kStages * STAGE + 1024 + 256;
+constexpr unsigned kTmemCols = 512;     // two 128 x 256 FP32 accumulators
+constexpr int kEpiThreads = 256;        // 8 epilogue warps
+constexpr int kThreads = 64 + kEpiThreads;
 constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s bound on every mbarrier wait
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
@@ -45,7 +51,8 @@ __device__ __forceinline__ unsigned long long globaltimer() {
   return t;
 }
 
-__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
+// bounded wait on an mbarrier phase; gives up early when another role aborted
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, volatile int* abort_flag) {
   const unsigned long long t0 = globaltimer();
   while (true) {
     unsigned done;
@@ -57,6 +64,7 @@ __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
         : "r"(bar), "r"(parity)
         : "memory");
     if (done) return true;
+    if (abort_flag && *abort_flag) return false;
     if (globaltimer() - t0 > kWaitNs) return false;
   }
 }
@@ -67,7 +75,17 @@ __device__ __forceinline__ uint64_t sw128_desc(unsigned saddr) {
   return (uint64_t)((saddr >> 4) & 0x3FFF) | (1ull << 16) | (64ull << 32) | (1ull << 46) | (2ull << 61);
 }
 
-__global__ void __launch_bounds__(128, 1)
+__device__ __forceinline__ void umma_commit(unsigned bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+// Persistent, warp-specialised: warp 0 (one lane) streams K chunks with TMA through a
+// two-stage ring, warp 1 (one lane) issues the MMAs into one of two TMEM accumulators,
+// warps 2-9 drain the other accumulator into C, so the read-modify-write of one tile
+// overlaps the loads and MMAs of the next.  Tiles run m-fastest so a CTA wave shares
+// the B operand band; C is read and written with streaming (evict-first) hints so it
+// does not push the operands out of L2.
+__global__ void __launch_bounds__(kThreads, 1)
     umma_update_kernel(const __grid_constant__ CUtensorMap tAh, const __grid_constant__ CUtensorMap tAl,
                        const __grid_constant__ CUtensorMap tBh, const __grid_constant__ CUtensorMap tBl, int M,
                        int N, int K, float* C, int64_t ldc, int* err) {
@@ -75,22 +93,34 @@ __global__ void __launch_bounds__(128, 1)
   const unsigned raw = smem_u32(umma_smem);
   const unsigned base = (raw + 1023u) & ~1023u;  // 1024-byte aligned operand tiles
   unsigned char* gbase = umma_smem + (base - raw);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(gbase + kChunks * STAGE);  // full[kChunks], done
-  unsigned* tmem_slot = reinterpret_cast<unsigned*>(gbase + kChunks * STAGE + 128);
-  __shared__ int s_fail;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(gbase + kStages * STAGE);
+  uint64_t* full = bars;        // [kStages] TMA -> MMA
+  uint64_t* empty = bars + 2;   // [kStages] MMA -> TMA
+  uint64_t* tfull = bars + 4;   // [2] MMA -> epilogue
+  uint64_t* tempty = bars + 6;  // [2] epilogue -> MMA
+  uint64_t* drain = bars + 8;   // MMA completion before teardown
+  unsigned* tmem_slot = reinterpret_cast<unsigned*>(gbase + kStages * STAGE + 128);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(gbase + kStages * STAGE + 136);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int m0 = blockIdx.x * UM, n0 = blockIdx.y * UN;
-  const int nchunk = (K + UK - 1) / UK;
+  const int tiles_m = (M + UM - 1) / UM, tiles_n = (N + UN - 1) / UN, total = tiles_m * tiles_n;
+  const int nchunk = K / UK;
 
   if (threadIdx.x == 0) {
-    s_fail = 0;
-    for (int c = 0; c <= kChunks; ++c)
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&bars[c])), "r"(1) : "memory");
+    *abort_flag = 0;
+    for (int s = 0; s < kStages; ++s) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&full[s])), "r"(1) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&empty[s])), "r"(1) : "memory");
+    }
+    for (int b = 0; b < 2; ++b) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&tfull[b])), "r"(1) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&tempty[b])), "r"(kEpiThreads) : "memory");
+    }
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(drain)), "r"(1) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
-  if (warp == 0) {
+  if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
                  "r"(kTmemCols)
                  : "memory");
@@ -101,105 +131,175 @@ __global__ void __launch_bounds__(128, 1)
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const unsigned tmem = *tmem_slot;
 
-  if (threadIdx.x == 0) {
-    // producer: every K chunk of A (hi, lo) and B (hi, lo) at once
-    for (int c = 0; c < nchunk; ++c) {
-      const unsigned st = base + c * STAGE;
-      const unsigned bar = smem_u32(&bars[c]);
-      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"((unsigned)STAGE)
-                   : "memory");
-      const int kx = c * UK;
+  auto fail = [&]() {
+    *abort_flag = 1;
+    atomicCAS(err, 0, BEM_ERR_TIMEOUT);
+  };
+
+  if (warp == 0) {
+    if (lane == 0) {
+      int stage = 0;
+      unsigned phase = 0;
+      int last[kStages] = {-1, -1};
       const CUtensorMap* maps[4] = {&tAh, &tAl, &tBh, &tBl};
-      const unsigned dst[4] = {st, st + A_TILE, st + 2 * A_TILE, st + 2 * A_TILE + B_TILE};
-      const int row[4] = {m0, m0, n0, n0};
-      for (int t = 0; t < 4; ++t)
-        asm volatile(
-            "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
-            "[%4];" ::"r"(dst[t]),
-            "l"(reinterpret_cast<uint64_t>(maps[t])), "r"(kx), "r"(row[t]), "r"(bar)
-            : "memory");
+      for (int t = blockIdx.x; t < total && !*abort_flag; t += gridDim.x) {
+        const int m0 = (t % tiles_m) * UM, n0 = (t / tiles_m) * UN;
+        const int row[4] = {m0, m0, n0, n0};
+        for (int c = 0; c < nchunk; ++c) {
+          if (!mbar_wait(smem_u32(&empty[stage]), phase ^ 1u, abort_flag)) {
+            fail();
+            break;
+          }
+          const unsigned st = base + stage * STAGE;
+          const unsigned bar = smem_u32(&full[stage]);
+          asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"((unsigned)STAGE)
+                       : "memory");
+          const unsigned dst[4] = {st, st + A_TILE, st + 2 * A_TILE, st + 2 * A_TILE + B_TILE};
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            asm volatile(
+                "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+                "[%4];" ::"r"(dst[q]),
+                "l"(reinterpret_cast<uint64_t>(maps[q])), "r"(c * UK), "r"(row[q]), "r"(bar)
+                : "memory");
+          last[stage] = (int)phase;
+          if (++stage == kStages) {
+            stage = 0;
+            phase ^= 1u;
+          }
+        }
+      }
+      // this CTA's own copies must have landed before its shared memory goes away
+      for (int s = 0; s < kStages; ++s)
+        if (last[s] >= 0) mbar_wait(smem_u32(&full[s]), (unsigned)last[s], nullptr);
     }
-    // MMA issue: D (TMEM) = sum over chunks, K steps and the three split products
-    // instruction descriptor: F32 accumulate, BF16 A and B, K-major both, N = 256, M = 128
-    const unsigned idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(UN >> 3) << 17) | ((unsigned)(UM >> 4) << 24);
-    int acc = 0;
-    bool ok = true;
-    for (int c = 0; c < nchunk && ok; ++c) {
-      if (!mbar_wait(smem_u32(&bars[c]), 0)) {
-        ok = false;
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // F32 accumulate, BF16 A and B, both K-major, N = 256, M = 128
+      const unsigned idesc =
+          (1u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(UN >> 3) << 17) | ((unsigned)(UM >> 4) << 24);
+      int stage = 0, ab = 0;
+      unsigned phase = 0, aphase = 0;
+      for (int t = blockIdx.x; t < total && !*abort_flag; t += gridDim.x) {
+        if (!mbar_wait(smem_u32(&tempty[ab]), aphase ^ 1u, abort_flag)) {
+          fail();
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const unsigned d = tmem + (unsigned)(ab * UN);
+        bool ok = true;
+        for (int c = 0; c < nchunk; ++c) {
+          if (!mbar_wait(smem_u32(&full[stage]), phase, abort_flag)) {
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const unsigned st = base + stage * STAGE;
+          const unsigned ah = st, al = st + A_TILE, bh = st + 2 * A_TILE, bl = st + 2 * A_TILE + B_TILE;
+#pragma unroll
+          for (int kk = 0; kk < UK / 16; ++kk) {
+            const unsigned off = kk * 32;  // 16 BF16 = 32 bytes along K inside the swizzle atom
+            const uint64_t a_h = sw128_desc(ah + off), a_l = sw128_desc(al + off);
+            const uint64_t b_h = sw128_desc(bh + off), b_l = sw128_desc(bl + off);
+            const uint64_t pa[3] = {a_h, a_h, a_l}, pb[3] = {b_h, b_l, b_h};
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+              const int acc = (c | kk | q) != 0;
+              asm volatile(
+                  "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                  "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+                  "l"(pa[q]), "l"(pb[q]), "r"(idesc), "r"(acc)
+                  : "memory");
+            }
+          }
+          umma_commit(smem_u32(&empty[stage]));  // frees the stage once these MMAs are done
+          if (++stage == kStages) {
+            stage = 0;
+            phase ^= 1u;
+          }
+        }
+        if (!ok) {
+          fail();
+          break;
+        }
+        umma_commit(smem_u32(&tfull[ab]));  // accumulator ready for the epilogue
+        if (++ab == 2) {
+          ab = 0;
+          aphase ^= 1u;
+        }
+      }
+      umma_commit(smem_u32(drain));
+      mbar_wait(smem_u32(drain), 0, nullptr);
+    }
+    __syncwarp();
+  } else {
+    // 8 epilogue warps: warp w reads TMEM lane quarter (w % 4) and one half of the
+    // 256 columns; each chunk's C loads are issued before the previous chunk is stored,
+    // keeping ~64 loads per thread in flight (the C stream is latency-bound otherwise)
+    const int lq = warp & 3;
+    const int half = (warp - 2) >> 2;  // 0 or 1
+    int ab = 0;
+    unsigned aphase = 0;
+    for (int t = blockIdx.x; t < total && !*abort_flag; t += gridDim.x) {
+      const int m0 = (t % tiles_m) * UM, n0 = (t / tiles_m) * UN;
+      if (!mbar_wait(smem_u32(&tfull[ab]), aphase, abort_flag)) {
+        fail();
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const unsigned st = base + c * STAGE;
-      const unsigned ah = st, al = st + A_TILE, bh = st + 2 * A_TILE, bl = st + 2 * A_TILE + B_TILE;
-      for (int kk = 0; kk < UK / 16; ++kk) {
-        const unsigned off = kk * 32;  // 16 BF16 = 32 bytes along K inside the swizzle atom
-        const uint64_t a_h = sw128_desc(ah + off), a_l = sw128_desc(al + off);
-        const uint64_t b_h = sw128_desc(bh + off), b_l = sw128_desc(bl + off);
-        const uint64_t pa[3] = {a_h, a_h, a_l}, pb[3] = {b_h, b_l, b_h};
-        for (int t = 0; t < 3; ++t) {
-          asm volatile(
-              "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-              "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
-              "l"(pa[t]), "l"(pb[t]), "r"(idesc), "r"(acc)
-              : "memory");
-          acc = 1;
-        }
+      const int row = m0 + lq * 32 + lane;
+      const bool rok = row < M;
+      float cur[32], nxt[32];
+      const int cbase = n0 + half * (UN / 2);
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        const int col = cbase + j;
+        cur[j] = (rok && col < N) ? __ldcs(C + row + (int64_t)col * ldc) : 0.f;
       }
-    }
-    if (ok) {
-      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                       smem_u32(&bars[kChunks]))
-                   : "memory");
-    } else {
-      s_fail = 1;
-      atomicCAS(err, 0, BEM_ERR_TIMEOUT);
-      // let this CTA's own copies land (bounded) before the shared memory is released
-      for (int c = 0; c < nchunk; ++c) mbar_wait(smem_u32(&bars[c]), 0);
-    }
-  }
-  __syncwarp();
-  // epilogue: wait for the MMAs, then 32 columns at a time TMEM -> registers -> C
-  bool ok = true;
-  if (!s_fail) ok = mbar_wait(smem_u32(&bars[kChunks]), 0);
-  __syncthreads();
-  if (!ok || s_fail) {
-    if (threadIdx.x == 0) atomicCAS(err, 0, BEM_ERR_TIMEOUT);
-  } else {
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const int row = m0 + warp * 32 + lane;
-    for (int j0 = 0; j0 < UN; j0 += 32) {
-      unsigned r[32];
-      const unsigned taddr = tmem + ((unsigned)(warp * 32) << 16) + (unsigned)j0;
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-          "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-            "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]),
-            "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]),
-            "=r"(r[30]), "=r"(r[31])
-          : "r"(taddr)
-          : "memory");
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (row < M) {
-        float old[32];
+#pragma unroll 1
+      for (int q = 0; q < UN / 64; ++q) {
+        const int j0 = half * (UN / 2) + 32 * q;
+        if (q + 1 < UN / 64) {
 #pragma unroll
-        for (int j = 0; j < 32; ++j) {
-          const int col = n0 + j0 + j;
-          old[j] = (col < N) ? C[row + (int64_t)col * ldc] : 0.f;
+          for (int j = 0; j < 32; ++j) {
+            const int col = n0 + j0 + 32 + j;
+            nxt[j] = (rok && col < N) ? __ldcs(C + row + (int64_t)col * ldc) : 0.f;
+          }
+        }
+        unsigned r[32];
+        const unsigned taddr = tmem + ((unsigned)(lq * 32) << 16) + (unsigned)(ab * UN + j0);
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+            "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+              "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+              "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+              "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+              "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+            : "r"(taddr)
+            : "memory");
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if (rok) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            const int col = n0 + j0 + j;
+            if (col < N) __stcs(C + row + (int64_t)col * ldc, cur[j] - __uint_as_float(r[j]));
+          }
         }
 #pragma unroll
-        for (int j = 0; j < 32; ++j) {
-          const int col = n0 + j0 + j;
-          if (col < N) C[row + (int64_t)col * ldc] = old[j] - __uint_as_float(r[j]);
-        }
+        for (int j = 0; j < 32; ++j) cur[j] = nxt[j];
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&tempty[ab])) : "memory");
+      if (++ab == 2) {
+        ab = 0;
+        aphase ^= 1u;
       }
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
-  if (warp == 0) {
+  if (warp == 1) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
   }
@@ -260,7 +360,7 @@ bool umma_supported(int K) { return K > 0 && K <= kMaxK && K % UK == 0; }
 // C (M x N) -= A (M x K) * B (K x N) on tcgen05 with the three-term BF16 split.
 int gemm_umma_bf16x3(bem_ctx* c, int M, int N, int K, const float* A, int64_t lda, const float* B, int64_t ldb,
                      float* C, int64_t ldc) {
-  if (!umma_supported(K)) return bem_fail(c, BEM_ERR_ARG, "umma: K must be a multiple of 64 up to 128");
+  if (!umma_supported(K)) return bem_fail(c, BEM_ERR_ARG, "umma: K must be a multiple of 64 up to 256");
   if (!g_encode) {
     cudaDriverEntryPointQueryResult q;
     void* fn = nullptr;
@@ -289,9 +389,10 @@ int gemm_umma_bf16x3(bem_ctx* c, int M, int N, int K, const float* A, int64_t ld
   if (!make_map(&mAh, ah, M, K, UM) || !make_map(&mAl, al, M, K, UM) || !make_map(&mBh, bh, N, K, UN) ||
       !make_map(&mBl, bl, N, K, UN))
     return bem_fail(c, BEM_ERR_CUDA, "umma: tensor map encoding failed");
-  dim3 grid((M + UM - 1) / UM, (N + UN - 1) / UN);
-  if (grid.y > 65535) return bem_fail(c, BEM_ERR_ARG, "umma: N too large");
-  umma_update_kernel<<<grid, 128, kSmem, c->stream>>>(mAh, mAl, mBh, mBl, M, N, K, C, ldc, c->umma_err.p);
+  const int64_t tiles = (int64_t)((M + UM - 1) / UM) * ((N + UN - 1) / UN);
+  if (tiles > INT32_MAX) return bem_fail(c, BEM_ERR_ARG, "umma: too many tiles");
+  const int grid = (int)std::min<int64_t>(tiles, c->sm_count);
+  umma_update_kernel<<<grid, kThreads, kSmem, c->stream>>>(mAh, mAl, mBh, mBl, M, N, K, C, ldc, c->umma_err.p);
   BEM_LAUNCH_CHECK(c);
   return BEM_OK;
 }
