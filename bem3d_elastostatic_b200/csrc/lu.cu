@@ -740,38 +740,42 @@ __device__ void warp_upper_unit_solve(const T* D, int jb, double* w) {
 }
 
 // Forward step: every CTA subtracts the (final) unknowns of block [j0, j0+jb) from its
-// 256 rows of b below the block; CTA 0, whose first rows are the next block
-// [jn, jn+jnb), then solves that block.  jb = 0 skips the update (first block).
+// 128 rows of b below the block (4 threads per row, 32 columns each, all loads issued
+// at once); CTA 0, whose rows are the next block [jn, jn+jnb), then solves that block.
+// jb = 0 skips the update (first block).
 template <typename T>
-__global__ void __launch_bounds__(256) fwd_step_kernel(const T* __restrict__ S, int64_t lda, int n, int j0, int jb,
+__global__ void __launch_bounds__(512) fwd_step_kernel(const T* __restrict__ S, int64_t lda, int n, int j0, int jb,
                                                        int jn, int jnb, double* b) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* D = reinterpret_cast<T*>(smem_raw);  // [kSolveBlock][kSolveBlock] column-major
   __shared__ double wb[kSolveBlock];
   __shared__ double wn[kSolveBlock];
   __shared__ double rdiag[kSolveBlock];
+  __shared__ double red[4][kSolveBlock];
   const int t = threadIdx.x;
+  const int rl = t & (kSolveBlock - 1), qtr = t >> 7;
+  const int64_t r = (int64_t)jn + (int64_t)blockIdx.x * kSolveBlock + rl;
   if (jb > 0) {
     if (t < jb) wb[t] = b[j0 + t];
     __syncthreads();
-    const int64_t r = (int64_t)j0 + jb + (int64_t)blockIdx.x * blockDim.x + t;
+    double acc = 0.0;
     if (r < n) {
-      const T* p = S + r + (int64_t)j0 * lda;
-      double acc0 = 0.0, acc1 = 0.0;
-      int cidx = 0;
-#pragma unroll 8
-      for (; cidx + 1 < jb; cidx += 2) {
-        acc0 = fma((double)p[(int64_t)cidx * lda], wb[cidx], acc0);
-        acc1 = fma((double)p[(int64_t)(cidx + 1) * lda], wb[cidx + 1], acc1);
-      }
-      if (cidx < jb) acc0 = fma((double)p[(int64_t)cidx * lda], wb[cidx], acc0);
-      b[r] -= acc0 + acc1;
+      const int cb = qtr * 32;
+      const T* p = S + r + (int64_t)(j0 + cb) * lda;
+      T a[32];
+#pragma unroll
+      for (int u = 0; u < 32; ++u) a[u] = (cb + u < jb) ? p[(int64_t)u * lda] : T(0);
+#pragma unroll
+      for (int u = 0; u < 32; ++u) acc = fma((double)a[u], (cb + u < jb) ? wb[cb + u] : 0.0, acc);
     }
+    red[qtr][rl] = acc;
+    __syncthreads();
+    if (qtr == 0 && r < n) b[r] -= (red[0][rl] + red[1][rl]) + (red[2][rl] + red[3][rl]);
   }
   if (blockIdx.x != 0 || jnb <= 0) return;
   __syncthreads();  // this CTA's updates of rows [jn, jn+jnb) are visible to the block
   stage_block<T>(D, kSolveBlock, S + jn + (int64_t)jn * lda, lda, jnb, jnb, kSolveBlock, kSolveBlock,
-                 [](int r, int cc) { return r >= cc; });
+                 [](int rr, int cc) { return rr >= cc; });
   if (t < jnb) wn[t] = b[jn + t];
   __syncthreads();
   if (t < kSolveBlock) rdiag[t] = (t < jnb) ? 1.0 / (double)D[t + t * kSolveBlock] : 0.0;
@@ -806,7 +810,7 @@ __global__ void __launch_bounds__(256) bwd_dot_kernel(const T* __restrict__ S, i
     const int lane_row = lane + 32 * g;
     if (lane_row >= LANES) break;
     const int r0 = lane_row * RPL;
-#pragma unroll 4
+#pragma unroll 16
     for (int cc = cs + warp; cc < ce; cc += 8) {
       const double vc = v[cc];
       const T* p = S + (j0 + r0) + (int64_t)cc * lda;
@@ -904,7 +908,8 @@ int lu_solve_ws(bem_ctx* c, const T* S, int64_t lda, int n, const int* piv, int 
     const int jnb = std::min(db, n - jn);
     jb = (jn == 0) ? 0 : std::min(db, n - j0);
     const int rows = n - jn;
-    fwd_step_kernel<T><<<(rows + 255) / 256, 256, dsm, c->stream>>>(S, lda, n, j0, jb, jn, jnb, b);
+    fwd_step_kernel<T><<<(rows + kSolveBlock - 1) / kSolveBlock, 512, dsm, c->stream>>>(S, lda, n, j0, jb, jn, jnb,
+                                                                                      b);
     BEM_LAUNCH_CHECK(c);
   }
   const int last_panel = ((n - 1) / nb) * nb;
