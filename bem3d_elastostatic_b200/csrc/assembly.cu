@@ -60,7 +60,7 @@ __device__ __forceinline__ int sym_idx(int a, int b) {
 
 // fi_acc (3) and d1_acc (9) are this lane's running sums over its elements, kept in
 // shared memory so the 9 x NC accumulators below have the register file to themselves.
-template <int NC, int MODE>
+template <int NC, int MODE, typename R>
 __device__ __forceinline__ void regular_pair(const AsmArgs& P, int e, const int* kc, double xi0,
                                              double xi1, double xi2, int64_t row,
                                              double* fi_acc, double* d1) {
@@ -71,30 +71,32 @@ __device__ __forceinline__ void regular_pair(const AsmArgs& P, int e, const int*
 
   // ---- G: U* (symmetric, 6 values) x p12 -------------------------------------------
   {
-    double g[NC][6];
+    R g[NC][6];
 #pragma unroll
     for (int k = 0; k < NC; ++k)
 #pragma unroll
-      for (int p = 0; p < 6; ++p) g[k][p] = 0.0;
+      for (int p = 0; p < 6; ++p) g[k][p] = R(0);
+    const R rc3 = (R)c3, rc4 = (R)c4;
 #pragma unroll 2
     for (int q = 0; q < NG; ++q) {
-      const double r0 = __ldg(T + 6 * q + 0) - xi0;
-      const double r1 = __ldg(T + 6 * q + 1) - xi1;
-      const double r2 = __ldg(T + 6 * q + 2) - xi2;
-      const double ri = rsqrt(r0 * r0 + r1 * r1 + r2 * r2);
-      const double a0 = r0 * ri, a1 = r1 * ri, a2 = r2 * ri;
-      const double c3r = c3 * ri;
-      double u[6];
-      u[0] = (c4 + a0 * a0) * c3r;
-      u[1] = (c4 + a1 * a1) * c3r;
-      u[2] = (c4 + a2 * a2) * c3r;
+      // the coordinate difference is always formed in FP64 (no cancellation in R)
+      const R r0 = (R)(__ldg(T + 6 * q + 0) - xi0);
+      const R r1 = (R)(__ldg(T + 6 * q + 1) - xi1);
+      const R r2 = (R)(__ldg(T + 6 * q + 2) - xi2);
+      const R ri = rsqrt(r0 * r0 + r1 * r1 + r2 * r2);
+      const R a0 = r0 * ri, a1 = r1 * ri, a2 = r2 * ri;
+      const R c3r = rc3 * ri;
+      R u[6];
+      u[0] = (rc4 + a0 * a0) * c3r;
+      u[1] = (rc4 + a1 * a1) * c3r;
+      u[2] = (rc4 + a2 * a2) * c3r;
       u[3] = a0 * a1 * c3r;
       u[4] = a1 * a2 * c3r;
       u[5] = a2 * a0 * c3r;
       const double* W = T + kTabGeo + 9 * q;
 #pragma unroll
       for (int k = 0; k < NC; ++k) {
-        const double w = __ldg(W + k);
+        const R w = (R)__ldg(W + k);
 #pragma unroll
         for (int p = 0; p < 6; ++p) g[k][p] = fma(u[p], w, g[k][p]);
       }
@@ -148,34 +150,35 @@ __device__ __forceinline__ void regular_pair(const AsmArgs& P, int e, const int*
 
   // ---- H: T* (9 values) x p12 ------------------------------------------------------
   {
-    double h[NC][9];  // h[k][jj + 3*ii]
+    R h[NC][9];  // h[k][jj + 3*ii]
 #pragma unroll
     for (int k = 0; k < NC; ++k)
 #pragma unroll
-      for (int p = 0; p < 9; ++p) h[k][p] = 0.0;
+      for (int p = 0; p < 9; ++p) h[k][p] = R(0);
+    const R rc5 = (R)c5, rc6 = (R)c6;
 #pragma unroll 1
     for (int q = 0; q < NG; ++q) {
-      const double r0 = __ldg(T + 6 * q + 0) - xi0;
-      const double r1 = __ldg(T + 6 * q + 1) - xi1;
-      const double r2 = __ldg(T + 6 * q + 2) - xi2;
-      const double n[3] = {__ldg(T + 6 * q + 3), __ldg(T + 6 * q + 4), __ldg(T + 6 * q + 5)};
-      const double ri = rsqrt(r0 * r0 + r1 * r1 + r2 * r2);
-      const double a[3] = {r0 * ri, r1 * ri, r2 * ri};
-      const double rdn = a[0] * n[0] + a[1] * n[1] + a[2] * n[2];
-      const double c5r2 = c5 * ri * ri;
-      double t[9];
+      const R r0 = (R)(__ldg(T + 6 * q + 0) - xi0);
+      const R r1 = (R)(__ldg(T + 6 * q + 1) - xi1);
+      const R r2 = (R)(__ldg(T + 6 * q + 2) - xi2);
+      const R n[3] = {(R)__ldg(T + 6 * q + 3), (R)__ldg(T + 6 * q + 4), (R)__ldg(T + 6 * q + 5)};
+      const R ri = rsqrt(r0 * r0 + r1 * r1 + r2 * r2);
+      const R a[3] = {r0 * ri, r1 * ri, r2 * ri};
+      const R rdn = a[0] * n[0] + a[1] * n[1] + a[2] * n[2];
+      const R c5r2 = rc5 * ri * ri;
+      R t[9];
 #pragma unroll
       for (int ii = 0; ii < 3; ++ii)
 #pragma unroll
         for (int jj = 0; jj < 3; ++jj) {
-          const double d = (ii == jj) ? c6 : 0.0;
+          const R d = (ii == jj) ? rc6 : R(0);
           t[jj + 3 * ii] =
-              c5r2 * (rdn * (d + 3.0 * a[ii] * a[jj]) + c6 * (n[jj] * a[ii] - n[ii] * a[jj]));
+              c5r2 * (rdn * (d + R(3) * a[ii] * a[jj]) + rc6 * (n[jj] * a[ii] - n[ii] * a[jj]));
         }
       const double* W = T + kTabGeo + 9 * q;
 #pragma unroll
       for (int k = 0; k < NC; ++k) {
-        const double w = __ldg(W + k);
+        const R w = (R)__ldg(W + k);
 #pragma unroll
         for (int p = 0; p < 9; ++p) h[k][p] = fma(t[p], w, h[k][p]);
       }
@@ -185,7 +188,7 @@ __device__ __forceinline__ void regular_pair(const AsmArgs& P, int e, const int*
     for (int p = 0; p < 9; ++p) {
       double s = 0.0;
 #pragma unroll
-      for (int k = 0; k < NC; ++k) s += h[k][p];
+      for (int k = 0; k < NC; ++k) s += (double)h[k][p];
       d1[p] -= s;
     }
     if (MODE == kModeA) {
@@ -259,7 +262,10 @@ __device__ __forceinline__ void regular_pair(const AsmArgs& P, int e, const int*
     for (int jj = 0; jj < 3; ++jj) fi_acc[jj] += fi[jj];
 }
 
-template <int MODE>
+// PREC 0: every regular pair in FP64.  PREC 1: pairs farther than 3.5 element radii
+// from the element centroid (the near-field radius of stress_mod.f90:603-604) evaluate
+// and accumulate the Kelvin kernels in FP32; nearer pairs stay in FP64.
+template <int MODE, int PREC>
 __global__ void __launch_bounds__(256, 1) ghmat_regular_kernel(AsmArgs P) {
   __shared__ double s_red[kBatch][32][12];
   const int w = threadIdx.x >> 5;
@@ -285,11 +291,37 @@ __global__ void __launch_bounds__(256, 1) ghmat_regular_kernel(AsmArgs P) {
         kc[m] = (m < ncone) ? __ldg(P.kconec + m + 9 * e) - 1 : 0;
         sing |= (m < ncone) && (kc[m] == in);
       }
+      bool far32 = false;
+      if (PREC == 1) {
+        double cx = 0.0, cy = 0.0, cz = 0.0;
+        for (int m = 0; m < ncone; ++m) {
+          cx += P.x[kc[m]];
+          cy += P.y[kc[m]];
+          cz += P.z[kc[m]];
+        }
+        cx /= ncone;
+        cy /= ncone;
+        cz /= ncone;
+        double r2 = 0.0;
+        for (int m = 0; m < ncone; ++m) {
+          const double dx = P.x[kc[m]] - cx, dy = P.y[kc[m]] - cy, dz = P.z[kc[m]] - cz;
+          r2 = fmax(r2, dx * dx + dy * dy + dz * dz);
+        }
+        const double dx = xi0 - cx, dy = xi1 - cy, dz = xi2 - cz;
+        far32 = dx * dx + dy * dy + dz * dz > 12.25 * r2;
+      }
       if (active && !sing) {
-        if (ncone == 9)
-          regular_pair<9, MODE>(P, e, kc, xi0, xi1, xi2, row, fi, d1);
-        else
-          regular_pair<6, MODE>(P, e, kc, xi0, xi1, xi2, row, fi, d1);
+        if (ncone == 9) {
+          if (far32)
+            regular_pair<9, MODE, float>(P, e, kc, xi0, xi1, xi2, row, fi, d1);
+          else
+            regular_pair<9, MODE, double>(P, e, kc, xi0, xi1, xi2, row, fi, d1);
+        } else {
+          if (far32)
+            regular_pair<6, MODE, float>(P, e, kc, xi0, xi1, xi2, row, fi, d1);
+          else
+            regular_pair<6, MODE, double>(P, e, kc, xi0, xi1, xi2, row, fi, d1);
+        }
       }
     }
     __syncthreads();
@@ -624,7 +656,10 @@ int launch_ghmat8(bem_ctx* c, int precision) {
   P.lda = lda;
   P.FI = c->FI.p;
   const int tiles = (c->n + 31) / 32;
-  ghmat_regular_kernel<kModeA><<<tiles, 256, 0, c->stream>>>(P);
+  if (precision == BEM_ASM_FP32_FAR)
+    ghmat_regular_kernel<kModeA, 1><<<tiles, 256, 0, c->stream>>>(P);
+  else
+    ghmat_regular_kernel<kModeA, 0><<<tiles, 256, 0, c->stream>>>(P);
   BEM_LAUNCH_CHECK(c);
   ghmat_singular_kernel<kModeA><<<(c->n + 3) / 4, 128, 0, c->stream>>>(P);
   BEM_LAUNCH_CHECK(c);
@@ -652,7 +687,7 @@ int launch_hg(bem_ctx* c, int in0, int in1, double* dH, int64_t ldh, double* dG,
   P.G = dG;
   P.ldg = ldg;
   const int tiles = (P.nrows_nodes + 31) / 32;
-  ghmat_regular_kernel<kModeHG><<<tiles, 256, 0, c->stream>>>(P);
+  ghmat_regular_kernel<kModeHG, 0><<<tiles, 256, 0, c->stream>>>(P);
   BEM_LAUNCH_CHECK(c);
   ghmat_singular_kernel<kModeHG><<<(P.nrows_nodes + 3) / 4, 128, 0, c->stream>>>(P);
   BEM_LAUNCH_CHECK(c);

@@ -23,6 +23,65 @@ __global__ void axpy_kernel(int n, const double* d, double* x) {
   if (i < n) x[i] += d[i];
 }
 
+// ---------------------------------------------------------------------------------
+// GMRES-IR building blocks: FP64 vectors, deterministic reductions
+// ---------------------------------------------------------------------------------
+constexpr int kGmresM = 30;       // restart length
+constexpr int kDotBlocks = 296;   // 2 CTAs per SM for the multi-dot partials
+
+// part[b][i] = sum over block b's slice of V[i] . w, i < k
+__global__ void __launch_bounds__(256) multidot_kernel(int n, int k, const double* V, int64_t ldv, const double* w,
+                                                       double* part) {
+  __shared__ double red[8][kGmresM + 1];
+  double acc[kGmresM + 1];
+#pragma unroll
+  for (int i = 0; i <= kGmresM; ++i) acc[i] = 0.0;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+    const double we = w[e];
+#pragma unroll
+    for (int i = 0; i <= kGmresM; ++i)
+      if (i < k) acc[i] = fma(V[e + i * ldv], we, acc[i]);
+  }
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+#pragma unroll
+  for (int i = 0; i <= kGmresM; ++i) {
+    double v = acc[i];
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+    if (lane == 0) red[wp][i] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < k) {
+    double sacc = 0.0;
+    for (int q = 0; q < 8; ++q) sacc += red[q][threadIdx.x];
+    part[(int64_t)blockIdx.x * (kGmresM + 1) + threadIdx.x] = sacc;
+  }
+}
+
+__global__ void reduce_parts_kernel(int nb, int k, const double* part, double* out) {
+  const int i = threadIdx.x;
+  if (i >= k) return;
+  double sacc = 0.0;
+  for (int b = 0; b < nb; ++b) sacc += part[(int64_t)b * (kGmresM + 1) + i];
+  out[i] = sacc;
+}
+
+// w += sign * sum_{i<k} V[i] h[i]
+__global__ void vcomb_kernel(int n, int k, const double* V, int64_t ldv, const double* h, double sign, double* w) {
+  __shared__ double hs[kGmresM + 1];
+  if (threadIdx.x < k) hs[threadIdx.x] = h[threadIdx.x];
+  __syncthreads();
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  double sacc = 0.0;
+  for (int i = 0; i < k; ++i) sacc = fma(V[e + i * ldv], hs[i], sacc);
+  w[e] = fma(sign, sacc, w[e]);
+}
+
+__global__ void scale_kernel(int n, double a, const double* x, double* y) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < n) y[e] = a * x[e];
+}
+
 int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_solve_info* st, int* info) {
   const int n = 3 * c->n;
   const int64_t lda = c->lda;
@@ -63,41 +122,153 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
   if (rc) return rc;
   BEM_CUDA(c, cudaEventRecord(e1, c->stream));
   if (*info != 0) return BEM_OK;
-  // x0 = LU^{-1} b, then x += LU^{-1} (b - A x)
+  // x0 = LU^{-1} b, then x += LU^{-1} (b - A x)   (plain refinement), or
+  // x += GMRES(M^{-1} A, M^{-1} r) with M = the low-precision LU (GMRES-IR)
   BEM_CUDA(c, cudaMemsetAsync(c->X.p, 0, n * sizeof(double), c->stream));
   BEM_CUDA(c, cudaMemcpyAsync(r.p, c->FI.p, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
   double norms[4] = {0, 0, 0, 0};
   double anorm = -1.0, berr = 1.0, prev = 1e300;
-  int it = 0;
+  int it = 0, restarts = 0;
   const bool ir_prof = getenv("BEM_IR_PROFILE") != nullptr;
-  cudaEvent_t q0, q1, q2;
-  if (ir_prof) {
-    cudaEventCreate(&q0);
-    cudaEventCreate(&q1);
-    cudaEventCreate(&q2);
-  }
-  for (it = 1; it <= max_iter; ++it) {
-    if (ir_prof) cudaEventRecord(q0, c->stream);
-    BEM_CUDA(c, cudaMemcpyAsync(d.p, r.p, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-    if ((rc = lu_solve<float>(c, c->A32.p, lda, n, c->piv.p, kNbMixed, d.p))) return rc;
-    axpy_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(n, d.p, c->X.p);
-    BEM_LAUNCH_CHECK(c);
-    if (ir_prof) cudaEventRecord(q1, c->stream);
-    if ((rc = residual_fp64(c, c->A.p, lda, n, c->X.p, c->FI.p, r.p, norms, anorm < 0))) return rc;
+  const bool use_gmres = (precision == BEM_PREC_BF16_IR);
+  if (!use_gmres) {
+    cudaEvent_t q0, q1, q2;
     if (ir_prof) {
-      cudaEventRecord(q2, c->stream);
-      cudaEventSynchronize(q2);
-      float a = 0.f, b2 = 0.f;
-      cudaEventElapsedTime(&a, q0, q1);
-      cudaEventElapsedTime(&b2, q1, q2);
-      fprintf(stderr, "[ir it=%d] lu-solve %.2f ms residual %.2f ms\n", it, a, b2);
+      cudaEventCreate(&q0);
+      cudaEventCreate(&q1);
+      cudaEventCreate(&q2);
     }
-    if (anorm < 0) anorm = norms[3];
-    berr = norms[0] / (anorm * norms[1] + norms[2]);
-    if (!(berr == berr)) break;  // NaN: diverged
-    if (berr <= rel_tol) break;
-    if (berr > 0.5 * prev && it > 3) break;  // stagnation
-    prev = berr;
+    for (it = 1; it <= max_iter; ++it) {
+      if (ir_prof) cudaEventRecord(q0, c->stream);
+      BEM_CUDA(c, cudaMemcpyAsync(d.p, r.p, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+      if ((rc = lu_solve<float>(c, c->A32.p, lda, n, c->piv.p, kNbMixed, d.p))) return rc;
+      axpy_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(n, d.p, c->X.p);
+      BEM_LAUNCH_CHECK(c);
+      if (ir_prof) cudaEventRecord(q1, c->stream);
+      if ((rc = residual_fp64(c, c->A.p, lda, n, c->X.p, c->FI.p, r.p, norms, anorm < 0))) return rc;
+      if (ir_prof) {
+        cudaEventRecord(q2, c->stream);
+        cudaEventSynchronize(q2);
+        float a = 0.f, b2 = 0.f;
+        cudaEventElapsedTime(&a, q0, q1);
+        cudaEventElapsedTime(&b2, q1, q2);
+        fprintf(stderr, "[ir it=%d] lu-solve %.2f ms residual %.2f ms\n", it, a, b2);
+      }
+      if (anorm < 0) anorm = norms[3];
+      berr = norms[0] / (anorm * norms[1] + norms[2]);
+      if (!(berr == berr)) break;  // NaN: diverged
+      if (berr <= rel_tol) break;
+      if (berr > 0.5 * prev && it > 3) break;  // stagnation
+      prev = berr;
+    }
+  } else {
+    // GMRES-IR: Krylov basis V (kGmresM + 1 vectors), FP64; Hessenberg least squares
+    // by Givens rotations on the host
+    const int64_t ldv = ((int64_t)n + 31) / 32 * 32;
+    DBuf<double> Vb, hd, part, zero;
+    BEM_CUDA(c, Vb.alloc((size_t)ldv * (kGmresM + 1)));
+    BEM_CUDA(c, hd.alloc(2 * (kGmresM + 1)));
+    BEM_CUDA(c, part.alloc((size_t)kDotBlocks * (kGmresM + 1)));
+    BEM_CUDA(c, zero.alloc(n));
+    BEM_CUDA(c, cudaMemsetAsync(zero.p, 0, n * sizeof(double), c->stream));
+    double* V = Vb.p;
+    const int vb = (n + 255) / 256;
+    auto dots = [&](int k, const double* w, double* out_host) -> int {
+      multidot_kernel<<<kDotBlocks, 256, 0, c->stream>>>(n, k, V, ldv, w, part.p);
+      BEM_LAUNCH_CHECK(c);
+      reduce_parts_kernel<<<1, 32, 0, c->stream>>>(kDotBlocks, k, part.p, hd.p);
+      BEM_LAUNCH_CHECK(c);
+      BEM_CUDA(c, cudaMemcpyAsync(out_host, hd.p, k * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+      BEM_CUDA(c, cudaStreamSynchronize(c->stream));
+      return BEM_OK;
+    };
+    auto norm2 = [&](const double* w, double* out) -> int {
+      // ||w||_2 through the multi-dot with V[0] temporarily replaced is awkward; use a
+      // dedicated pass over w . w
+      multidot_kernel<<<kDotBlocks, 256, 0, c->stream>>>(n, 1, w, ldv, w, part.p);
+      BEM_LAUNCH_CHECK(c);
+      reduce_parts_kernel<<<1, 32, 0, c->stream>>>(kDotBlocks, 1, part.p, hd.p);
+      BEM_LAUNCH_CHECK(c);
+      double v2 = 0.0;
+      BEM_CUDA(c, cudaMemcpyAsync(&v2, hd.p, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+      BEM_CUDA(c, cudaStreamSynchronize(c->stream));
+      *out = std::sqrt(v2);
+      return BEM_OK;
+    };
+    const double inner_tol = 1e-6;
+    for (restarts = 0; restarts < max_iter; ++restarts) {
+      if ((rc = residual_fp64(c, c->A.p, lda, n, c->X.p, c->FI.p, r.p, norms, anorm < 0))) return rc;
+      if (anorm < 0) anorm = norms[3];
+      berr = norms[0] / (anorm * norms[1] + norms[2]);
+      if (!(berr == berr) || berr <= rel_tol) break;
+      if (berr > 0.5 * prev && restarts > 3) break;  // stagnation
+      prev = berr;
+      // v0 = M^{-1} r / beta
+      BEM_CUDA(c, cudaMemcpyAsync(V, r.p, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+      if ((rc = lu_solve<float>(c, c->A32.p, lda, n, c->piv.p, kNbMixed, V))) return rc;
+      double beta = 0.0;
+      if ((rc = norm2(V, &beta))) return rc;
+      if (!(beta > 0.0)) break;
+      scale_kernel<<<vb, 256, 0, c->stream>>>(n, 1.0 / beta, V, V);
+      BEM_LAUNCH_CHECK(c);
+      double H[kGmresM + 1][kGmresM] = {}, cs[kGmresM] = {}, sn[kGmresM] = {}, g[kGmresM + 1] = {};
+      g[0] = beta;
+      int kdim = 0;
+      for (int j = 0; j < kGmresM; ++j) {
+        double* w = V + (int64_t)(j + 1) * ldv;
+        // w = M^{-1} A v_j  (residual_fp64 with b = 0 gives -A v_j)
+        if ((rc = residual_fp64(c, c->A.p, lda, n, V + (int64_t)j * ldv, zero.p, w, norms, false))) return rc;
+        if ((rc = lu_solve<float>(c, c->A32.p, lda, n, c->piv.p, kNbMixed, w))) return rc;
+        scale_kernel<<<vb, 256, 0, c->stream>>>(n, -1.0, w, w);
+        BEM_LAUNCH_CHECK(c);
+        // classical Gram-Schmidt, twice
+        double h1[kGmresM + 1], h2[kGmresM + 1];
+        if ((rc = dots(j + 1, w, h1))) return rc;
+        BEM_CUDA(c, cudaMemcpyAsync(hd.p, h1, (j + 1) * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        vcomb_kernel<<<vb, 256, 0, c->stream>>>(n, j + 1, V, ldv, hd.p, -1.0, w);
+        BEM_LAUNCH_CHECK(c);
+        if ((rc = dots(j + 1, w, h2))) return rc;
+        BEM_CUDA(c, cudaMemcpyAsync(hd.p, h2, (j + 1) * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        vcomb_kernel<<<vb, 256, 0, c->stream>>>(n, j + 1, V, ldv, hd.p, -1.0, w);
+        BEM_LAUNCH_CHECK(c);
+        for (int i = 0; i <= j; ++i) H[i][j] = h1[i] + h2[i];
+        double hn = 0.0;
+        if ((rc = norm2(w, &hn))) return rc;
+        H[j + 1][j] = hn;
+        if (hn > 0.0) {
+          scale_kernel<<<vb, 256, 0, c->stream>>>(n, 1.0 / hn, w, w);
+          BEM_LAUNCH_CHECK(c);
+        }
+        // apply the previous rotations, then a new one for (H[j][j], H[j+1][j])
+        for (int i = 0; i < j; ++i) {
+          const double a = H[i][j], b2 = H[i + 1][j];
+          H[i][j] = cs[i] * a + sn[i] * b2;
+          H[i + 1][j] = -sn[i] * a + cs[i] * b2;
+        }
+        const double a = H[j][j], b2 = H[j + 1][j];
+        const double rr = std::hypot(a, b2);
+        cs[j] = rr > 0 ? a / rr : 1.0;
+        sn[j] = rr > 0 ? b2 / rr : 0.0;
+        H[j][j] = rr;
+        H[j + 1][j] = 0.0;
+        g[j + 1] = -sn[j] * g[j];
+        g[j] = cs[j] * g[j];
+        ++it;
+        kdim = j + 1;
+        if (std::fabs(g[j + 1]) <= inner_tol * beta || hn == 0.0) break;
+      }
+      // y = H^{-1} g, x += V y
+      double y[kGmresM] = {};
+      for (int i = kdim - 1; i >= 0; --i) {
+        double sacc = g[i];
+        for (int q = i + 1; q < kdim; ++q) sacc -= H[i][q] * y[q];
+        y[i] = sacc / H[i][i];
+      }
+      BEM_CUDA(c, cudaMemcpyAsync(hd.p, y, kdim * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+      vcomb_kernel<<<vb, 256, 0, c->stream>>>(n, kdim, V, ldv, hd.p, 1.0, c->X.p);
+      BEM_LAUNCH_CHECK(c);
+      BEM_CUDA(c, cudaStreamSynchronize(c->stream));
+    }
   }
   BEM_CUDA(c, cudaEventRecord(e2, c->stream));
   BEM_CUDA(c, cudaEventSynchronize(e2));
@@ -108,8 +279,8 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
   cudaEventDestroy(e1);
   cudaEventDestroy(e2);
   if (st) {
-    st->iterations = std::min(it, max_iter);
-    st->restarts = 0;
+    st->iterations = use_gmres ? it : std::min(it, max_iter);
+    st->restarts = restarts;
     st->rel_residual = berr;
     st->factor_seconds = f_ms * 1e-3;
     st->refine_seconds = r_ms * 1e-3;

@@ -168,3 +168,37 @@ def test_dgesv_singular_reports_info():
     A = np.ones((40, 40))
     _, _, _, info = dgesv(A, np.ones(40))
     assert info > 0
+
+
+def test_bf16_gmres_ir_cube8(cube8_mesh):
+    """BF16 tensor-core factors as the GMRES preconditioner, FP64 residuals: the
+    refined solution meets the FP64 bar."""
+    from bem3d_elastostatic_b200.api import Quadesth
+
+    ref = O.Oracle(cube8_mesh).run()
+    q = Quadesth(cube8_mesh)
+    q.precompute_element_geometry()
+    q.ghmat8()
+    x = q.solve_linear_system("bf16-ir", tol=1e-14, max_iter=60)
+    err = np.abs(x - ref["x"]).max() / np.abs(ref["x"]).max()
+    assert err <= 1e-10, err
+    assert q.solve_info["rel_residual"] <= 1e-14
+    q.close()
+
+
+def test_fp32_far_assembly(cube2, gpu_cube2):
+    """Far pairs in FP32 (near pairs, singular pairs and all sums in FP64): A agrees
+    with the FP64 assembly to FP32 rounding, and the near-singular diagonal blocks are
+    the FP64 ones."""
+    A64, FI64 = gpu_cube2.ghmat8("fp64", return_system=True)
+    A32, FI32 = gpu_cube2.ghmat8("fp32-far", return_system=True)
+    rowmax = np.abs(A64).max(axis=1, keepdims=True)
+    rel = np.abs(A32 - A64) / rowmax
+    assert rel.max() <= 2e-6, rel.max()
+    assert rel.max() > 0.0  # some pairs were far
+    n = cube2.n
+    for i in range(n):
+        blk = np.s_[3 * i:3 * i + 3, 3 * i:3 * i + 3]
+        # the diagonal block mixes FP64 singular terms with the FP64 sums of FP32 terms
+        assert np.abs(A32[blk] - A64[blk]).max() <= 2e-6 * rowmax[3 * i:3 * i + 3].max()
+    assert np.abs(FI32 - FI64).max() <= 2e-6 * np.abs(FI64).max()
