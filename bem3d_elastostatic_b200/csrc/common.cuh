@@ -125,6 +125,7 @@ struct bem_ctx {
   // LU / refinement workspace
   bem::DBuf<float> A32;
   bem::DBuf<int> piv;
+  bem::DBuf<int> perm;  // gather form of the pivots of the latest factorisation (solve side)
   bem::DBuf<double> work;
   bem::DBuf<float> work32;
   bem::DBuf<unsigned int> sync;
@@ -170,8 +171,7 @@ int launch_hg(bem_ctx* c, int in0, int in1, double* dH, int64_t ldh, double* dG,
               int64_t ldg);
 int lu_factor_fp64(bem_ctx* c, double* A, int64_t lda, int n, int* d_piv, int* info,
                    double* seconds);
-int lu_solve_fp64(bem_ctx* c, const double* LU, int64_t lda, int n, const int* d_piv,
-                  double* b);
+int lu_solve_fp64(bem_ctx* c, const double* LU, int64_t lda, int n, double* b);
 int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter,
                 bem_solve_info* stats, int* info);
 int launch_reorganize(bem_ctx* c);

@@ -315,7 +315,7 @@ int bem_solve(bem_ctx* c, int precision, double rel_tol, int max_iter, double* F
     st.gflops = secs > 0 ? (2.0 / 3.0) * (double)N * N * N / secs * 1e-9 : 0.0;
     if (*info != 0) return *info;  // DGESV: singular U, no solution
     BEM_CUDA(c, cudaMemcpyAsync(c->X.p, c->FI.p, N * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-    rc = bem::lu_solve_fp64(c, c->A.p, c->lda, (int)N, c->piv.p, c->X.p);
+    rc = bem::lu_solve_fp64(c, c->A.p, c->lda, (int)N, c->X.p);
     if (rc) return rc;
   } else if (precision == BEM_PREC_FP32_IR || precision == BEM_PREC_BF16_IR) {
     rc = bem::solve_mixed(c, precision, rel_tol > 0 ? rel_tol : 1e-12, max_iter > 0 ? max_iter : 50, &st,
@@ -355,7 +355,7 @@ int bem_dgesv(bem_ctx* c, int n, int nrhs, double* A, int lda, int* ipiv, double
   if (rc) return rc;
   if (*info == 0)
     for (int j = 0; j < nrhs; ++j)
-      if ((rc = bem::lu_solve_fp64(c, dA.p, ld, n, dp.p, dB.p + (int64_t)j * ld))) return rc;
+      if ((rc = bem::lu_solve_fp64(c, dA.p, ld, n, dB.p + (int64_t)j * ld))) return rc;
   std::vector<int> hp(n);
   BEM_CUDA(c, cudaMemcpyAsync(hp.data(), dp.p, n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   BEM_CUDA(c, cudaMemcpy2DAsync(A, (size_t)lda * sizeof(double), dA.p, ld * sizeof(double), n * sizeof(double), n,

@@ -30,11 +30,22 @@ constexpr int kInvBlock = 128;       // unit-triangle inverse block of the block
 constexpr int kSolveBlock = 128;     // diagonal block of the triangular solves
 constexpr int kPanelSmemMax = 200 * 1024;
 constexpr long long kSpinLimit = 1ll << 24;
+constexpr int kSweepThreads = 512;   // threads of a triangular sweep CTA (4 per row of a block)
 
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
   unsigned v;
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
+}
+
+__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
 }
 
 __device__ __forceinline__ void better(double& bv, int& bc, int& bg, double v, int cidx, int gidx) {
@@ -567,16 +578,30 @@ LUWorkspace lu_workspace_carve(void* base, int n, int nb, int gmax, int elem) {
 size_t lu_solve_work_count(int n) { return ((size_t)n + 127) / 128 * 256 + 256; }
 
 template <typename T>
-int lu_factor(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int nb, int* info) {
+int lu_factor(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int* perm, int nb, int* info) {
   DBuf<unsigned char> scratch;
   const int gmax = c->sm_count;
   BEM_CUDA(c, scratch.alloc(lu_workspace_bytes(n, nb, gmax, sizeof(T))));
   const LUWorkspace ws = lu_workspace_carve(scratch.p, n, nb, gmax, sizeof(T));
-  return lu_factor_ws<T>(c, S, lda, n, piv, nb, info, ws);
+  return lu_factor_ws<T>(c, S, lda, n, piv, perm, nb, info, ws);
+}
+
+// x = P v with P = tau_0 tau_1 ... tau_{n-1} (tau_i swaps i and piv[i]) as a gather
+// x[i] = v[perm[i]]; composed on the host once per factorisation
+static int make_perm(bem_ctx* c, const int* d_piv, int n, int* d_perm) {
+  std::vector<int> p(n), a(n);
+  BEM_CUDA(c, cudaMemcpyAsync(p.data(), d_piv, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  BEM_CUDA(c, cudaStreamSynchronize(c->stream));
+  for (int i = 0; i < n; ++i) a[i] = i;
+  for (int i = n - 1; i >= 0; --i) std::swap(a[i], a[p[i]]);
+  BEM_CUDA(c, cudaMemcpyAsync(d_perm, a.data(), (size_t)n * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  BEM_CUDA(c, cudaStreamSynchronize(c->stream));
+  return BEM_OK;
 }
 
 template <typename T>
-int lu_factor_ws(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int nb, int* info, const LUWorkspace& ws) {
+int lu_factor_ws(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int* perm, int nb, int* info,
+                 const LUWorkspace& ws) {
   *info = 0;
   // barrier counter (offset 0) and status words (offset 8) of the workspace's sync slot
   BEM_CUDA(c, cudaMemsetAsync(ws.barrier, 0, 16, c->stream));
@@ -601,8 +626,9 @@ int lu_factor_ws(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int nb, int* in
       if ((rc = panel_launch<T>(c, ws, S, lda, n, r0, w, piv, bar_base))) return rc;
       prof.end(c->stream);
       prof.begin(1, c->stream);
-      // swaps on the other rows of the panel and on the trailing rows
-      const int a0 = j0, a1 = r0, b0 = r0 + w, b1 = n;
+      // swaps on every other row of S: the earlier panels' multipliers (rows [0, r0),
+      // so that the factors end up as T = P L U) and the trailing rows
+      const int a0 = 0, a1 = r0, b0 = r0 + w, b1 = n;
       const int64_t rows = (int64_t)(a1 - a0) + (b1 - b0);
       if (rows > 0) {
         swap_rows_kernel<T><<<(unsigned)((rows + 255) / 256), 256, 0, c->stream>>>(S, lda, piv, r0, w, a0, a1, b0,
@@ -659,13 +685,14 @@ int lu_factor_ws(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int nb, int* in
     if (ue != 0) return bem_fail(c, ue, "tcgen05 trailing update: an mbarrier wait timed out");
   }
   *info = st[1];
+  if (*info == 0 && perm) return make_perm(c, piv, n, perm);
   return BEM_OK;
 }
 
-template int lu_factor<double>(bem_ctx*, double*, int64_t, int, int*, int, int*);
-template int lu_factor_ws<double>(bem_ctx*, double*, int64_t, int, int*, int, int*, const LUWorkspace&);
-template int lu_factor_ws<float>(bem_ctx*, float*, int64_t, int, int*, int, int*, const LUWorkspace&);
-template int lu_factor<float>(bem_ctx*, float*, int64_t, int, int*, int, int*);
+template int lu_factor<double>(bem_ctx*, double*, int64_t, int, int*, int*, int, int*);
+template int lu_factor_ws<double>(bem_ctx*, double*, int64_t, int, int*, int*, int, int*, const LUWorkspace&);
+template int lu_factor_ws<float>(bem_ctx*, float*, int64_t, int, int*, int*, int, int*, const LUWorkspace&);
+template int lu_factor<float>(bem_ctx*, float*, int64_t, int, int*, int*, int, int*);
 
 // ---------------------------------------------------------------------------------
 // triangular solves
@@ -673,36 +700,36 @@ template int lu_factor<float>(bem_ctx*, float*, int64_t, int, int*, int, int*);
 
 // Triangular solves of the factors (see lu.cuh): forward with the lower triangle of S
 // (non-unit diagonal), backward with the panels' multipliers and their interchanges.
-// Diagonal blocks are solved by one warp from a shared-memory copy of the block: each
-// lane holds 4 of the 128 unknowns, each step broadcasts the newest unknown with a
-// shuffle, so a block costs ~128 dependent FMA+shuffle steps instead of 128 barriers.
+// Diagonal blocks are solved by one warp from a shared-memory copy of the block: lane
+// L holds unknowns L, L+32, L+64, L+96 in registers, and step c broadcasts the newest
+// unknown from its owner lane (c % 32, register c / 32) with a shuffle.  The loops over
+// the register slot and the owner lane are unrolled, so the owner and the slot are
+// compile-time constants and each step's dependent chain is one shuffle, one multiply
+// and one FMA; the shared-memory reads of the block's column do not depend on it.
 
-// Solve the jb x jb lower (non-unit) block of S at (j0, j0) in shared memory D
-// (column-major, leading dimension kSolveBlock) for the unknowns w (in/out, shared);
-// rdiag holds the reciprocals of the diagonal, so the dependent chain of each step is
-// a shuffle and a multiply-add.
+// Solve the jb x jb lower (non-unit) block D (column-major, leading dimension
+// kSolveBlock, zero outside jb x jb) for the unknowns w (in/out, shared); rdiag holds
+// the reciprocals of the diagonal.
 template <typename T>
 __device__ void warp_lower_solve(const T* D, const double* rdiag, int jb, double* w) {
   const int lane = threadIdx.x & 31;
   double x[kSolveBlock / 32];
 #pragma unroll
   for (int q = 0; q < kSolveBlock / 32; ++q) x[q] = (lane + 32 * q < jb) ? w[lane + 32 * q] : 0.0;
-#pragma unroll 4
-  for (int cidx = 0; cidx < jb; ++cidx) {
-    double dcol[kSolveBlock / 32];
 #pragma unroll
-    for (int q = 0; q < kSolveBlock / 32; ++q) dcol[q] = (double)D[lane + 32 * q + cidx * kSolveBlock];
-    const int owner = cidx & 31, slot = cidx >> 5;
-    double xc = x[0];
+  for (int slot = 0; slot < kSolveBlock / 32; ++slot) {
 #pragma unroll
-    for (int q = 1; q < kSolveBlock / 32; ++q)
-      if (q == slot) xc = x[q];
-    xc = __shfl_sync(0xffffffffu, xc, owner) * rdiag[cidx];
+    for (int o = 0; o < 32; ++o) {
+      const int cidx = slot * 32 + o;
+      if (cidx < jb) {
+        const double xc = __shfl_sync(0xffffffffu, x[slot], o) * rdiag[cidx];
+        if (lane == o) x[slot] = xc;
 #pragma unroll
-    for (int q = 0; q < kSolveBlock / 32; ++q) {
-      const int r = lane + 32 * q;
-      if (r == cidx) x[q] = xc;
-      else if (r > cidx) x[q] = fma(-dcol[q], xc, x[q]);
+        for (int q = slot; q < kSolveBlock / 32; ++q) {
+          const int r = lane + 32 * q;
+          if (r > cidx) x[q] = fma(-(double)D[r + cidx * kSolveBlock], xc, x[q]);
+        }
+      }
     }
   }
 #pragma unroll
@@ -717,21 +744,19 @@ __device__ void warp_upper_unit_solve(const T* D, int jb, double* w) {
   double x[kSolveBlock / 32];
 #pragma unroll
   for (int q = 0; q < kSolveBlock / 32; ++q) x[q] = (lane + 32 * q < jb) ? w[lane + 32 * q] : 0.0;
-#pragma unroll 4
-  for (int cidx = jb - 1; cidx >= 0; --cidx) {
-    double dcol[kSolveBlock / 32];
 #pragma unroll
-    for (int q = 0; q < kSolveBlock / 32; ++q) dcol[q] = (double)D[lane + 32 * q + cidx * kSolveBlock];
-    const int owner = cidx & 31, slot = cidx >> 5;
-    double xc = x[0];
+  for (int slot = kSolveBlock / 32 - 1; slot >= 0; --slot) {
 #pragma unroll
-    for (int q = 1; q < kSolveBlock / 32; ++q)
-      if (q == slot) xc = x[q];
-    xc = __shfl_sync(0xffffffffu, xc, owner);
+    for (int o = 31; o >= 0; --o) {
+      const int cidx = slot * 32 + o;
+      if (cidx < jb) {
+        const double xc = __shfl_sync(0xffffffffu, x[slot], o);
 #pragma unroll
-    for (int q = 0; q < kSolveBlock / 32; ++q) {
-      const int r = lane + 32 * q;
-      if (r < cidx) x[q] = fma(-dcol[q], xc, x[q]);
+        for (int q = 0; q <= slot; ++q) {
+          const int r = lane + 32 * q;
+          if (r < cidx) x[q] = fma(-(double)D[r + cidx * kSolveBlock], xc, x[q]);
+        }
+      }
     }
   }
 #pragma unroll
@@ -739,211 +764,169 @@ __device__ void warp_upper_unit_solve(const T* D, int jb, double* w) {
     if (lane + 32 * q < jb) w[lane + 32 * q] = x[q];
 }
 
-// Forward step: every CTA subtracts the (final) unknowns of block [j0, j0+jb) from its
-// 128 rows of b below the block (4 threads per row, 32 columns each, all loads issued
-// at once); CTA 0, whose rows are the next block [jn, jn+jnb), then solves that block.
-// jb = 0 skips the update (first block).
-template <typename T>
-__global__ void __launch_bounds__(512) fwd_step_kernel(const T* __restrict__ S, int64_t lda, int n, int j0, int jb,
-                                                       int jn, int jnb, double* b) {
+// One sweep of blocked substitution over the 128-row blocks of S in one cooperative
+// launch.  UPPER = false: forward with S's lower triangle (non-unit diagonal), blocks
+// first to last; UPPER = true: backward with S's strict upper triangle (unit diagonal),
+// blocks last to first.  Step s solves block k(s) and is owned by CTA s % G, which also
+// owns the rows of that block: as soon as block k(s) is published (flags[s] = tag,
+// release/acquire at gpu scope) every CTA subtracts S(its rows, block k(s)) * y_k(s)
+// from its blocks' rows of b (128 x 128 tiles, contiguous column segments), the owner
+// of step s+1 first, and that owner then solves and publishes block k(s+1) before it
+// turns to its other blocks.  The dependent chain is one tile GEMV and one warp solve
+// per block; the rest of the factor streams from HBM alongside.  Diagonal blocks are
+// staged into shared memory one owned step ahead.  A wait that exceeds 2 s records
+// BEM_ERR_TIMEOUT in *status and ends the CTA.
+template <typename T, bool UPPER>
+__global__ void __launch_bounds__(kSweepThreads, 1)
+    sweep_kernel(const T* __restrict__ S, int64_t lda, int n, double* b, unsigned* flags, unsigned tag,
+                 int* status) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* D = reinterpret_cast<T*>(smem_raw);  // [kSolveBlock][kSolveBlock] column-major
-  __shared__ double wb[kSolveBlock];
+  __shared__ double ys[kSolveBlock];
   __shared__ double wn[kSolveBlock];
   __shared__ double rdiag[kSolveBlock];
   __shared__ double red[4][kSolveBlock];
-  const int t = threadIdx.x;
-  const int rl = t & (kSolveBlock - 1), qtr = t >> 7;
-  const int64_t r = (int64_t)jn + (int64_t)blockIdx.x * kSolveBlock + rl;
-  if (jb > 0) {
-    if (t < jb) wb[t] = b[j0 + t];
+  __shared__ int s_abort;
+  const int t = threadIdx.x, G = gridDim.x, g = blockIdx.x;
+  const int nblk = (n + kSolveBlock - 1) / kSolveBlock;
+  auto blk0 = [&](int s) { return (UPPER ? nblk - 1 - s : s) * kSolveBlock; };
+  auto stage_diag = [&](int s) {
+    const int k0 = blk0(s), kb = min(kSolveBlock, n - k0);
+    if (UPPER)
+      stage_block<T>(D, kSolveBlock, S + k0 + (int64_t)k0 * lda, lda, kb, kb, kSolveBlock, kSolveBlock,
+                     [](int r, int c) { return r < c; });
+    else
+      stage_block<T>(D, kSolveBlock, S + k0 + (int64_t)k0 * lda, lda, kb, kb, kSolveBlock, kSolveBlock,
+                     [](int r, int c) { return r >= c; });
+  };
+  auto solve = [&](int s) {
+    const int k0 = blk0(s), kb = min(kSolveBlock, n - k0);
+    if (t < kb) wn[t] = b[k0 + t];
+    if (!UPPER && t < kSolveBlock) rdiag[t] = (t < kb) ? 1.0 / (double)D[t + t * kSolveBlock] : 0.0;
     __syncthreads();
-    double acc = 0.0;
-    if (r < n) {
-      const int cb = qtr * 32;
-      const T* p = S + r + (int64_t)(j0 + cb) * lda;
-      T a[32];
-#pragma unroll
-      for (int u = 0; u < 32; ++u) a[u] = (cb + u < jb) ? p[(int64_t)u * lda] : T(0);
-#pragma unroll
-      for (int u = 0; u < 32; ++u) acc = fma((double)a[u], (cb + u < jb) ? wb[cb + u] : 0.0, acc);
+    if (t < 32) {
+      if (UPPER)
+        warp_upper_unit_solve<T>(D, kb, wn);
+      else
+        warp_lower_solve<T>(D, rdiag, kb, wn);
     }
-    red[qtr][rl] = acc;
     __syncthreads();
-    if (qtr == 0 && r < n) b[r] -= (red[0][rl] + red[1][rl]) + (red[2][rl] + red[3][rl]);
-  }
-  if (blockIdx.x != 0 || jnb <= 0) return;
-  __syncthreads();  // this CTA's updates of rows [jn, jn+jnb) are visible to the block
-  stage_block<T>(D, kSolveBlock, S + jn + (int64_t)jn * lda, lda, jnb, jnb, kSolveBlock, kSolveBlock,
-                 [](int rr, int cc) { return rr >= cc; });
-  if (t < jnb) wn[t] = b[jn + t];
-  __syncthreads();
-  if (t < kSolveBlock) rdiag[t] = (t < jnb) ? 1.0 / (double)D[t + t * kSolveBlock] : 0.0;
-  __syncthreads();
-  if (t < 32) warp_lower_solve<T>(D, rdiag, jnb, wn);
-  __syncthreads();
-  if (t < jnb) b[jn + t] = wn[t];
-}
+    if (t < kb) b[k0 + t] = wn[t];
+    __syncthreads();
+    if (t == 0) {
+      __threadfence();
+      st_release_u32(flags + s, tag);
+    }
+    if (s + G < nblk) stage_diag(s + G);  // D is free again: the next owned block
+  };
 
-// Backward, off-block part: part[chunk][t] = sum over the chunk's 512 columns c' >= c0
-// of S(j0+t, c') v[c'] for the block's rows t < jb.  A warp reads one column's rows
-// with 16-byte loads (each lane 16 bytes of rows), the 8 warps of a CTA take columns
-// 8 apart, and their per-row partials meet in shared memory.
-template <typename T>
-__global__ void __launch_bounds__(256) bwd_dot_kernel(const T* __restrict__ S, int64_t lda, int n, int j0, int jb,
-                                                      int c0, const double* v, double* part) {
-  constexpr int RPL = 16 / sizeof(T);            // rows per lane per 16-byte load
-  constexpr int LANES = kSolveBlock / RPL;       // lanes that cover the 128 rows
-  __shared__ double red[8][kSolveBlock];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int cs = c0 + blockIdx.x * 512;
-  const int ce = min(n, cs + 512);
-  double acc[RPL];
-#pragma unroll
-  for (int q = 0; q < RPL; ++q) acc[q] = 0.0;
-  // 16-byte loads need the block's rows aligned; jb is the full 128 except for the
-  // very last (partial) block, which takes the scalar path
-  const bool vec = (jb == kSolveBlock) && ((((uintptr_t)(S + j0)) & 15) == 0) && ((lda * sizeof(T)) % 16 == 0);
-  for (int g = 0; g < 2; ++g) {
-    // lanes [0, LANES) cover the rows; with FP32 (LANES = 32) one column per warp, with
-    // FP64 (LANES = 64) a column spans two passes g
-    const int lane_row = lane + 32 * g;
-    if (lane_row >= LANES) break;
-    const int r0 = lane_row * RPL;
-#pragma unroll 16
-    for (int cc = cs + warp; cc < ce; cc += 8) {
-      const double vc = v[cc];
-      const T* p = S + (j0 + r0) + (int64_t)cc * lda;
-      if (vec) {
-        if (sizeof(T) == 4) {
-          const float4 a = *reinterpret_cast<const float4*>(p);
-          acc[0] = fma((double)a.x, vc, acc[0]);
-          acc[1 % RPL] = fma((double)a.y, vc, acc[1 % RPL]);
-          acc[2 % RPL] = fma((double)a.z, vc, acc[2 % RPL]);
-          acc[3 % RPL] = fma((double)a.w, vc, acc[3 % RPL]);
-        } else {
-          const double2 a = *reinterpret_cast<const double2*>(p);
-          acc[0] = fma(a.x, vc, acc[0]);
-          acc[1 % RPL] = fma(a.y, vc, acc[1 % RPL]);
+  if (t == 0) s_abort = 0;
+  if (g < nblk) stage_diag(g);
+  __syncthreads();
+  if (g == 0) solve(0);
+  const int rl = t & (kSolveBlock - 1), q = t >> 7;
+  for (int s = 0; s + 1 < nblk; ++s) {
+    int s2 = s + 1 + ((g - (s + 1)) % G + G) % G;  // this CTA's first step after s
+    if (s2 >= nblk) break;                          // no rows left to update
+    if (t == 0 && s % G != g) {
+      const unsigned long long t0 = globaltimer_ns();
+      unsigned it = 0;
+      while (ld_acquire_u32(flags + s) != tag) {
+        if ((++it & 255u) == 0 && globaltimer_ns() - t0 > 2000000000ull) {
+          atomicExch(status, BEM_ERR_TIMEOUT);
+          s_abort = 1;
+          break;
         }
-      } else {
-#pragma unroll
-        for (int q = 0; q < RPL; ++q)
-          if (r0 + q < jb) acc[q] = fma((double)p[q], vc, acc[q]);
       }
+      __threadfence();
     }
-    if (sizeof(T) == 8 || g == 0) {
+    __syncthreads();
+    if (s_abort) return;
+    const int c0 = blk0(s), cb = min(kSolveBlock, n - c0);
+    if (t < kSolveBlock) ys[t] = (t < cb) ? __ldcg(b + c0 + t) : 0.0;
+    __syncthreads();
+    for (; s2 < nblk; s2 += G) {
+      const int r0 = blk0(s2), rb = min(kSolveBlock, n - r0);
+      double acc = 0.0;
+      // the row's current value travels with the tile's loads (only this thread writes it)
+      const double bold = (q == 0 && rl < rb) ? b[r0 + rl] : 0.0;
+      if (rl < rb) {
+        const int cq = 32 * q;
+        const T* p = S + (r0 + rl) + (int64_t)(c0 + cq) * lda;
+        T a[32];
 #pragma unroll
-      for (int q = 0; q < RPL; ++q) red[warp][r0 + q] = acc[q];
+        for (int u = 0; u < 32; ++u) a[u] = (cq + u < cb) ? p[(int64_t)u * lda] : T(0);
 #pragma unroll
-      for (int q = 0; q < RPL; ++q) acc[q] = 0.0;
-    }
-  }
-  __syncthreads();
-  if (threadIdx.x < kSolveBlock) {
-    double s0 = 0.0;
-#pragma unroll
-    for (int w = 0; w < 8; ++w) s0 += red[w][threadIdx.x];
-    part[(int64_t)blockIdx.x * kSolveBlock + threadIdx.x] = s0;
-  }
-}
-
-// Backward, block part: reduce the partial sums, solve the block's unit upper part with
-// one warp, and after the panel's first block apply the panel's interchanges
-// (in reverse order) when do_swaps is set.
-template <typename T>
-__global__ void __launch_bounds__(256) bwd_finish_kernel(const T* __restrict__ S, int64_t lda, int j0, int jb,
-                                                         int nchunk, const double* part, const int* piv,
-                                                         int do_swaps, int p0, int pb, double* v) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* D = reinterpret_cast<T*>(smem_raw);
-  __shared__ double w[kSolveBlock];
-  const int t = threadIdx.x;
-  stage_block<T>(D, kSolveBlock, S + j0 + (int64_t)j0 * lda, lda, jb, jb, kSolveBlock, kSolveBlock,
-                 [](int r, int cc) { return r < cc; });
-  if (t < jb) {
-    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    int k = 0;
-    for (; k + 8 <= nchunk; k += 8) {
-#pragma unroll
-      for (int u = 0; u < 8; ++u) acc[u] += part[(int64_t)(k + u) * kSolveBlock + t];
-    }
-    for (; k < nchunk; ++k) acc[0] += part[(int64_t)k * kSolveBlock + t];
-    w[t] = v[j0 + t] - (((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7])));
-  }
-  __syncthreads();
-  if (t < 32) warp_upper_unit_solve<T>(D, jb, w);
-  __syncthreads();
-  if (t < jb) v[j0 + t] = w[t];
-  if (!do_swaps) return;
-  __syncthreads();
-  if (t == 0) {
-    __threadfence_block();
-    for (int q = pb - 1; q >= 0; --q) {
-      const int p = piv[p0 + q];
-      if (p != p0 + q) {
-        const double a = v[p0 + q];
-        v[p0 + q] = v[p];
-        v[p] = a;
+        for (int u = 0; u < 32; ++u) acc = fma((double)a[u], ys[cq + u], acc);
       }
+      red[q][rl] = acc;
+      __syncthreads();
+      if (q == 0 && rl < rb) b[r0 + rl] = bold - ((red[0][rl] + red[1][rl]) + (red[2][rl] + red[3][rl]));
+      __syncthreads();
+      if (s2 == s + 1) solve(s2);
     }
   }
 }
 
-template <typename T>
-int lu_solve_ws(bem_ctx* c, const T* S, int64_t lda, int n, const int* piv, int nb, double* b, double* work) {
-  // triangular blocks of kSolveBlock; the interchanges are applied per factorisation
-  // panel of width nb (the product form of the factors)
-  const int db = kSolveBlock;
-  const size_t dsm = (size_t)db * db * sizeof(T);
-  static int attr = 0;
-  const int bit = sizeof(T) == 8 ? 1 : 2;
-  if (!(attr & bit)) {
-    cudaFuncSetAttribute(fwd_step_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm);
-    cudaFuncSetAttribute(bwd_finish_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm);
-    attr |= bit;
+__global__ void permute_kernel(int n, const int* __restrict__ perm, const double* __restrict__ v,
+                               double* __restrict__ x) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) x[i] = v[perm[i]];
+}
+
+template <typename T, bool UPPER>
+int sweep_launch(bem_ctx* c, const T* S, int64_t lda, int n, double* b, unsigned* flags, unsigned tag,
+                 int* status) {
+  static int grid[2][2] = {{0, 0}, {0, 0}};  // CTAs per SM, per (T, direction)
+  const size_t dsm = (size_t)kSolveBlock * kSolveBlock * sizeof(T);
+  int& per_sm = grid[sizeof(T) == 8][UPPER ? 1 : 0];
+  if (per_sm == 0) {
+    BEM_CUDA(c, cudaFuncSetAttribute(sweep_kernel<T, UPPER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm));
+    BEM_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_kernel<T, UPPER>, kSweepThreads, dsm));
+    if (per_sm < 1) return bem_fail(c, BEM_ERR_CUDA, "triangular sweep kernel does not fit on an SM");
   }
-  // forward: launch k updates with block k-1 and solves block k
-  for (int jn = 0, j0 = 0, jb = 0; jn < n; j0 = jn, jn += db) {
-    const int jnb = std::min(db, n - jn);
-    jb = (jn == 0) ? 0 : std::min(db, n - j0);
-    const int rows = n - jn;
-    fwd_step_kernel<T><<<(rows + kSolveBlock - 1) / kSolveBlock, 512, dsm, c->stream>>>(S, lda, n, j0, jb, jn, jnb,
-                                                                                      b);
-    BEM_LAUNCH_CHECK(c);
-  }
-  const int last_panel = ((n - 1) / nb) * nb;
-  for (int p0 = last_panel; p0 >= 0; p0 -= nb) {
-    const int pb = std::min(nb, n - p0);
-    const int last_blk = p0 + ((pb - 1) / db) * db;
-    for (int j0 = last_blk; j0 >= p0; j0 -= db) {
-      const int jb = std::min(db, p0 + pb - j0);
-      const int c0 = j0 + jb;
-      const int nchunk = (n - c0 + 511) / 512;
-      if (nchunk > 0) {
-        bwd_dot_kernel<T><<<nchunk, 256, 0, c->stream>>>(S, lda, n, j0, jb, c0, b, work);
-        BEM_LAUNCH_CHECK(c);
-      }
-      bwd_finish_kernel<T><<<1, 256, dsm, c->stream>>>(S, lda, j0, jb, nchunk, work, piv, j0 == p0 ? 1 : 0, p0, pb, b);
-      BEM_LAUNCH_CHECK(c);
-    }
-  }
+  const int nblk = (n + kSolveBlock - 1) / kSolveBlock;
+  const int G = std::min(nblk, c->sm_count);  // one CTA per SM: the whole diagonal block in smem
+  void* args[] = {(void*)&S, (void*)&lda, (void*)&n, (void*)&b, (void*)&flags, (void*)&tag, (void*)&status};
+  BEM_CUDA(c, cudaLaunchCooperativeKernel((void*)sweep_kernel<T, UPPER>, dim3(G), dim3(kSweepThreads), args, dsm,
+                                          c->stream));
+  ++c->launches;
   return BEM_OK;
 }
 
 template <typename T>
-int lu_solve(bem_ctx* c, const T* S, int64_t lda, int n, const int* piv, int nb, double* b) {
+int lu_solve_ws(bem_ctx* c, const T* S, int64_t lda, int n, const int* perm, double* b, double* work) {
+  // work: [0, n) gather buffer, then the per-block flags and the status word
+  const int nblk = (n + kSolveBlock - 1) / kSolveBlock;
+  unsigned* flags = reinterpret_cast<unsigned*>(work + n);
+  int* status = reinterpret_cast<int*>(flags + nblk);
+  BEM_CUDA(c, cudaMemsetAsync(flags, 0, (nblk + 1) * sizeof(unsigned), c->stream));
+  int rc;
+  if ((rc = sweep_launch<T, false>(c, S, lda, n, b, flags, 1u, status))) return rc;
+  if ((rc = sweep_launch<T, true>(c, S, lda, n, b, flags, 2u, status))) return rc;
+  permute_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(n, perm, b, work);
+  BEM_LAUNCH_CHECK(c);
+  BEM_CUDA(c, cudaMemcpyAsync(b, work, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  int st = 0;
+  BEM_CUDA(c, cudaMemcpyAsync(&st, status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  BEM_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (st != 0) return bem_fail(c, st, "triangular solve: a wait for a solved block timed out");
+  return BEM_OK;
+}
+
+template <typename T>
+int lu_solve(bem_ctx* c, const T* S, int64_t lda, int n, const int* perm, double* b) {
   const size_t need = lu_solve_work_count(n);
   if (c->work.count < need) {
     c->work.release();
     BEM_CUDA(c, c->work.alloc(need));
   }
-  return lu_solve_ws<T>(c, S, lda, n, piv, nb, b, c->work.p);
+  return lu_solve_ws<T>(c, S, lda, n, perm, b, c->work.p);
 }
 
-template int lu_solve<double>(bem_ctx*, const double*, int64_t, int, const int*, int, double*);
-template int lu_solve_ws<double>(bem_ctx*, const double*, int64_t, int, const int*, int, double*, double*);
-template int lu_solve<float>(bem_ctx*, const float*, int64_t, int, const int*, int, double*);
+template int lu_solve<double>(bem_ctx*, const double*, int64_t, int, const int*, double*);
+template int lu_solve_ws<double>(bem_ctx*, const double*, int64_t, int, const int*, double*, double*);
+template int lu_solve<float>(bem_ctx*, const float*, int64_t, int, const int*, double*);
 
 // ---------------------------------------------------------------------------------
 // residual r = b - A x (FP64) with infinity norms
@@ -1051,7 +1034,8 @@ int lu_factor_fp64(bem_ctx* c, double* A, int64_t lda, int n, int* d_piv, int* i
   BEM_CUDA(c, cudaEventCreate(&e0));
   BEM_CUDA(c, cudaEventCreate(&e1));
   BEM_CUDA(c, cudaEventRecord(e0, c->stream));
-  int rc = lu_factor<double>(c, A, lda, n, d_piv, kNbFp64, info);
+  BEM_CUDA(c, c->perm.alloc(n));
+  int rc = lu_factor<double>(c, A, lda, n, d_piv, c->perm.p, kNbFp64, info);
   BEM_CUDA(c, cudaEventRecord(e1, c->stream));
   BEM_CUDA(c, cudaEventSynchronize(e1));
   float ms = 0.f;
@@ -1062,8 +1046,8 @@ int lu_factor_fp64(bem_ctx* c, double* A, int64_t lda, int n, int* d_piv, int* i
   return rc;
 }
 
-int lu_solve_fp64(bem_ctx* c, const double* LU, int64_t lda, int n, const int* d_piv, double* b) {
-  return lu_solve<double>(c, LU, lda, n, d_piv, kNbFp64, b);
+int lu_solve_fp64(bem_ctx* c, const double* LU, int64_t lda, int n, double* b) {
+  return lu_solve<double>(c, LU, lda, n, c->perm.p, b);
 }
 
 }  // namespace bem

@@ -5,12 +5,12 @@
 // Layout.  The matrix S is the reference's column-major A (lda >= n).  The
 // factorisation is of T = S^T with row pivoting, i.e. column pivoting of S, so that
 // every pivot swap and every panel load touches contiguous column segments of S:
-//   T = P_1 L_1 P_2 L_2 ... P_K L_K U      (product form, one factor per NB panel)
-// with U in the lower triangle of S (diagonal included) and the unit multipliers of
-// panel k in the strict upper part of S's rows [j0, j0+NB).  Swaps of a panel are not
-// applied to the multipliers of earlier panels (their rows of S), so the solve
-// applies P_k panel by panel:
-//   S x = b  ->  x = P_1 L_1^{-T} P_2 L_2^{-T} ... P_K L_K^{-T} U^{-T} b.
+//   T = P L U,   P = tau_0 tau_1 ... tau_{n-1}   (tau_i swaps rows i and piv[i])
+// with U in the lower triangle of S (diagonal included) and the unit multipliers L in
+// the strict upper triangle of S; every panel's swaps are applied to all other rows
+// of S, the earlier panels' multipliers included (LAPACK's dgetrf convention for T).
+// The solve is two substitution sweeps and one gather:
+//   S x = b  ->  x = P L^{-T} U^{-T} b,   (P v)[i] = v[perm[i]].
 // LU of A^T with partial pivoting is as stable as that of A; info follows DGESV (the
 // 1-based step of the first exactly zero pivot).
 #pragma once
@@ -45,16 +45,21 @@ LUWorkspace lu_workspace_carve(void* base, int n, int nb, int gmax, int elem);
 // doubles of triangular-solve scratch for order n
 size_t lu_solve_work_count(int n);
 
+// piv: the 0-based pivot rows of T; perm (n ints, nullable): the gather form of P
+// that the solve takes, written when the factorisation succeeds (a host round trip)
 template <typename T>
-int lu_factor_ws(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int nb, int* info, const LUWorkspace& ws);
+int lu_factor_ws(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int* perm, int nb, int* info,
+                 const LUWorkspace& ws);
+// b (device, FP64) := S^{-1} b; work: lu_solve_work_count(n) doubles.  Synchronises
+// the stream to read the sweeps' status word.
 template <typename T>
-int lu_solve_ws(bem_ctx* c, const T* S, int64_t lda, int n, const int* piv, int nb, double* b, double* work);
+int lu_solve_ws(bem_ctx* c, const T* S, int64_t lda, int n, const int* perm, double* b, double* work);
 
 template <typename T>
-int lu_factor(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int nb, int* info);
+int lu_factor(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int* perm, int nb, int* info);
 
 template <typename T>
-int lu_solve(bem_ctx* c, const T* S, int64_t lda, int n, const int* piv, int nb, double* b);
+int lu_solve(bem_ctx* c, const T* S, int64_t lda, int n, const int* perm, double* b);
 
 // y = b - A x (FP64 A, column-major) and the infinity norms of y; |A| row sums on request
 int residual_fp64(bem_ctx* c, const double* A, int64_t lda, int n, const double* x, const double* b,

@@ -7,9 +7,10 @@
 // or adjoint loop that must not pay for cudaMalloc/cudaFree (both may synchronise the
 // whole device); an application that runs under a fixed memory budget set at start
 // up.  For them this entry point takes its scratch (the panel kernel's candidate
-// exchange and grid-barrier words, the TRSM inverse, the TRSM buffer and the
-// triangular-solve partial sums) from one file-scope __device__ array of
-// kNoAllocBytes (4.5 MiB), sized for systems of order up to kNoAllocMaxN = 4096.
+// exchange and grid-barrier words, the TRSM inverse, the TRSM buffer, the triangular
+// sweeps' gather buffer and flags, and the pivot permutation) from one file-scope
+// __device__ array of kNoAllocBytes (4.3 MiB), sized for systems of order up to
+// kNoAllocMaxN = 4096.
 //
 // Rules that follow from the shared static array:
 //   * every GPU that loads the library holds the array until the process exits;
@@ -36,7 +37,8 @@ constexpr size_t kFactorBytes = up256(2 * kNoAllocGmax * sizeof(double)) + up256
                                 up256((size_t)kNoAllocNb * kNoAllocNb * 8) +
                                 up256((size_t)kNoAllocMaxN * kNoAllocNb * 8);
 constexpr size_t kSolveDoubles = ((size_t)kNoAllocMaxN + 127) / 128 * 256 + 256;
-constexpr size_t kNoAllocBytes = kFactorBytes + up256(kSolveDoubles * sizeof(double));
+constexpr size_t kPermBytes = up256((size_t)kNoAllocMaxN * sizeof(int));
+constexpr size_t kNoAllocBytes = kFactorBytes + up256(kSolveDoubles * sizeof(double)) + kPermBytes;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
@@ -75,11 +77,12 @@ extern "C" int bem_dgesv_noalloc(int n, int nrhs, double* dA, int lda, int* d_ip
   cudaDeviceGetAttribute(&c.sm_count, cudaDevAttrMultiProcessorCount, dev);
   const bem::LUWorkspace ws = bem::lu_workspace_carve(base, n, kNoAllocNb, kNoAllocGmax, sizeof(double));
   double* solve_work = reinterpret_cast<double*>(base + kFactorBytes);
-  int rc = bem::lu_factor_ws<double>(&c, dA, lda, n, d_ipiv, kNoAllocNb, info, ws);
+  int* perm = reinterpret_cast<int*>(base + kFactorBytes + up256(kSolveDoubles * sizeof(double)));
+  int rc = bem::lu_factor_ws<double>(&c, dA, lda, n, d_ipiv, perm, kNoAllocNb, info, ws);
   if (rc) return rc;
   if (*info == 0)
     for (int j = 0; j < nrhs; ++j)
-      if ((rc = bem::lu_solve_ws<double>(&c, dA, lda, n, d_ipiv, kNoAllocNb, dB + (int64_t)j * ldb, solve_work)))
+      if ((rc = bem::lu_solve_ws<double>(&c, dA, lda, n, perm, dB + (int64_t)j * ldb, solve_work)))
         return rc;
   one_based_kernel<<<(n + 255) / 256, 256, 0, c.stream>>>(n, d_ipiv);
   if (cudaGetLastError() != cudaSuccess) return BEM_ERR_CUDA;

@@ -93,6 +93,7 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
     if (e != cudaSuccess) return bem_fail(c, BEM_ERR_OOM, "allocating the FP32 factor copy");
   }
   BEM_CUDA(c, c->piv.alloc(n));
+  BEM_CUDA(c, c->perm.alloc(n));
   DBuf<double> r, d;
   BEM_CUDA(c, r.alloc(n));
   BEM_CUDA(c, d.alloc(n));
@@ -117,7 +118,7 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
     c->f32_gemm = c->f32_gemm_override;
   else
     c->f32_gemm = (precision == BEM_PREC_BF16_IR) ? 1 : 4;
-  int rc = lu_factor<float>(c, c->A32.p, lda, n, c->piv.p, kNbMixed, info);
+  int rc = lu_factor<float>(c, c->A32.p, lda, n, c->piv.p, c->perm.p, kNbMixed, info);
   c->f32_gemm = saved;
   if (rc) return rc;
   BEM_CUDA(c, cudaEventRecord(e1, c->stream));
@@ -141,7 +142,7 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
     for (it = 1; it <= max_iter; ++it) {
       if (ir_prof) cudaEventRecord(q0, c->stream);
       BEM_CUDA(c, cudaMemcpyAsync(d.p, r.p, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-      if ((rc = lu_solve<float>(c, c->A32.p, lda, n, c->piv.p, kNbMixed, d.p))) return rc;
+      if ((rc = lu_solve<float>(c, c->A32.p, lda, n, c->perm.p, d.p))) return rc;
       axpy_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(n, d.p, c->X.p);
       BEM_LAUNCH_CHECK(c);
       if (ir_prof) cudaEventRecord(q1, c->stream);
@@ -205,7 +206,7 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
       prev = berr;
       // v0 = M^{-1} r / beta
       BEM_CUDA(c, cudaMemcpyAsync(V, r.p, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-      if ((rc = lu_solve<float>(c, c->A32.p, lda, n, c->piv.p, kNbMixed, V))) return rc;
+      if ((rc = lu_solve<float>(c, c->A32.p, lda, n, c->perm.p, V))) return rc;
       double beta = 0.0;
       if ((rc = norm2(V, &beta))) return rc;
       if (!(beta > 0.0)) break;
@@ -218,7 +219,7 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
         double* w = V + (int64_t)(j + 1) * ldv;
         // w = M^{-1} A v_j  (residual_fp64 with b = 0 gives -A v_j)
         if ((rc = residual_fp64(c, c->A.p, lda, n, V + (int64_t)j * ldv, zero.p, w, norms, false))) return rc;
-        if ((rc = lu_solve<float>(c, c->A32.p, lda, n, c->piv.p, kNbMixed, w))) return rc;
+        if ((rc = lu_solve<float>(c, c->A32.p, lda, n, c->perm.p, w))) return rc;
         scale_kernel<<<vb, 256, 0, c->stream>>>(n, -1.0, w, w);
         BEM_LAUNCH_CHECK(c);
         // classical Gram-Schmidt, twice

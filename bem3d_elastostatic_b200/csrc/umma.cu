@@ -7,9 +7,13 @@
 // K chunks into 128-byte-swizzled shared memory.  One thread issues, per K chunk and
 // per 16-wide K step, the three products hi*hi + hi*lo + lo*hi as tcgen05.mma
 // (kind::f16, BF16 inputs, FP32 accumulation in tensor memory, M = 128, N = 256); a
-// tcgen05.commit signals an mbarrier when they are done, and four warps drain the
-// 128 x 256 accumulator with tcgen05.ld (one TMEM lane = one row of C) into a
-// coalesced read-modify-write of C.
+// tcgen05.commit signals an mbarrier when they are done, and eight warps drain the
+// 128 x 256 accumulator with tcgen05.ld (one TMEM lane = one row of C): they stage
+// -acc for 128 x 32 boxes in shared memory and add each box into C with a bulk tensor
+// reduction (cp.reduce.async.bulk.tensor .add.f32), so the L2 performs the
+// read-modify-write of C and the SM never waits on a load of C.  Every element of C
+// receives exactly one addition per call, C + (-acc), the same IEEE operation as
+// C - acc: the result is deterministic.
 //
 // Every mbarrier wait is bounded: on timeout the kernel records an error word, the
 // other roles stop at their next wait, the producer waits (bounded) for its own copies
@@ -35,7 +39,8 @@ constexpr int kStages = 2;              // shared-memory ring of K chunks
 constexpr int A_TILE = UM * UK * 2;     // 16 KB
 constexpr int B_TILE = UN * UK * 2;     // 32 KB
 constexpr int STAGE = 2 * A_TILE + 2 * B_TILE;  // hi + lo of A and B: 96 KB
-constexpr int kSmem = kStages * STAGE + 1024 + 256;
+constexpr int kStg = 2 * 32 * UM * 4;  // two 128 x 32 FP32 staging boxes (one per epilogue half)
+constexpr int kSmem = kStages * STAGE + 1024 + 256 + kStg;
 constexpr unsigned kTmemCols = 512;     // two 128 x 256 FP32 accumulators
 constexpr int kEpiThreads = 256;        // 8 epilogue warps
 constexpr int kThreads = 64 + kEpiThreads;
@@ -81,14 +86,13 @@ __device__ __forceinline__ void umma_commit(unsigned bar) {
 
 // Persistent, warp-specialised: warp 0 (one lane) streams K chunks with TMA through a
 // two-stage ring, warp 1 (one lane) issues the MMAs into one of two TMEM accumulators,
-// warps 2-9 drain the other accumulator into C, so the read-modify-write of one tile
+// warps 2-9 drain the other accumulator into C, so the update of C by one tile
 // overlaps the loads and MMAs of the next.  Tiles run m-fastest so a CTA wave shares
-// the B operand band; C is read and written with streaming (evict-first) hints so it
-// does not push the operands out of L2.
+// the B operand band.
 __global__ void __launch_bounds__(kThreads, 1)
     umma_update_kernel(const __grid_constant__ CUtensorMap tAh, const __grid_constant__ CUtensorMap tAl,
-                       const __grid_constant__ CUtensorMap tBh, const __grid_constant__ CUtensorMap tBl, int M,
-                       int N, int K, float* C, int64_t ldc, int* err) {
+                       const __grid_constant__ CUtensorMap tBh, const __grid_constant__ CUtensorMap tBl,
+                       const __grid_constant__ CUtensorMap tC, int M, int N, int K, int* err) {
   extern __shared__ __align__(16) unsigned char umma_smem[];
   const unsigned raw = smem_u32(umma_smem);
   const unsigned base = (raw + 1023u) & ~1023u;  // 1024-byte aligned operand tiles
@@ -233,39 +237,36 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     __syncwarp();
   } else {
-    // 8 epilogue warps: warp w reads TMEM lane quarter (w % 4) and one half of the
-    // 256 columns; each chunk's C loads are issued before the previous chunk is stored,
-    // keeping ~64 loads per thread in flight (the C stream is latency-bound otherwise)
+    // 8 epilogue warps: warp w reads TMEM lane quarter (w % 4) of one half (128
+    // columns) of the accumulator, 32 columns at a time; the 4 warps of a half fill
+    // that half's staging box and its leader thread issues the box's reduction
     const int lq = warp & 3;
     const int half = (warp - 2) >> 2;  // 0 or 1
+    float* stg = reinterpret_cast<float*>(gbase + kStages * STAGE + 256) + half * (32 * UM);
+    const unsigned stg_s = smem_u32(stg);
+    const bool leader = (lq == 0 && lane == 0);
     int ab = 0;
     unsigned aphase = 0;
+    bool pending = false;
     for (int t = blockIdx.x; t < total && !*abort_flag; t += gridDim.x) {
       const int m0 = (t % tiles_m) * UM, n0 = (t / tiles_m) * UN;
-      if (!mbar_wait(smem_u32(&tfull[ab]), aphase, abort_flag)) {
+      // the four warps of a half leave together (they meet at named barriers below)
+      const int ok = mbar_wait(smem_u32(&tfull[ab]), aphase, abort_flag) ? 1 : 0;
+      int all_ok;
+      asm volatile(
+          "{\n\t.reg .pred p, q;\n\tsetp.ne.b32 p, %1, 0;\n\t"
+          "bar.red.and.pred q, %2, 128, p;\n\tselp.b32 %0, 1, 0, q;\n\t}\n"
+          : "=r"(all_ok)
+          : "r"(ok), "r"(1 + half)
+          : "memory");
+      if (!all_ok) {
         fail();
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const int row = m0 + lq * 32 + lane;
-      const bool rok = row < M;
-      float cur[32], nxt[32];
-      const int cbase = n0 + half * (UN / 2);
-#pragma unroll
-      for (int j = 0; j < 32; ++j) {
-        const int col = cbase + j;
-        cur[j] = (rok && col < N) ? __ldcs(C + row + (int64_t)col * ldc) : 0.f;
-      }
 #pragma unroll 1
       for (int q = 0; q < UN / 64; ++q) {
         const int j0 = half * (UN / 2) + 32 * q;
-        if (q + 1 < UN / 64) {
-#pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            const int col = n0 + j0 + 32 + j;
-            nxt[j] = (rok && col < N) ? __ldcs(C + row + (int64_t)col * ldc) : 0.f;
-          }
-        }
         unsigned r[32];
         const unsigned taddr = tmem + ((unsigned)(lq * 32) << 16) + (unsigned)(ab * UN + j0);
         asm volatile(
@@ -278,16 +279,26 @@ __global__ void __launch_bounds__(kThreads, 1)
               "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
             : "r"(taddr)
             : "memory");
+        // the half's previous box must have been read out of shared memory
+        if (leader && pending) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+        asm volatile("bar.sync %0, 128;" ::"r"(1 + half) : "memory");
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        if (rok) {
+        const int rr = lq * 32 + lane;
 #pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            const int col = n0 + j0 + j;
-            if (col < N) __stcs(C + row + (int64_t)col * ldc, cur[j] - __uint_as_float(r[j]));
-          }
+        for (int j = 0; j < 32; ++j) stg[j * UM + rr] = -__uint_as_float(r[j]);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("bar.sync %0, 128;" ::"r"(1 + half) : "memory");
+        if (leader) {
+          // rows m0.. (128-aligned, never negative), columns n0 + j0..; the tensor map
+          // clips the box at M and N
+          asm volatile(
+              "cp.reduce.async.bulk.tensor.2d.global.shared::cta.add.tile.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
+                  reinterpret_cast<uint64_t>(&tC)),
+              "r"(m0), "r"(n0 + j0), "r"(stg_s)
+              : "memory");
+          asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+          pending = true;
         }
-#pragma unroll
-        for (int j = 0; j < 32; ++j) cur[j] = nxt[j];
       }
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&tempty[ab])) : "memory");
@@ -296,6 +307,8 @@ __global__ void __launch_bounds__(kThreads, 1)
         aphase ^= 1u;
       }
     }
+    // the reductions this CTA issued complete before it ends
+    if (leader && pending) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
@@ -391,8 +404,24 @@ int gemm_umma_bf16x3(bem_ctx* c, int M, int N, int K, const float* A, int64_t ld
     return bem_fail(c, BEM_ERR_CUDA, "umma: tensor map encoding failed");
   const int64_t tiles = (int64_t)((M + UM - 1) / UM) * ((N + UN - 1) / UN);
   if (tiles > INT32_MAX) return bem_fail(c, BEM_ERR_ARG, "umma: too many tiles");
+  // C: FP32, column-major; box 128 rows x 32 columns.  The base is 16-byte aligned
+  // (the trailing block of an lda-multiple-of-32 matrix at a 256-multiple offset) and
+  // ldc * 4 is a multiple of 16 bytes.
+  if ((reinterpret_cast<uintptr_t>(C) & 15) != 0 || (ldc * 4) % 16 != 0)
+    return bem_fail(c, BEM_ERR_ARG, "umma: C must be 16-byte aligned with ldc a multiple of 4");
+  CUtensorMap mC;
+  {
+    cuuint64_t dims[2] = {(cuuint64_t)M, (cuuint64_t)N};
+    cuuint64_t strides[1] = {(cuuint64_t)ldc * 4};
+    cuuint32_t box[2] = {(cuuint32_t)UM, 32u};
+    cuuint32_t estr[2] = {1, 1};
+    if (g_encode(&mC, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, C, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                 CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return bem_fail(c, BEM_ERR_CUDA, "umma: tensor map encoding of C failed");
+  }
   const int grid = (int)std::min<int64_t>(tiles, c->sm_count);
-  umma_update_kernel<<<grid, kThreads, kSmem, c->stream>>>(mAh, mAl, mBh, mBl, M, N, K, C, ldc, c->umma_err.p);
+  umma_update_kernel<<<grid, kThreads, kSmem, c->stream>>>(mAh, mAl, mBh, mBl, mC, M, N, K, c->umma_err.p);
   BEM_LAUNCH_CHECK(c);
   return BEM_OK;
 }

@@ -295,7 +295,9 @@ def run_gpu(args, ws, rank, local):
     achieved = prof["lu_trailing_bytes"] / (t_ms * 1e-3) / 1e9 if t_ms > 0 else 0.0
     n_launch = max(1, prof["lu_trailing_launches"])
     roofline = {
-        "kernel": "sgemm_bf16_kernel<0,3> (LU trailing update, FP32 C op= BF16x3 products)",
+        "kernel": ("umma_update_kernel + its BF16 split kernels (LU trailing update: C -= A B, "
+                   "tcgen05 BF16x3 into TMEM, TMA-reduce epilogue)" if args.precision == "fp32-ir" else
+                   "sgemm_bf16_kernel<0,1> (LU trailing update, BF16 mma.sync)"),
         "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
         "frac": achieved / peaks["hbm_gbs"], "peak_source": f"{src} hbm_gbs",
         "traffic": None,

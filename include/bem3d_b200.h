@@ -127,7 +127,7 @@ int bem_dgesv(bem_ctx* ctx, int n, int nrhs, double* A, int lda, int* ipiv, doub
  * that performs no device allocation, for callers that cannot allocate at the point
  * of the solve (a host that owns all device memory through its own pool, a loop that
  * must not pay for cudaMalloc/cudaFree synchronisation, a fixed memory budget).  Its
- * scratch is one static 4.5 MiB device array per GPU, which limits n to 4096
+ * scratch is one static 4.3 MiB device array per GPU, which limits n to 4096
  * (larger n returns BEM_ERR_TOO_LARGE).  dA (n x n, lda) is overwritten by the factors,
  * dB (n x nrhs, ldb) by the solution, d_ipiv (n ints) by the 1-based pivots; *info
  * (host) follows DGESV.  Work is queued on `stream` (a cudaStream_t, 0 = legacy
