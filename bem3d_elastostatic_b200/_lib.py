@@ -27,6 +27,9 @@ NOALLOC_MAX_N = 4096
 BEM_PREC_FP64 = 0
 BEM_PREC_FP32_IR = 1
 BEM_PREC_BF16_IR = 2
+BEM_PROF_COUNT = 0
+BEM_PROF_PHASES = 1
+BEM_PROF_TRAILING = 2
 BEM_ASM_FP64 = 0
 BEM_ASM_FP32_FAR = 1
 BEM_IP_KELVIN_CONSISTENT = 1
@@ -161,8 +164,11 @@ class Context:
     def sync(self):
         self.check(self.L.bem_sync(self.h), "sync")
 
-    def profile_begin(self, timing: bool = True):
-        self.check(self.L.bem_profile_begin(self.h, 1 if timing else 0), "profile_begin")
+    def profile_begin(self, timing=True):
+        """timing: True / BEM_PROF_PHASES (every LU phase), BEM_PROF_TRAILING (the
+        trailing updates only), False / BEM_PROF_COUNT (launch counts only)."""
+        mode = BEM_PROF_PHASES if timing is True else (BEM_PROF_COUNT if timing is False else int(timing))
+        self.check(self.L.bem_profile_begin(self.h, mode), "profile_begin")
 
     def profile_end(self) -> dict:
         p = Profile()

@@ -144,6 +144,10 @@ struct bem_ctx {
   long long launches = 0;
   int prof_timing = 0;
   bem_profile prof{};
+  std::vector<cudaEvent_t> ev_pool;  // timing events of the LU phase profile, reused
+  ~bem_ctx() {
+    for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
+  }
 };
 
 // Status helpers (host).

@@ -421,7 +421,8 @@ int bem_profile_begin(bem_ctx* c, int timing) {
   if (!c) return BEM_ERR_ARG;
   c->launches = 0;
   c->prof = bem_profile{};
-  c->prof_timing = timing ? 1 : 0;
+  if (timing < BEM_PROF_COUNT || timing > BEM_PROF_TRAILING) return BEM_ERR_ARG;
+  c->prof_timing = timing;
   return BEM_OK;
 }
 

@@ -490,26 +490,39 @@ int panel_launch(bem_ctx* c, const LUWorkspace& ws, T* S, int64_t lda, int n, in
 // events around every phase, summed per phase and printed to stderr at the end.
 struct LUProfile {
   bool on = false;
+  bem_ctx* c = nullptr;
   struct Ev {
     int phase;
-    cudaEvent_t a, b;
+    int a, b;  // indices into c->ev_pool
     double flops, bytes;
   };
   std::vector<Ev> ev;
-  int cur = -1;
-  cudaEvent_t start{};
+  size_t used = 0;
+  int cur = -1, start = -1;
+  // events come from the context's pool (created once, reused by later factorisations)
+  int take(cudaStream_t s) {
+    if (used == c->ev_pool.size()) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) != cudaSuccess) return -1;
+      c->ev_pool.push_back(e);
+    }
+    cudaEventRecord(c->ev_pool[used], s);
+    return (int)used++;
+  }
+  // trailing-only mode times the trailing update of every 16th panel (events between
+  // consecutive launches disturb the factorisation's timing; a sparse sample does not)
+  bool trailing_only = false;
+  int panel = 0;
+  bool skip(int phase) const { return !on || (trailing_only && (phase != 4 || panel % 16 != 0)); }
   void begin(int phase, cudaStream_t s) {
-    if (!on) return;
-    cudaEventCreate(&start);
-    cudaEventRecord(start, s);
     cur = phase;
+    if (skip(phase)) return;
+    start = take(s);
   }
   void end(cudaStream_t s, double flops = 0.0, double bytes = 0.0) {
-    if (!on) return;
-    cudaEvent_t b;
-    cudaEventCreate(&b);
-    cudaEventRecord(b, s);
-    ev.push_back({cur, start, b, flops, bytes});
+    if (skip(cur)) return;
+    const int b = take(s);
+    if (start >= 0 && b >= 0) ev.push_back({cur, start, b, flops, bytes});
   }
   void report(bem_ctx* c, int n) {
     if (!on) return;
@@ -517,16 +530,14 @@ struct LUProfile {
     long long cnt = 0;
     for (auto& e : ev) {
       float ms = 0.f;
-      cudaEventSynchronize(e.b);
-      cudaEventElapsedTime(&ms, e.a, e.b);
+      cudaEventSynchronize(c->ev_pool[e.b]);
+      cudaEventElapsedTime(&ms, c->ev_pool[e.a], c->ev_pool[e.b]);
       t[e.phase] += ms;
       if (e.phase == 4) {
         ++cnt;
         fl += e.flops;
         by += e.bytes;
       }
-      cudaEventDestroy(e.a);
-      cudaEventDestroy(e.b);
     }
     if (c->prof_timing) {
       c->prof.lu_panel_ms += t[0];
@@ -617,9 +628,12 @@ int lu_factor_ws(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int* perm, int 
   cudaFuncSetAttribute(inv_unit_upper_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inv_smem);
   int rc;
   LUProfile prof;
-  prof.on = getenv("BEM_LU_PROFILE") != nullptr || c->prof_timing;
+  prof.c = c;
+  prof.on = getenv("BEM_LU_PROFILE") != nullptr || c->prof_timing != BEM_PROF_COUNT;
+  prof.trailing_only = c->prof_timing == BEM_PROF_TRAILING && getenv("BEM_LU_PROFILE") == nullptr;
   for (int j0 = 0; j0 < n; j0 += nb) {
     const int jb = std::min(nb, n - j0);
+    prof.panel = j0 / nb;
     for (int r0 = j0; r0 < j0 + jb; r0 += kPanelW) {
       const int w = std::min(kPanelW, j0 + jb - r0);
       prof.begin(0, c->stream);

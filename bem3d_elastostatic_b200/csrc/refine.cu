@@ -118,7 +118,12 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
     c->f32_gemm = c->f32_gemm_override;
   else
     c->f32_gemm = (precision == BEM_PREC_BF16_IR) ? 1 : 4;
-  int rc = lu_factor<float>(c, c->A32.p, lda, n, c->piv.p, c->perm.p, kNbMixed, info);
+  int nb = kNbMixed;
+  if (const char* e = getenv("BEM_LU_NB")) {  // panel width override: 128, 256, 384 or 512
+    const int v = atoi(e);
+    if (v >= 128 && v <= 512 && v % 128 == 0) nb = v;
+  }
+  int rc = lu_factor<float>(c, c->A32.p, lda, n, c->piv.p, c->perm.p, nb, info);
   c->f32_gemm = saved;
   if (rc) return rc;
   BEM_CUDA(c, cudaEventRecord(e1, c->stream));

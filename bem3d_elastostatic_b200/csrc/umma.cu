@@ -34,7 +34,7 @@ namespace {
 constexpr int UM = 128;                 // tile rows (UMMA M)
 constexpr int UN = 256;                 // tile columns (UMMA N)
 constexpr int UK = 64;                  // K chunk per TMA box (128 bytes of BF16)
-constexpr int kMaxK = 256;              // largest panel width
+constexpr int kMaxK = 512;              // largest panel width
 constexpr int kStages = 2;              // shared-memory ring of K chunks
 constexpr int A_TILE = UM * UK * 2;     // 16 KB
 constexpr int B_TILE = UN * UK * 2;     // 32 KB
@@ -373,7 +373,7 @@ bool umma_supported(int K) { return K > 0 && K <= kMaxK && K % UK == 0; }
 // C (M x N) -= A (M x K) * B (K x N) on tcgen05 with the three-term BF16 split.
 int gemm_umma_bf16x3(bem_ctx* c, int M, int N, int K, const float* A, int64_t lda, const float* B, int64_t ldb,
                      float* C, int64_t ldc) {
-  if (!umma_supported(K)) return bem_fail(c, BEM_ERR_ARG, "umma: K must be a multiple of 64 up to 256");
+  if (!umma_supported(K)) return bem_fail(c, BEM_ERR_ARG, "umma: K must be a multiple of 64 up to 512");
   if (!g_encode) {
     cudaDriverEntryPointQueryResult q;
     void* fn = nullptr;

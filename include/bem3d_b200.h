@@ -149,10 +149,15 @@ int bem_internal_points(bem_ctx* ctx, int l, const double* cx, const double* cy,
                         double* vm, int flags);
 
 /* Profiling of the library's own kernels.  bem_profile_begin zeroes the counters;
- * with timing != 0 the LU phases are bracketed by CUDA events on the context's stream
- * (the stream every kernel of the context runs on).  bem_profile_end syncs the stream
- * and reports.  Trailing flops/bytes are the algorithmic work of the trailing-update
+ * with timing = BEM_PROF_PHASES the LU phases are bracketed by CUDA events on the
+ * context's stream (the stream every kernel of the context runs on); with
+ * BEM_PROF_TRAILING only the trailing updates of every 16th panel are (a sample with
+ * little disturbance of the run: events between all launches slow it down).  bem_profile_end syncs the stream and reports.  Trailing flops/bytes are the algorithmic work of the trailing-update
  * GEMMs: 2*m*m*nb flops and the C read+write plus one read of each operand. */
+#define BEM_PROF_COUNT 0     /* launch counts only */
+#define BEM_PROF_PHASES 1    /* every LU phase timed */
+#define BEM_PROF_TRAILING 2  /* a sample of the trailing updates timed */
+
 typedef struct {
   long long kernel_launches;    /* kernels this context launched */
   double lu_panel_ms;           /* cooperative panel factorisation */
