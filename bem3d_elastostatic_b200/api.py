@@ -101,6 +101,19 @@ class Quadesth:
         self.ctx.check(self.ctx.L.bem_reorganize(self.ctx.h, _lib.ptr(u), _lib.ptr(t)), "reorganize")
         return u, t
 
+    # stress_mod.f90:365
+    def compute_boundary_stresses(self, element_nodal: bool = True):
+        """Traction-recovery boundary stresses: (sigma_elem (6, 9, ne) or None,
+        sigma_node (6, n), principal (3, n), von Mises (n))."""
+        m = self.mesh
+        se = np.zeros((6, 9, m.ne), order="F") if element_nodal else None
+        sn = np.zeros((6, m.n), order="F")
+        pr = np.zeros((3, m.n), order="F")
+        vm = np.zeros(m.n)
+        self.ctx.check(self.ctx.L.bem_boundary_stresses(self.ctx.h, _lib.ptr(se), _lib.ptr(sn), _lib.ptr(pr),
+                                                        _lib.ptr(vm)), "boundary_stresses")
+        return se, sn, pr, vm
+
     # stress_mod.f90:511
     def compute_internal_points(self, points: Optional[np.ndarray] = None,
                                 kelvin_consistent: bool = False):
@@ -129,6 +142,8 @@ class Quadesth:
         x = self.solve_linear_system(precision, tol=tol)
         u, t = self.reorganize_solution()
         res = {"x": x, "u": u, "t": t, "solve_info": self.solve_info}
+        (res["sigma_elem"], res["sigma_node"], res["sigma_node_prin"],
+         res["sigma_node_vm"]) = self.compute_boundary_stresses()
         if self.mesh.l > 0:
             res["u_int"], res["sigma"], res["prin"], res["vm"] = self.compute_internal_points(
                 kelvin_consistent=kelvin_consistent)

@@ -22,7 +22,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
           "-Xptxas", "-warn-spills"]
-PER_FILE = {"geometry.cu": ["--fmad=false"]}
+PER_FILE = {"geometry.cu": ["--fmad=false"], "boundary.cu": ["--fmad=false"]}
 
 
 def _sources():

@@ -179,6 +179,7 @@ int lu_solve_fp64(bem_ctx* c, const double* LU, int64_t lda, int n, double* b);
 int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter,
                 bem_solve_info* stats, int* info);
 int launch_reorganize(bem_ctx* c);
+int launch_boundary_stresses(bem_ctx* c, double* se, double* sn, double* pr, double* vm);
 int launch_internal_points(bem_ctx* c, int l, const double* cx, const double* cy,
                            const double* cz, double* u, double* s, double* pr, double* vm,
                            int flags);

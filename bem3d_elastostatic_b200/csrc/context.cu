@@ -384,6 +384,28 @@ int bem_reorganize(bem_ctx* c, double* FI_out, double* DFI_out) {
   return BEM_OK;
 }
 
+int bem_boundary_stresses(bem_ctx* c, double* sigma_elem, double* sigma_node, double* prin, double* vm) {
+  if (!c) return BEM_ERR_ARG;
+  if (!sigma_node || !prin || !vm) return bem_fail(c, BEM_ERR_ARG, "boundary_stresses: null output");
+  if (!c->have_solution) return bem_fail(c, BEM_ERR_STATE, "boundary stresses before solve");
+  BEM_CUDA(c, cudaSetDevice(c->device));
+  // u and t of the current solution (cheap: two small kernels)
+  int rc = bem::launch_reorganize(c);
+  if (rc) return rc;
+  const size_t ne = c->ne, n = c->n;
+  bem::DBuf<double> d;
+  BEM_CUDA(c, d.alloc(54 * ne + 10 * n));
+  double *se = d.p, *sn = se + 54 * ne, *pr = sn + 6 * n, *v = pr + 3 * n;
+  if ((rc = bem::launch_boundary_stresses(c, se, sn, pr, v))) return rc;
+  if (sigma_elem)
+    BEM_CUDA(c, cudaMemcpyAsync(sigma_elem, se, 54 * ne * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  BEM_CUDA(c, cudaMemcpyAsync(sigma_node, sn, 6 * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  BEM_CUDA(c, cudaMemcpyAsync(prin, pr, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  BEM_CUDA(c, cudaMemcpyAsync(vm, v, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  BEM_CUDA(c, cudaStreamSynchronize(c->stream));
+  return BEM_OK;
+}
+
 int bem_internal_points_device(bem_ctx* c, int l, const double* cx, const double* cy, const double* cz,
                                double* u, double* s, double* pr, double* vm, int flags) {
   if (!c || l < 0) return BEM_ERR_ARG;

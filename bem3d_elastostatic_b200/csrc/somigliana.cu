@@ -20,6 +20,7 @@
 
 #include "common.cuh"
 #include "shape.cuh"
+#include "stress.cuh"
 
 namespace bem {
 
@@ -226,34 +227,6 @@ __device__ __forceinline__ void somigliana_point(const SomConst& K, const double
   sa[3] += Dxy - Sxy;
   sa[4] += Dyz - Syz;
   sa[5] += Dzx - Szx;
-}
-
-// calc_principal_and_vm (:299-359)
-__device__ void principal_vm(const double* s, double* pr, double* vm) {
-  const double sxx = s[0], syy = s[1], szz = s[2], sxy = s[3], syz = s[4], szx = s[5];
-  *vm = sqrt(0.5 * ((sxx - syy) * (sxx - syy) + (syy - szz) * (syy - szz) + (szz - sxx) * (szz - sxx) +
-                    6.0 * (sxy * sxy + syz * syz + szx * szx)));
-  const double i1 = sxx + syy + szz, q = i1 / 3.0;
-  const double pxx = sxx - q, pyy = syy - q, pzz = szz - q;
-  const double j2 = 0.5 * (pxx * pxx + pyy * pyy + pzz * pzz) + sxy * sxy + syz * syz + szx * szx;
-  if (j2 <= 1.0e-20 * (i1 * i1 + 1.0)) {
-    pr[0] = pr[1] = pr[2] = q;
-    return;
-  }
-  const double j3 = pxx * (pyy * pzz - syz * syz) - sxy * (sxy * pzz - syz * szx) + szx * (sxy * syz - pyy * szx);
-  const double r = sqrt(4.0 * j2 / 3.0);
-  double c3 = 4.0 * j3 / (r * r * r);
-  c3 = fmin(1.0, fmax(-1.0, c3));
-  const double phi = acos(c3) / 3.0;
-  double a = q + r * cos(phi);
-  double cc = q + r * cos(phi + 2.0 * kPi / 3.0);
-  double b = 3.0 * q - a - cc, t;
-  if (a < b) { t = a; a = b; b = t; }
-  if (b < cc) { t = b; b = cc; cc = t; }
-  if (a < b) { t = a; a = b; b = t; }
-  pr[0] = a;
-  pr[1] = b;
-  pr[2] = cc;
 }
 
 __global__ void __launch_bounds__(256) far_kernel(int l, const double* cx, const double* cy, const double* cz,

@@ -123,7 +123,7 @@ def allreduce_max(x: float, ws: int) -> float:
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if dist.get_backend() == "nccl" else "cpu")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -202,6 +202,7 @@ def run_reference(args, ws, rank):
 
 def run_gpu(args, ws, rank, local):
     import torch
+    import torch.cuda.profiler
 
     from bem3d_elastostatic_b200 import _lib
     from bem3d_elastostatic_b200.api import Quadesth
@@ -228,6 +229,8 @@ def run_gpu(args, ws, rank, local):
     with ClockSampler(local) as clk:
         # inside the timed region only the trailing updates carry events (two per panel)
         q.ctx.profile_begin(timing=_lib.BEM_PROF_TRAILING)
+        # the timed region is the profiler range (ncu --profile-from-start off)
+        torch.cuda.profiler.start()
         ev0.record(stream)
         marks = [ev0]
         for _ in range(args.steps):
@@ -237,6 +240,7 @@ def run_gpu(args, ws, rank, local):
             e.record(stream)
             marks.append(e)
         ev1.record(stream)
+        torch.cuda.profiler.stop()
         prof = q.ctx.profile_end()
         ev1.synchronize()
     torch.cuda.synchronize()

@@ -142,6 +142,14 @@ int bem_dgesv_noalloc(int n, int nrhs, double* dA, int lda, int* d_ipiv, double*
  * DFI (27, ne) element-nodal tractions.  Host outputs nullable. */
 int bem_reorganize(bem_ctx* ctx, double* FI_out, double* DFI_out);
 
+/* compute_boundary_stresses (stress_mod.f90:119-406): traction-recovery stresses at
+ * every node of every element, sigma_elem (6, 9, ne) (nullable), their average over
+ * each node's elements, sigma_node (6, n), and the nodal principal (3, n) and von
+ * Mises (n) stresses; order xx, yy, zz, xy, yz, zx.  Needs a solved system (it
+ * reorganizes the current solution itself). */
+int bem_boundary_stresses(bem_ctx* ctx, double* sigma_elem, double* sigma_node,
+                          double* prin, double* vm);
+
 /* compute_internal_points (stress_mod.f90:511-886): Somigliana displacement and stress
  * with calc_principal_and_vm (:299-359) at l points.  flags: BEM_IP_*. */
 int bem_internal_points(bem_ctx* ctx, int l, const double* cx, const double* cy,

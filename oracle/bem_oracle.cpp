@@ -18,6 +18,7 @@
 //   geometry tables all_*(36, ne) and all_ff(9, 36, ne), column-major.
 // Compile with -O2 -ffp-contract=off (no FMA contraction, no reassociation) so the
 // arithmetic matches gfortran -O3 on baseline x86-64.
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -679,6 +680,140 @@ void orc_principal(const double* sig, double* prin, double* vm) {
   if (prin[0] < prin[1]) { tmp = prin[0]; prin[0] = prin[1]; prin[1] = tmp; }
   if (prin[1] < prin[2]) { tmp = prin[1]; prin[1] = prin[2]; prin[2] = tmp; }
   if (prin[0] < prin[1]) { tmp = prin[0]; prin[0] = prin[1]; prin[1] = tmp; }
+}
+
+// axes_cos_lagrange: stress_mod.f90:119-168.  Orthonormal triad L (rows e1, e2, e3)
+// and the intrinsic-to-local map CL at a point of an element.
+static void axes_cos(int ncone, const double* fd1, const double* fd2, const double* cx, const double* cy,
+                     const double* cz, double L[3][3], double CL[2][2]) {
+  double g1[3] = {0, 0, 0}, g2[3] = {0, 0, 0}, g3[3];
+  for (int a = 0; a < ncone; ++a) {
+    const double c[3] = {cx[a], cy[a], cz[a]};
+    for (int i = 0; i < 3; ++i) {
+      g1[i] = g1[i] + fd1[a] * c[i];
+      g2[i] = g2[i] + fd2[a] * c[i];
+    }
+  }
+  const double v1 = std::sqrt(g1[0] * g1[0] + g1[1] * g1[1] + g1[2] * g1[2]);
+  const double v2 = std::sqrt(g2[0] * g2[0] + g2[1] * g2[1] + g2[2] * g2[2]);
+  g3[0] = g1[1] * g2[2] - g1[2] * g2[1];
+  g3[1] = g1[2] * g2[0] - g1[0] * g2[2];
+  g3[2] = g1[0] * g2[1] - g1[1] * g2[0];
+  const double jcb = std::sqrt(g3[0] * g3[0] + g3[1] * g3[1] + g3[2] * g3[2]);
+  for (int i = 0; i < 3; ++i) {
+    L[2][i] = g3[i] / jcb;
+    L[0][i] = g1[i] / v1;
+  }
+  L[1][0] = L[2][1] * L[0][2] - L[2][2] * L[0][1];
+  L[1][1] = L[2][2] * L[0][0] - L[2][0] * L[0][2];
+  L[1][2] = L[2][0] * L[0][1] - L[2][1] * L[0][0];
+  double cos_th = (g1[0] * g2[0] + g1[1] * g2[1] + g1[2] * g2[2]) / (v1 * v2);
+  if (cos_th > 1.0) cos_th = 1.0;
+  if (cos_th < -1.0) cos_th = -1.0;
+  double sin_th = std::sqrt(std::max(0.0, 1.0 - cos_th * cos_th));
+  if (sin_th < 1.0e-12) sin_th = 1.0e-12;
+  CL[0][0] = 1.0 / v1;
+  CL[0][1] = -cos_th / (v1 * sin_th);
+  CL[1][0] = 0.0;
+  CL[1][1] = 1.0 / (v2 * sin_th);
+}
+
+// compute_boundary_stresses with boundary_stresses_elem: stress_mod.f90:174-297,
+// 365-406.  FI: nodal displacements, DFI(27, ne): element-nodal tractions (after
+// reorganize_solution).  Outputs: sigma_elem(6, 9, ne) (nullable), sigma_node(6, n),
+// prin(3, n), vm(n).  Stress order xx, yy, zz, xy, yz, zx.
+int orc_boundary_stresses(const orc_mesh* M, const double* FI, const double* DFI, double* sigma_elem,
+                          double* sigma_node, double* prin, double* vm) {
+  const int n = M->n, ne = M->ne;
+  std::vector<int> nesim(n), ke(8 * (size_t)n, 0);
+  if (orc_adjacency(M, nesim.data(), ke.data()) > 8) return -1;
+  std::vector<double> se(54 * (size_t)ne, 0.0);
+  const double rge = M->mu, xnu = M->nu;
+  const double c_eps = 2.0 * rge / (1.0 - xnu);
+  const double c_nu = 2.0 * rge * xnu / (1.0 - xnu);
+  const double c_sig3 = xnu / (1.0 - xnu);
+  const double q1[9] = {-1.0, 0.0, 1.0, 1.0, 1.0, 0.0, -1.0, -1.0, 0.0};
+  const double q2[9] = {-1.0, -1.0, -1.0, 0.0, 1.0, 1.0, 1.0, 0.0, 0.0};
+  const double t1[6] = {1.0, 0.0, 0.0, 0.5, 0.0, 0.5};
+  const double t2[6] = {0.0, 1.0, 0.0, 0.5, 0.5, 0.0};
+#pragma omp parallel for schedule(dynamic)
+  for (int e = 0; e < ne; ++e) {
+    const int ncone = M->nconec[e];
+    double cx[9], cy[9], cz[9], ue[3][9], te[3][9];
+    for (int a = 0; a < ncone; ++a) {
+      const int ik = M->kconec[a + 9 * e] - 1;
+      cx[a] = M->x[ik];
+      cy[a] = M->y[ik];
+      cz[a] = M->z[ik];
+      for (int i = 0; i < 3; ++i) {
+        ue[i][a] = FI[3 * ik + i];
+        te[i][a] = DFI[3 * a + i + 27 * e];
+      }
+    }
+    for (int k = 0; k < ncone; ++k) {
+      const double g1 = ncone == 9 ? q1[k] : t1[k], g2 = ncone == 9 ? q2[k] : t2[k];
+      double ff[9], fd1[9], fd2[9], L[3][3], CL[2][2];
+      shape(ncone, g1, g2, ff, fd1, fd2);
+      axes_cos(ncone, fd1, fd2, cx, cy, cz, L, CL);
+      double u1_1 = 0.0, u2_2 = 0.0, u1_2 = 0.0, u2_1 = 0.0;
+      for (int a = 0; a < ncone; ++a) {
+        const double dn1 = CL[0][0] * fd1[a] + CL[1][0] * fd2[a];
+        const double dn2 = CL[0][1] * fd1[a] + CL[1][1] * fd2[a];
+        const double ul1 = L[0][0] * ue[0][a] + L[0][1] * ue[1][a] + L[0][2] * ue[2][a];
+        const double ul2 = L[1][0] * ue[0][a] + L[1][1] * ue[1][a] + L[1][2] * ue[2][a];
+        u1_1 = u1_1 + dn1 * ul1;
+        u2_2 = u2_2 + dn2 * ul2;
+        u1_2 = u1_2 + dn2 * ul1;
+        u2_1 = u2_1 + dn1 * ul2;
+      }
+      const double eps11 = u1_1, eps22 = u2_2, eps12 = 0.5 * (u1_2 + u2_1);
+      double tl[3];
+      for (int i = 0; i < 3; ++i) tl[i] = L[i][0] * te[0][k] + L[i][1] * te[1][k] + L[i][2] * te[2][k];
+      double S[3][3];
+      S[0][2] = tl[0];
+      S[2][0] = S[0][2];
+      S[1][2] = tl[1];
+      S[2][1] = S[1][2];
+      S[2][2] = tl[2];
+      S[0][0] = c_eps * eps11 + c_nu * eps22 + c_sig3 * S[2][2];
+      S[1][1] = c_eps * eps22 + c_nu * eps11 + c_sig3 * S[2][2];
+      S[0][1] = 2.0 * rge * eps12;
+      S[1][0] = S[0][1];
+      // S_glob = L^T (S_loc L)
+      double T[3][3], Gm[3][3];
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) T[i][j] = S[i][0] * L[0][j] + S[i][1] * L[1][j] + S[i][2] * L[2][j];
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) Gm[i][j] = L[0][i] * T[0][j] + L[1][i] * T[1][j] + L[2][i] * T[2][j];
+      double* o = &se[6 * (k + 9 * (size_t)e)];
+      o[0] = Gm[0][0];
+      o[1] = Gm[1][1];
+      o[2] = Gm[2][2];
+      o[3] = 0.5 * (Gm[0][1] + Gm[1][0]);
+      o[4] = 0.5 * (Gm[1][2] + Gm[2][1]);
+      o[5] = 0.5 * (Gm[2][0] + Gm[0][2]);
+    }
+  }
+  for (int in = 0; in < n; ++in) {
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    const int ns = std::min(nesim[in], 8);
+    if (ns > 0) {
+      for (int j = 0; j < ns; ++j) {
+        const int e = ke[j + 8 * in] - 1;
+        for (int k = 0; k < M->nconec[e]; ++k)
+          if (M->kconec[k + 9 * e] - 1 == in) {
+            for (int c = 0; c < 6; ++c) acc[c] = acc[c] + se[c + 6 * (k + 9 * (size_t)e)];
+            break;
+          }
+      }
+      for (int c = 0; c < 6; ++c) acc[c] = acc[c] / (double)ns;
+    }
+    for (int c = 0; c < 6; ++c) sigma_node[c + 6 * (size_t)in] = acc[c];
+    orc_principal(acc, prin + 3 * (size_t)in, vm + in);
+  }
+  if (sigma_elem)
+    for (size_t i = 0; i < se.size(); ++i) sigma_elem[i] = se[i];
+  return 0;
 }
 
 // compute_internal_points: stress_mod.f90:511-781 with accumulate_somigliana_range

@@ -8,6 +8,7 @@ reference's phases on a :class:`bem3d_elastostatic_b200.mesh.Mesh`:
 * ``hg``                  H and G as separate products          (blocks combined by ghmat8)
 * ``solve``               LAPACK dgesv                          (solver_mod.f90:17-36)
 * ``reorganize``          un-swap into u and t                  (io_mod.f90:148-183)
+* ``boundary_stresses``   traction-recovery boundary stresses   (stress_mod.f90:119-406)
 * ``internal_points``     Somigliana displacement and stress    (stress_mod.f90:511-886)
 * ``principal``           principal and von Mises stress        (stress_mod.f90:299-359)
 
@@ -65,6 +66,7 @@ def lib():
         L.orc_ghmat8.argtypes = [P(_Mesh), P(_Geo), C.c_int, C.c_int, _dp, C.c_int64, _dp]
         L.orc_hg.argtypes = [P(_Mesh), P(_Geo), C.c_int, C.c_int, _dp, C.c_int64, _dp, C.c_int64]
         L.orc_reorganize.argtypes = [P(_Mesh), _dp, _dp]
+        L.orc_boundary_stresses.argtypes = [P(_Mesh), _dp, _dp, _dp, _dp, _dp, _dp]
         L.orc_gauss_legendre.argtypes = [C.c_int, _dp, _dp]
         L.orc_gauss_legendre.restype = None
         L.orc_principal.argtypes = [_dp, _dp, _dp]
@@ -170,6 +172,21 @@ class Oracle:
         assert rc == 0
         return u, s, pr, vm
 
+    def boundary_stresses(self, FI: np.ndarray, DFI: np.ndarray):
+        """compute_boundary_stresses (stress_mod.f90:174-297, 365-406): element-nodal
+        stresses (6, 9, ne), nodal averages (6, n), principal (3, n), von Mises (n)."""
+        m = self.mesh
+        se = np.zeros((6, 9, m.ne), order="F")
+        sn = np.zeros((6, m.n), order="F")
+        pr = np.zeros((3, m.n), order="F")
+        vm = np.zeros(m.n)
+        FI = np.ascontiguousarray(FI, dtype=np.float64)
+        DFI = np.asfortranarray(DFI, dtype=np.float64)
+        rc = lib().orc_boundary_stresses(C.byref(self.cm), _d(FI), _d(DFI), _d(se), _d(sn), _d(pr),
+                                         _d(vm))
+        assert rc == 0
+        return se, sn, pr, vm
+
     def run(self, kelvin_consistent: bool = False):
         """The whole reference sequence (main.f90:38-68) on this mesh."""
         self.geometry()
@@ -179,6 +196,8 @@ class Oracle:
             raise RuntimeError(f"dgesv info = {info}")
         u, t = self.reorganize(x)
         res = {"x": x, "u": u, "t": t}
+        (res["sigma_elem"], res["sigma_node"], res["sigma_node_prin"],
+         res["sigma_node_vm"]) = self.boundary_stresses(u, t)
         if self.mesh.l > 0:
             res["u_int"], res["sigma"], res["prin"], res["vm"] = self.internal_points(
                 u, t, kelvin_consistent=kelvin_consistent)

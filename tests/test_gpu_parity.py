@@ -202,3 +202,53 @@ def test_fp32_far_assembly(cube2, gpu_cube2):
         # the diagonal block mixes FP64 singular terms with the FP64 sums of FP32 terms
         assert np.abs(A32[blk] - A64[blk]).max() <= 2e-6 * rowmax[3 * i:3 * i + 3].max()
     assert np.abs(FI32 - FI64).max() <= 2e-6 * np.abs(FI64).max()
+
+
+def test_internal_points_sharded_single_rank(cube2, tmp_path):
+    """The sharded internal-point path on one rank (gloo group of size 1) returns the
+    single-call arrays exactly."""
+    import socket
+    from datetime import timedelta
+
+    import torch.distributed as dist
+
+    from bem3d_elastostatic_b200.api import Quadesth
+    from bem3d_elastostatic_b200.shard import internal_points_sharded
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=timedelta(seconds=60))
+    try:
+        q = Quadesth(cube2)
+        q.run()
+        ref = q.compute_internal_points()
+        got = internal_points_sharded(q)
+        for a, b in zip(got, ref):
+            np.testing.assert_array_equal(a, b)
+        q.close()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("which", ["cube2", "cube8"])
+def test_boundary_stresses_vs_oracle(which, cube2, cube8_mesh):
+    """compute_boundary_stresses on the GPU against the oracle on the same mesh: the
+    element-nodal and averaged stresses to 1e-10 of their scale, principal to 1e-8."""
+    from bem3d_elastostatic_b200.api import Quadesth
+
+    mesh = cube2 if which == "cube2" else cube8_mesh
+    ref = O.Oracle(mesh).run()
+    q = Quadesth(mesh)
+    res = q.run()
+    # the oracle's recovery applied to the GPU's own u and t isolates the kernel
+    se, sn, pr, vm = O.Oracle(mesh).boundary_stresses(res["u"], res["t"])
+    scale = np.abs(sn).max()
+    assert np.abs(res["sigma_elem"] - se).max() <= 1e-12 * scale
+    assert np.abs(res["sigma_node"] - sn).max() <= 1e-12 * scale
+    assert np.abs(res["sigma_node_vm"] - vm).max() <= 1e-12 * scale
+    assert np.abs(res["sigma_node_prin"] - pr).max() <= 1e-8 * scale
+    # and end to end against the oracle's own solve
+    assert np.abs(res["sigma_node"] - ref["sigma_node"]).max() <= 1e-10 * scale
+    q.close()

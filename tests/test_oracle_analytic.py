@@ -103,3 +103,21 @@ def test_ghmat8_matches_hg_recombination(cube2_runs):
     scale = np.abs(A).max()
     assert np.abs(A - A2).max() < 1e-13 * scale
     assert np.abs(FI - F2).max() < 1e-13 * max(1.0, np.abs(FI).max())
+
+
+def test_boundary_stresses_uniaxial_cube():
+    """Traction-recovery boundary stresses (stress_mod.f90:365-406) of the uniaxially
+    loaded cube: sigma_zz = 1 and the other components 0 at every boundary node."""
+    from bem3d_elastostatic_b200.mesh import uniaxial_cube
+
+    mesh = uniaxial_cube(3, young=1.0, nu=0.3)
+    r = O.Oracle(mesh).run()
+    sn = r["sigma_node"]
+    assert np.abs(sn[2] - 1.0).max() < 5e-4
+    assert np.abs(sn[[0, 1, 3, 4, 5]]).max() < 5e-4
+    assert np.abs(r["sigma_node_vm"] - 1.0).max() < 1e-3
+    assert np.abs(r["sigma_node_prin"][0] - 1.0).max() < 1e-3
+    # every element-nodal value of a node averages to the nodal value
+    se = r["sigma_elem"]
+    k0 = mesh.kconec[0, 0] - 1
+    assert np.isfinite(se).all() and np.abs(se[2, 0, 0] - sn[2, k0]) < 1e-3
