@@ -28,7 +28,7 @@ namespace bem {
 constexpr int kPitch = kPanelW + 1;  // shared-memory column pitch (conflict-free)
 constexpr int kInvBlock = 128;       // unit-triangle inverse block of the block-row TRSM
 constexpr int kSolveBlock = 128;     // diagonal block of the triangular solves
-constexpr int kPanelSmemMax = 200 * 1024;
+constexpr int kPanelSmemMax = 200 * 1024;  // dynamic shared memory of a panel CTA
 constexpr long long kSpinLimit = 1ll << 24;
 constexpr int kSweepThreads = 512;   // threads of a triangular sweep CTA (4 per row of a block)
 
@@ -36,6 +36,10 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
   unsigned v;
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
+}
+
+__device__ __forceinline__ void red_release_add_u32(unsigned* p, unsigned v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
 __device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
@@ -86,10 +90,11 @@ __global__ void __launch_bounds__(256, 1)
                  int* cand_idx, T* cand_col, T* diag_col, unsigned* barrier, unsigned bar_base, int* status) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* col = reinterpret_cast<T*>(smem_raw);  // [chunk][kPitch]
-  __shared__ T pvt[kPanelW];
+  __shared__ T s_pv[kPanelW];  // the winning candidate column
+  __shared__ T s_dc[kPanelW];  // the diagonal column of the pivot step
   __shared__ double red_v[8];
-  __shared__ int red_c[8], red_g[8];
-  __shared__ int s_local_c, s_win_g, s_win_c, s_abort;
+  __shared__ int red_c[8];
+  __shared__ int s_local_c, s_abort, s_win[2];
   const int G = gridDim.x, g = blockIdx.x, tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
   const int c_beg = r0 + g * chunk;
   const int c_end = min(n, c_beg + chunk);
@@ -133,11 +138,10 @@ __global__ void __launch_bounds__(256, 1)
       if (lc != INT_MAX) cand_col[((int64_t)par * G + g) * kPanelW + tid] = col[(lc - c_beg) * kPitch + tid];
       if (k >= c_beg && k < c_end) diag_col[par * kPanelW + tid] = col[(k - c_beg) * kPitch + tid];
     }
-    __threadfence();
     __syncthreads();
-    // 2. grid barrier (bounded)
+    // 2. grid barrier (bounded): thread 0's release covers the CTA's writes above
     if (tid == 0) {
-      atomicAdd(barrier, 1u);
+      red_release_add_u32(barrier, 1u);
       const unsigned target = bar_base + (unsigned)(t + 1) * (unsigned)G;
       long long spins = 0;
       int abort = 0;
@@ -146,19 +150,20 @@ __global__ void __launch_bounds__(256, 1)
           abort = 1;
           break;
         }
-        __nanosleep(64);
+        __nanosleep(32);
       }
       if (abort) atomicCAS(status, 0, BEM_ERR_TIMEOUT);
       s_abort = abort;
-      __threadfence();
     }
     __syncthreads();
     if (s_abort) return;
-    // 3. global pivot
+    // 3. warp 0 reduces the CTAs' candidates while warp 1 fetches the diagonal column
+    //    (needed by the CTA that owns the winner); then the winner's column
     if (wp == 0) {
       double v = -1.0;
       int cidx = INT_MAX, gg = 0;
-      for (int i = lane; i < G; i += 32) better(v, cidx, gg, __ldcg(cand_val + par * G + i), __ldcg(cand_idx + par * G + i), i);
+      for (int i = lane; i < G; i += 32)
+        better(v, cidx, gg, __ldcg(cand_val + par * G + i), __ldcg(cand_idx + par * G + i), i);
       for (int off = 16; off > 0; off >>= 1) {
         const double ov = __shfl_xor_sync(0xffffffffu, v, off);
         const int oc = __shfl_xor_sync(0xffffffffu, cidx, off);
@@ -166,15 +171,17 @@ __global__ void __launch_bounds__(256, 1)
         better(v, cidx, gg, ov, oc, og);
       }
       if (lane == 0) {
-        s_win_g = gg;
-        s_win_c = cidx;
+        s_win[0] = gg;
+        s_win[1] = cidx;
       }
+    } else if (wp == 1) {
+      s_dc[lane] = (lane < w) ? __ldcg(diag_col + par * kPanelW + lane) : T(0);
     }
     __syncthreads();
-    const int p = s_win_c;
-    if (tid < kPanelW)
-      pvt[tid] = (tid < w) ? __ldcg(cand_col + ((int64_t)par * G + s_win_g) * kPanelW + tid) : T(0);
+    const int wg = s_win[0], p = s_win[1];
+    if (tid < kPanelW) s_pv[tid] = (tid < w) ? __ldcg(cand_col + ((int64_t)par * G + wg) * kPanelW + tid) : T(0);
     __syncthreads();
+    const T* pvt = s_pv;
     const T pv = pvt[t];
     if (g == 0 && tid == 0) {
       piv[k] = p;
@@ -182,10 +189,10 @@ __global__ void __launch_bounds__(256, 1)
     }
     if (tid < w) {
       if (k >= c_beg && k < c_end) col[(k - c_beg) * kPitch + tid] = pvt[tid];
-      if (p != k && p >= c_beg && p < c_end) col[(p - c_beg) * kPitch + tid] = __ldcg(diag_col + par * kPanelW + tid);
+      if (p != k && p >= c_beg && p < c_end) col[(p - c_beg) * kPitch + tid] = s_dc[tid];
     }
     __syncthreads();
-    // 4. scale the multipliers and update the rest of the sub-panel
+    // 5. scale the multipliers and update the rest of the sub-panel
     if (pv != T(0)) {
       for (int cc = tid; cc < ncols; cc += blockDim.x) {
         if (c_beg + cc <= k) continue;
