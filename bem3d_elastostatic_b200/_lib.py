@@ -42,7 +42,9 @@ EXPORTS = [
     "bem_get_geometry", "bem_ghmat8", "bem_get_hg", "bem_solve", "bem_dgesv",
     "bem_reorganize", "bem_boundary_stresses", "bem_internal_points", "bem_device_state",
     "bem_internal_points_device", "bem_profile_begin", "bem_profile_end",
-    "bem_dgesv_noalloc",
+    "bem_dgesv_noalloc", "bem_batch_create", "bem_batch_destroy", "bem_batch_last_error",
+    "bem_batch_add", "bem_batch_assemble", "bem_batch_solve", "bem_batch_get_solution",
+    "bem_batch_get_system", "bem_batch_launches",
 ]
 
 
@@ -60,6 +62,16 @@ class SolveInfo(C.Structure):
     _fields_ = [("iterations", C.c_int), ("restarts", C.c_int), ("rel_residual", C.c_double),
                 ("factor_seconds", C.c_double), ("refine_seconds", C.c_double),
                 ("gflops", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class BatchInfo(C.Structure):
+    _fields_ = [("systems", C.c_int), ("sweeps", C.c_int), ("converged", C.c_int),
+                ("singular", C.c_int), ("max_backward_error", C.c_double),
+                ("solve_seconds", C.c_double), ("lu_threads", C.c_int),
+                ("lu_ms_256", C.c_float), ("lu_ms_512", C.c_float)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -123,6 +135,18 @@ def load(build_if_needed: bool = True):
     L.bem_device_state.argtypes = [_vp, C.POINTER(C.c_void_p), C.POINTER(C.c_int64),
                                    C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]
     L.bem_internal_points_device.argtypes = [_vp, C.c_int] + [_vp] * 7 + [C.c_int]
+    L.bem_batch_create.argtypes = [ctxp, C.c_int]
+    L.bem_batch_destroy.argtypes = [_vp]
+    L.bem_batch_last_error.argtypes = [_vp]
+    L.bem_batch_last_error.restype = C.c_char_p
+    L.bem_batch_add.argtypes = [_vp, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, C.c_double, C.c_double,
+                                _vp, C.c_int, _vp, C.c_int, _vp]
+    L.bem_batch_assemble.argtypes = [_vp]
+    L.bem_batch_solve.argtypes = [_vp, C.c_int, C.c_double, C.c_int, C.POINTER(BatchInfo)]
+    L.bem_batch_get_solution.argtypes = [_vp, C.c_int, _vp]
+    L.bem_batch_get_system.argtypes = [_vp, C.c_int, _vp, _vp]
+    L.bem_batch_launches.argtypes = [_vp]
+    L.bem_batch_launches.restype = C.c_longlong
     L.bem_profile_begin.argtypes = [_vp, C.c_int]
     L.bem_profile_end.argtypes = [_vp, C.POINTER(Profile)]
     _lib = L

@@ -153,6 +153,83 @@ class Quadesth:
         self.ctx.close()
 
 
+class Batch:
+    """Many independent systems solved together (no counterpart in the reference).
+
+    ``add(mesh, bcs)`` registers a mesh with its load cases: ``bcs`` is a list of
+    (27, ne) prescribed-value arrays for the mesh's ``kode`` (every system of a batch
+    has the same number of load cases, at most 8).  ``assemble()`` builds every A and
+    FI; ``solve(precision)`` factors and solves all of them ("fp32-ir": FP32 LU + FP64
+    refinement; "fp64": FP64 LU); ``solution(i)`` returns system i's (3n, nrhs)
+    solution.
+    """
+
+    def __init__(self, device: int = 0):
+        self.L = _lib.load()
+        h = _lib.C.c_void_p()
+        rc = self.L.bem_batch_create(_lib.C.byref(h), device)
+        if rc != 0:
+            raise _lib.BemError(rc, "bem_batch_create failed")
+        self.h = h
+        self.meshes = []
+        self.nrhs = []
+        self.info: Optional[dict] = None
+
+    def _check(self, rc: int, what: str) -> int:
+        if rc < 0:
+            msg = self.L.bem_batch_last_error(self.h)
+            raise _lib.BemError(rc, f"{what}: {msg.decode() if msg else ''}")
+        return rc
+
+    def add(self, mesh: Mesh, bcs=None) -> int:
+        mesh.validate()
+        bcs = [mesh.bc] if bcs is None else list(bcs)
+        bc = np.ascontiguousarray(np.stack([np.asfortranarray(b, dtype=np.float64).ravel(order="F") for b in bcs]))
+        pins = np.ascontiguousarray(mesh.pins, dtype=np.int32)
+        keep = [mesh.x, mesh.y, mesh.z, mesh.nconec, mesh.kconec, mesh.kode, bc, pins]
+        idx = self._check(self.L.bem_batch_add(
+            self.h, mesh.n, mesh.ne, _lib.ptr(mesh.x), _lib.ptr(mesh.y), _lib.ptr(mesh.z),
+            _lib.ptr(mesh.nconec), _lib.ptr(mesh.kconec), float(mesh.mu), float(mesh.nu),
+            _lib.ptr(mesh.kode), len(bcs), _lib.ptr(bc), int(pins.size), _lib.ptr(pins)), "batch_add")
+        del keep
+        self.meshes.append(mesh)
+        self.nrhs.append(len(bcs))
+        return idx
+
+    def assemble(self):
+        self._check(self.L.bem_batch_assemble(self.h), "batch_assemble")
+
+    def solve(self, precision: str = "fp32-ir", tol: float = 1e-14, max_iter: int = 6) -> dict:
+        st = _lib.BatchInfo()
+        rc = self.L.bem_batch_solve(self.h, PRECISIONS[precision], tol, max_iter, _lib.C.byref(st))
+        self.info = st.as_dict()
+        if rc == _lib.BEM_ERR_NOCONV:
+            raise SolverFailure(0)
+        self._check(rc, "batch_solve")
+        return self.info
+
+    def solution(self, i: int) -> np.ndarray:
+        m = self.meshes[i]
+        x = np.zeros((m.ndof, self.nrhs[i]), order="F")
+        self._check(self.L.bem_batch_get_solution(self.h, i, _lib.ptr(x)), "batch_get_solution")
+        return x
+
+    def system(self, i: int):
+        m = self.meshes[i]
+        A = np.zeros((m.ndof, m.ndof), order="F")
+        F = np.zeros((m.ndof, self.nrhs[i]), order="F")
+        self._check(self.L.bem_batch_get_system(self.h, i, _lib.ptr(A), _lib.ptr(F)), "batch_get_system")
+        return A, F
+
+    def launches(self) -> int:
+        return int(self.L.bem_batch_launches(self.h))
+
+    def close(self):
+        if self.h:
+            self.L.bem_batch_destroy(self.h)
+            self.h = None
+
+
 def dgesv(A: np.ndarray, B: np.ndarray, ctx: Optional[_lib.Context] = None):
     """LAPACK dgesv on the GPU (solver_mod.f90:28).  Returns (LU, ipiv, X, info); the
     factors are those of the column-pivoted form documented in csrc/lu.cuh."""

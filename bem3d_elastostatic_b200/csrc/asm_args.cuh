@@ -1,0 +1,40 @@
+// Arguments of the assembly kernels for one system (one collocation row range).
+#pragma once
+
+#include "common.cuh"
+
+namespace bem {
+
+struct AsmArgs {
+  int n, ne, nbatches;
+  int in0, nrows_nodes;  // collocation nodes [in0, in0 + nrows_nodes)
+  const int* batches;
+  const int* nconec;
+  const int* kconec;
+  const int* kode;
+  const double* bc;
+  const int* uknown;
+  const double* vp;
+  const int* nesim;
+  const int* ke;
+  const double* x;
+  const double* y;
+  const double* z;
+  const double* tab;
+  Material mat;
+  double* A;  // mode A: (3n, 3n); mode HG: H
+  int64_t lda;
+  double* FI;  // mode A only
+  double* G;   // mode HG only
+  int64_t ldg;
+};
+
+// Batched H/G assembly of many systems (assembly.cu): d_args[i] describes system i
+// (mode HG: H into A with lda, G with ldg).  Regular pairs: one persistent launch over
+// the work items `tiles` ((system, 32-node tile), taken in order from `counter`,
+// which must be zero).  Singular pairs: one warp per node of every system, the
+// systems' node offsets in node_off (nsys + 1 entries).
+int launch_batch_hg(cudaStream_t stream, int sm_count, const AsmArgs* d_args, const int2* d_tiles, int ntiles,
+                    unsigned* counter, const int* d_node_off, int nsys, int total_nodes, long long* launches);
+
+}  // namespace bem

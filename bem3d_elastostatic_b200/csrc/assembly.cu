@@ -20,6 +20,9 @@
 //     reduction.  Launched after the regular kernel on the same stream.
 // The column swap (:125-218) uses a per-(node, component) lookup built on the host
 // from the same node->element adjacency the reference scans (uknown / vp).
+#include <algorithm>
+
+#include "asm_args.cuh"
 #include "common.cuh"
 #include "shape.cuh"
 
@@ -27,29 +30,6 @@ namespace bem {
 
 enum { kModeA = 0, kModeHG = 1 };
 
-struct AsmArgs {
-  int n, ne, nbatches;
-  int in0, nrows_nodes;  // collocation nodes [in0, in0 + nrows_nodes)
-  const int* batches;
-  const int* nconec;
-  const int* kconec;
-  const int* kode;
-  const double* bc;
-  const int* uknown;
-  const double* vp;
-  const int* nesim;
-  const int* ke;
-  const double* x;
-  const double* y;
-  const double* z;
-  const double* tab;
-  Material mat;
-  double* A;  // mode A: (3n, 3n); mode HG: H
-  int64_t lda;
-  double* FI;  // mode A only
-  double* G;   // mode HG only
-  int64_t ldg;
-};
 
 // symmetric 3x3 index (jj, ii) -> 0..5 : xx yy zz xy yz zx
 __device__ __forceinline__ int sym_idx(int a, int b) {
@@ -266,11 +246,11 @@ __device__ __forceinline__ void regular_pair(const AsmArgs& P, int e, const int*
 // from the element centroid (the near-field radius of stress_mod.f90:603-604) evaluate
 // and accumulate the Kelvin kernels in FP32; nearer pairs stay in FP64.
 template <int MODE, int PREC>
-__global__ void __launch_bounds__(256, 1) ghmat_regular_kernel(AsmArgs P) {
+__device__ __forceinline__ void regular_tile(const AsmArgs& P, int tile) {
   __shared__ double s_red[kBatch][32][12];
   const int w = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
-  const int local = blockIdx.x * 32 + lane;  // node offset inside the row range
+  const int local = tile * 32 + lane;  // node offset inside the row range
   const bool active = local < P.nrows_nodes;
   const int in = P.in0 + (active ? local : 0);
   const double xi0 = P.x[in], xi1 = P.y[in], xi2 = P.z[in];
@@ -357,6 +337,11 @@ __global__ void __launch_bounds__(256, 1) ghmat_regular_kernel(AsmArgs P) {
   }
 }
 
+template <int MODE, int PREC>
+__global__ void __launch_bounds__(256, 1) ghmat_regular_kernel(AsmArgs P) {
+  regular_tile<MODE, PREC>(P, blockIdx.x);
+}
+
 // ---------------------------------------------------------------------------------
 // singular elements
 // ---------------------------------------------------------------------------------
@@ -439,13 +424,10 @@ __device__ int sub_triangles(int ncone, int nodo, double v1[4][3], double v2[4][
   return cnt;
 }
 
+// one warp: collocation node `local` of the row range; s_part is the warp's scratch
 template <int MODE>
-__global__ void __launch_bounds__(128) ghmat_singular_kernel(AsmArgs P) {
-  __shared__ double s_part[4][27][18];
-  const int wib = threadIdx.x >> 5;
+__device__ __forceinline__ void singular_node(const AsmArgs& P, int local, double (*s_part)[18]) {
   const int lane = threadIdx.x & 31;
-  const int local = blockIdx.x * 4 + wib;
-  if (local >= P.nrows_nodes) return;  // warp-uniform
   const int in = P.in0 + local;
   const int64_t row = 3 * (int64_t)local;
   const int k = lane % 9;
@@ -521,14 +503,14 @@ __global__ void __launch_bounds__(128) ghmat_singular_kernel(AsmArgs P) {
     // combine the three point subsets of each node k
     if (s < 3)
       for (int p = 0; p < 9; ++p) {
-        s_part[wib][lane][p] = g[p];
-        s_part[wib][lane][9 + p] = h[p];
+        s_part[lane][p] = g[p];
+        s_part[lane][9 + p] = h[p];
       }
     __syncwarp();
     if (s == 0) {
       for (int p = 0; p < 9; ++p) {
-        g[p] = s_part[wib][k][p] + s_part[wib][k + 9][p] + s_part[wib][k + 18][p];
-        h[p] = s_part[wib][k][9 + p] + s_part[wib][k + 9][9 + p] + s_part[wib][k + 18][9 + p];
+        g[p] = s_part[k][p] + s_part[k + 9][p] + s_part[k + 18][p];
+        h[p] = s_part[k][9 + p] + s_part[k + 9][9 + p] + s_part[k + 18][9 + p];
       }
     }
     __syncwarp();
@@ -590,6 +572,15 @@ __global__ void __launch_bounds__(128) ghmat_singular_kernel(AsmArgs P) {
       for (int r = 0; r < 3; ++r) col[r] += dsum[r + 3 * ld];
     }
   }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(128) ghmat_singular_kernel(AsmArgs P) {
+  __shared__ double s_part[4][27][18];
+  const int wib = threadIdx.x >> 5;
+  const int local = blockIdx.x * 4 + wib;
+  if (local >= P.nrows_nodes) return;  // warp-uniform
+  singular_node<MODE>(P, local, s_part[wib]);
 }
 
 // Pinned DOFs: row := unit row, rhs := 0.
@@ -691,6 +682,73 @@ int launch_hg(bem_ctx* c, int in0, int in1, double* dH, int64_t ldh, double* dG,
   BEM_LAUNCH_CHECK(c);
   ghmat_singular_kernel<kModeHG><<<(P.nrows_nodes + 3) / 4, 128, 0, c->stream>>>(P);
   BEM_LAUNCH_CHECK(c);
+  return BEM_OK;
+}
+
+
+// ---------------------------------------------------------------------------------
+// batched H/G assembly of many systems
+// ---------------------------------------------------------------------------------
+
+// Persistent: every CTA takes (system, tile) items from a global counter until the
+// list is exhausted; the host orders the items by cost (largest systems first), so the
+// uneven systems of a batch balance over the SMs.  An item is the body of
+// ghmat_regular_kernel for that system's tile, with the system's arguments staged in
+// shared memory.
+__global__ void __launch_bounds__(256, 1)
+    batch_regular_kernel(const AsmArgs* __restrict__ args, const int2* __restrict__ tiles, int ntiles,
+                         unsigned* counter) {
+  __shared__ AsmArgs sP;
+  __shared__ int s_item;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = (int)atomicAdd(counter, 1u);
+    __syncthreads();
+    const int it = s_item;
+    if (it >= ntiles) return;
+    const int2 w = tiles[it];
+    if (threadIdx.x == 0) sP = args[w.x];
+    __syncthreads();
+    regular_tile<kModeHG, 0>(sP, w.y);
+    __syncthreads();
+  }
+}
+
+// one warp per node of any system: the system by binary search of the node offsets
+__global__ void __launch_bounds__(128)
+    batch_singular_kernel(const AsmArgs* __restrict__ args, const int* __restrict__ node_off, int nsys,
+                          int total_nodes) {
+  __shared__ double s_part[4][27][18];
+  __shared__ AsmArgs sP[4];
+  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gnode = blockIdx.x * 4 + wib;
+  if (gnode >= total_nodes) return;  // warp-uniform
+  int lo = 0, hi = nsys - 1;         // largest i with node_off[i] <= gnode
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(node_off + mid) <= gnode) lo = mid;
+    else hi = mid - 1;
+  }
+  if (lane == 0) sP[wib] = args[lo];
+  __syncwarp();
+  singular_node<kModeHG>(sP[wib], gnode - __ldg(node_off + lo), s_part[wib]);
+}
+
+int launch_batch_hg(cudaStream_t stream, int sm_count, const AsmArgs* d_args, const int2* d_tiles, int ntiles,
+                    unsigned* counter, const int* d_node_off, int nsys, int total_nodes, long long* launches) {
+  static bool constants = false;
+  if (!constants) {
+    if (cudaMemcpyToSymbol(s_gi, kGiQuad, sizeof(kGiQuad)) != cudaSuccess ||
+        cudaMemcpyToSymbol(s_ome, kOmeQuad, sizeof(kOmeQuad)) != cudaSuccess)
+      return BEM_ERR_CUDA;
+    constants = true;
+  }
+  if (cudaMemsetAsync(counter, 0, sizeof(unsigned), stream) != cudaSuccess) return BEM_ERR_CUDA;
+  batch_regular_kernel<<<std::max(1, std::min(ntiles, sm_count)), 256, 0, stream>>>(d_args, d_tiles, ntiles,
+                                                                                     counter);
+  if (cudaGetLastError() != cudaSuccess) return BEM_ERR_CUDA;
+  batch_singular_kernel<<<(total_nodes + 3) / 4, 128, 0, stream>>>(d_args, d_node_off, nsys, total_nodes);
+  if (cudaGetLastError() != cudaSuccess) return BEM_ERR_CUDA;
+  if (launches) *launches += 2;
   return BEM_OK;
 }
 

@@ -170,6 +170,8 @@ int bem_cuda_fail(bem_ctx* c, cudaError_t e, const char* where);
 // Internal (C++) entry points implemented in the .cu files.
 namespace bem {
 int launch_geometry(bem_ctx* c);
+int launch_geometry_arrays(cudaStream_t stream, int ne, const double* x, const double* y, const double* z,
+                           const int* nconec, const int* kconec, double* ref, double* tab);
 int launch_ghmat8(bem_ctx* c, int precision);
 int launch_hg(bem_ctx* c, int in0, int in1, double* dH, int64_t ldh, double* dG,
               int64_t ldg);

@@ -125,4 +125,20 @@ int launch_geometry(bem_ctx* c) {
   return BEM_OK;
 }
 
+
+// The same for raw arrays (the systems of a batch, with global node numbers in
+// kconec): ref receives the reference-layout tables (16 x 36 x ne doubles: eta1..3,
+// xja, xg1..3, then ff), tab the packed table (kTabStride x ne).
+int launch_geometry_arrays(cudaStream_t stream, int ne, const double* x, const double* y, const double* z,
+                           const int* nconec, const int* kconec, double* ref, double* tab) {
+  if (upload_quadrature_constants() != 0) return BEM_ERR_CUDA;
+  const size_t ng = (size_t)kGp * ne;
+  const int threads = 128;
+  const int64_t blocks = ((int64_t)ng + threads - 1) / threads;
+  etaxja_kernel<<<(unsigned)blocks, threads, 0, stream>>>(ne, x, y, z, nconec, kconec, ref, ref + ng,
+                                                          ref + 2 * ng, ref + 3 * ng, ref + 4 * ng,
+                                                          ref + 5 * ng, ref + 6 * ng, ref + 7 * ng, tab);
+  return cudaGetLastError() == cudaSuccess ? BEM_OK : BEM_ERR_CUDA;
+}
+
 }  // namespace bem

@@ -371,6 +371,51 @@ def uniaxial_cube(m: int, young: float = 1.0, nu: float = 0.3, side: float = 1.0
                 title=f"UNIT CUBE {m}x{m} QUAD9 PER FACE, UNIAXIAL STRESS")
 
 
+def loaded_box(lx: float, ly: float, lz: float, k: int, nu: float, young: float = 1.0,
+               top_tractions: Optional[np.ndarray] = None):
+    """Box [0,lx]x[0,ly]x[0,lz], k quad9 elements along every edge, supported like the
+    uniaxial cube (u_z = 0 on z = 0 and three pins), one load case per row of
+    top_tractions ((nrhs, 3): a uniform traction vector on z = lz; default one case,
+    t = (0, 0, 1)).  Returns (mesh, [bc per load case])."""
+    coords, kconec, faces = box_mesh(lx, ly, lz, k, k, k)
+    ne = kconec.shape[1]
+    kode = np.ones(3 * ne, dtype=np.int32)
+    top = [e for e, f in enumerate(faces) if f == "z1"]
+    for e, f in enumerate(faces):
+        if f == "z0":
+            kode[3 * e + 2] = 0
+    tt = np.array([[0.0, 0.0, 1.0]]) if top_tractions is None else np.asarray(top_tractions, dtype=np.float64)
+    bcs = []
+    for t in tt:
+        bc = np.zeros((27, ne), order="F")
+        for e in top:
+            for ld in range(3):
+                bc[ld::3, e] = t[ld]
+        bcs.append(bc)
+    i0 = _find_node(coords, (0.0, 0.0, 0.0))
+    i1 = _find_node(coords, (lx, 0.0, 0.0))
+    pins = np.array([3 * i0 + 0, 3 * i0 + 1, 3 * i1 + 1], dtype=np.int32)
+    mu = young / (2.0 * (1.0 + nu))
+    mesh = Mesh(coords[:, 0], coords[:, 1], coords[:, 2], np.full(ne, 9, np.int32), kconec, kode,
+                bcs[0], mu, nu, pins=pins, title=f"BOX {lx:g}x{ly:g}x{lz:g}, {k} QUAD9 PER EDGE")
+    return mesh, bcs
+
+
+def box_batch(count: int = 512, seed: int = 20261203, loads: int = 8):
+    """The batching workload: boxes with sides uniform in [0.5, 2], k in {1..6} quad9
+    elements per edge, nu uniform in [0.05, 0.45], E = 1, `loads` random top-face
+    traction vectors ~ N(0, 1) each, supports as the uniaxial cube."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        lx, ly, lz = rng.uniform(0.5, 2.0, size=3)
+        k = int(rng.integers(1, 7))
+        nu = float(rng.uniform(0.05, 0.45))
+        tt = rng.standard_normal((loads, 3))
+        out.append(loaded_box(lx, ly, lz, k, nu, 1.0, tt))
+    return out
+
+
 def cube_grid_points(vals: Iterable[float]) -> np.ndarray:
     v = np.asarray(list(vals), dtype=np.float64)
     g = np.stack(np.meshgrid(v, v, v, indexing="ij"), axis=-1).reshape(-1, 3)

@@ -156,6 +156,49 @@ int bem_internal_points(bem_ctx* ctx, int l, const double* cx, const double* cy,
                         const double* cz, double* u_int, double* sigma_int, double* prin,
                         double* vm, int flags);
 
+/* Batches of small systems (no counterpart in the reference, which solves one system
+ * per run).  Each system is a boundary mesh of its own (size, material, supports) with
+ * nrhs load cases: nrhs sets of prescribed values bc (27 x ne each, consecutive), the
+ * same kode.  The systems are assembled together (one geometry launch, one persistent
+ * work-queue launch for the regular pairs, one for the singular ones) and solved
+ * together (one CTA per system: LU, substitution for all load cases, FP64 residual),
+ * the solve captured once in a CUDA graph.  A node's prescribed displacement must be
+ * the same in every element that prescribes it (BEM_ERR_MESH otherwise). */
+typedef struct bem_batch bem_batch;
+
+typedef struct {
+  int systems;                 /* systems in the batch */
+  int sweeps;                  /* refinement sweeps in the solve graph (0 for FP64) */
+  int converged;               /* systems whose backward error reached tol */
+  int singular;                /* systems with an exactly zero pivot */
+  double max_backward_error;   /* over the systems and their load cases */
+  double solve_seconds;        /* device time of the whole solve (factor + sweeps) */
+  int lu_threads;              /* CTA size of the per-system LU picked by the autotuner */
+  float lu_ms_256, lu_ms_512;  /* the autotuner's timings of one batch LU */
+} bem_batch_info;
+
+int bem_batch_create(bem_batch** batch, int device);
+int bem_batch_destroy(bem_batch* batch);
+const char* bem_batch_last_error(const bem_batch* batch);
+/* adds one system (arguments as bem_set_mesh / bem_set_material / bem_set_bc /
+ * bem_set_pins; bc holds nrhs load cases, nrhs <= 8 and the same for every system);
+ * returns the system's index (>= 0) or an error (< 0) */
+int bem_batch_add(bem_batch* batch, int n, int ne, const double* x, const double* y,
+                  const double* z, const int* nconec, const int* kconec, double mu, double nu,
+                  const int* kode, int nrhs, const double* bc, int npins, const int* pins);
+/* geometry, H and G, then A and FI of every system */
+int bem_batch_assemble(bem_batch* batch);
+/* solve every system for all its load cases: BEM_PREC_FP64 (FP64 LU) or
+ * BEM_PREC_FP32_IR (FP32 LU, then max_iter FP64 refinement sweeps; a system stops
+ * once its backward error is <= tol or stops halving).  Order <= 25,600. */
+int bem_batch_solve(bem_batch* batch, int precision, double tol, int max_iter,
+                    bem_batch_info* info);
+/* system i: its solution x (3n x nrhs, column-major), its A (3n x 3n) and FI (3n x nrhs) */
+int bem_batch_get_solution(bem_batch* batch, int i, double* x);
+int bem_batch_get_system(bem_batch* batch, int i, double* A, double* FI);
+/* kernels the batch launched so far (graph launches counted by their kernels) */
+long long bem_batch_launches(const bem_batch* batch);
+
 /* Profiling of the library's own kernels.  bem_profile_begin zeroes the counters;
  * with timing = BEM_PROF_PHASES the LU phases are bracketed by CUDA events on the
  * context's stream (the stream every kernel of the context runs on); with
