@@ -199,7 +199,7 @@ class Batch:
     def assemble(self):
         self._check(self.L.bem_batch_assemble(self.h), "batch_assemble")
 
-    def solve(self, precision: str = "fp32-ir", tol: float = 1e-14, max_iter: int = 6) -> dict:
+    def solve(self, precision: str = "fp32-ir", tol: float = 1e-15, max_iter: int = 10) -> dict:
         st = _lib.BatchInfo()
         rc = self.L.bem_batch_solve(self.h, PRECISIONS[precision], tol, max_iter, _lib.C.byref(st))
         self.info = st.as_dict()

@@ -37,7 +37,7 @@ namespace bem {
 namespace {
 
 constexpr int kLuNB = 32;              // panel width of the per-system LU
-constexpr int kTile = 64;              // trailing-update tile (kTile x kTile)
+constexpr int kTM = 128, kTN = 64;     // trailing-update tile (kTM x kTN)
 constexpr int kMaxRhs = 8;             // load cases per system
 constexpr int kSolveThreads = 512;
 constexpr size_t kSolveSmem = 200 * 1024;  // substitution workspace per CTA
@@ -132,16 +132,18 @@ __device__ __forceinline__ void take_max(double& bv, int& bi, double v, int i) {
   }
 }
 
+// dynamic shared memory of the LU kernel: the L21 (kLuNB x kTM) and U12 (kLuNB x kTN) tiles
+template <typename T>
+constexpr size_t lu_smem() { return (size_t)kLuNB * (kTM + kTN) * sizeof(T); }
+
 template <typename T, int NT>
-__device__ void cta_getrf(T* A, int64_t lda, int N, int* ipiv, int* info) {
+__device__ void cta_getrf(T* A, int64_t lda, int N, int* ipiv, int* info, T* s_a, T* s_b) {
   __shared__ double s_v[NT / 32];
   __shared__ int s_i[NT / 32];
   __shared__ int s_piv[kLuNB];
   __shared__ int s_rows[2 * kLuNB], s_src[2 * kLuNB], s_nrows;
   __shared__ T s_row[kLuNB];
   __shared__ T s_L[kLuNB][kLuNB + 1];
-  __shared__ T s_a[kLuNB][kTile];  // L21 tile, k-major
-  __shared__ T s_b[kLuNB][kTile];  // U12 tile
   const int tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
   if (tid == 0) *info = 0;
   for (int j0 = 0; j0 < N; j0 += kLuNB) {
@@ -258,35 +260,42 @@ __device__ void cta_getrf(T* A, int64_t lda, int N, int* ipiv, int* info) {
         if (q < jb) col[q] = x[q];
     }
     __syncthreads();
-    // ---- A22 -= L21 U12, tiles of kTile x kTile ------------------------------------
+    // ---- A22 -= L21 U12, tiles of kTM x kTN: the tile of C is loaded with the operand
+    //      tiles, so a tile costs one memory round trip before its FMAs ---------------
     const int m = N - t0;
-    const int tiles = (m + kTile - 1) / kTile;
-    const int r = tid % kTile, cg = tid / kTile;           // output row, column group
-    constexpr int CPT = kTile * kTile / NT;                // columns per thread
-    for (int tt = 0; tt < tiles * tiles; ++tt) {
-      const int ti = tt % tiles, tj = tt / tiles;
-      const int rb = t0 + ti * kTile, cb = t0 + tj * kTile;
-      for (int idx = tid; idx < kLuNB * kTile; idx += NT) {
-        const int rr = idx % kTile, k = idx / kTile;       // L21(rb + rr, j0 + k)
-        s_a[k][rr] = (k < jb && rb + rr < N) ? A[rb + rr + (int64_t)(j0 + k) * lda] : T(0);
-        const int kk = idx % kLuNB, cc = idx / kLuNB;      // U12(j0 + kk, cb + cc)
-        s_b[kk][cc] = (kk < jb && cb + cc < N) ? A[j0 + kk + (int64_t)(cb + cc) * lda] : T(0);
+    const int tm = (m + kTM - 1) / kTM, tn = (m + kTN - 1) / kTN;
+    constexpr int CPT = kTM * kTN / NT;  // columns per thread
+    const int r = tid % kTM, cg = tid / kTM;
+    for (int tt = 0; tt < tm * tn; ++tt) {
+      const int ti = tt % tm, tj = tt / tm;
+      const int rb = t0 + ti * kTM, cb = t0 + tj * kTN;
+      for (int idx = tid; idx < kLuNB * kTM; idx += NT) {
+        const int rr = idx % kTM, k = idx / kTM;  // L21(rb + rr, j0 + k)
+        s_a[k * kTM + rr] = (k < jb && rb + rr < N) ? A[rb + rr + (int64_t)(j0 + k) * lda] : T(0);
+      }
+      for (int idx = tid; idx < kLuNB * kTN; idx += NT) {
+        const int kk = idx % kLuNB, cc = idx / kLuNB;  // U12(j0 + kk, cb + cc)
+        s_b[kk * kTN + cc] = (kk < jb && cb + cc < N) ? A[j0 + kk + (int64_t)(cb + cc) * lda] : T(0);
+      }
+      T acc[CPT];
+      const bool row_ok = rb + r < N;
+#pragma unroll
+      for (int q = 0; q < CPT; ++q) {
+        const int cc = cb + cg * CPT + q;
+        acc[q] = (row_ok && cc < N) ? A[rb + r + (int64_t)cc * lda] : T(0);
       }
       __syncthreads();
-      T acc[CPT];
-#pragma unroll
-      for (int q = 0; q < CPT; ++q) acc[q] = T(0);
 #pragma unroll 4
       for (int k = 0; k < kLuNB; ++k) {
-        const T l = s_a[k][r];
+        const T l = s_a[k * kTM + r];
 #pragma unroll
-        for (int q = 0; q < CPT; ++q) acc[q] = fma(l, s_b[k][cg * CPT + q], acc[q]);
+        for (int q = 0; q < CPT; ++q) acc[q] = fma(-l, s_b[k * kTN + cg * CPT + q], acc[q]);
       }
-      if (rb + r < N) {
+      if (row_ok) {
 #pragma unroll
         for (int q = 0; q < CPT; ++q) {
           const int cc = cb + cg * CPT + q;
-          if (cc < N) A[rb + r + (int64_t)cc * lda] -= acc[q];
+          if (cc < N) A[rb + r + (int64_t)cc * lda] = acc[q];
         }
       }
       __syncthreads();
@@ -297,6 +306,9 @@ __device__ void cta_getrf(T* A, int64_t lda, int N, int* ipiv, int* info) {
 template <typename T, int NT>
 __global__ void __launch_bounds__(NT) batch_lu_kernel(const SysDev* __restrict__ sys, const int* __restrict__ order,
                                                       int nsys, T* F, int* piv, int* info, unsigned* counter) {
+  extern __shared__ __align__(16) unsigned char lu_dyn[];
+  T* s_a = reinterpret_cast<T*>(lu_dyn);
+  T* s_b = s_a + kLuNB * kTM;
   __shared__ int s_item;
   for (;;) {
     if (threadIdx.x == 0) s_item = (int)atomicAdd(counter, 1u);
@@ -306,7 +318,7 @@ __global__ void __launch_bounds__(NT) batch_lu_kernel(const SysDev* __restrict__
     if (it >= nsys) return;
     const int s = order[it];
     const SysDev S = sys[s];
-    cta_getrf<T, NT>(F + S.f_off, S.lda, S.N, piv + S.piv_off, info + s);
+    cta_getrf<T, NT>(F + S.f_off, S.lda, S.N, piv + S.piv_off, info + s, s_a, s_b);
     __syncthreads();
   }
 }
@@ -322,6 +334,7 @@ __global__ void __launch_bounds__(kSolveThreads)
   extern __shared__ double sB[];
   __shared__ int s_item;
   __shared__ double s_x[kLuNB][kMaxRhs];
+  __shared__ double s_d[kLuNB][kLuNB + 1];
   const int tid = threadIdx.x, lane = tid & 31;
   for (;;) {
     if (tid == 0) s_item = (int)atomicAdd(counter, 1u);
@@ -354,11 +367,16 @@ __global__ void __launch_bounds__(kSolveThreads)
       // forward, unit lower, blocks of 32
       for (int j0 = 0; j0 < N; j0 += kLuNB) {
         const int jb = min(kLuNB, N - j0);
+        for (int idx = tid; idx < kLuNB * kLuNB; idx += kSolveThreads) {  // the diagonal block
+          const int rr = idx % kLuNB, cc = idx / kLuNB;
+          s_d[rr][cc] = (rr < jb && cc < jb) ? (double)A[j0 + rr + (int64_t)(j0 + cc) * S.lda] : 0.0;
+        }
+        __syncthreads();
         if (tid < 32) {
           double b[kMaxRhs];
           for (int r = 0; r < nc; ++r) b[r] = (lane < jb) ? sB[(j0 + lane) * nc + r] : 0.0;
           for (int t = 0; t < jb; ++t) {
-            const double l = (lane > t && lane < jb) ? (double)A[j0 + lane + (int64_t)(j0 + t) * S.lda] : 0.0;
+            const double l = (lane > t && lane < jb) ? s_d[lane][t] : 0.0;
             for (int r = 0; r < nc; ++r) {
               const double xt = __shfl_sync(0xffffffffu, b[r], t);
               b[r] = fma(-l, xt, b[r]);
@@ -385,12 +403,17 @@ __global__ void __launch_bounds__(kSolveThreads)
       // backward, non-unit upper, blocks of 32 from the last
       for (int j0 = ((N - 1) / kLuNB) * kLuNB; j0 >= 0; j0 -= kLuNB) {
         const int jb = min(kLuNB, N - j0);
+        for (int idx = tid; idx < kLuNB * kLuNB; idx += kSolveThreads) {
+          const int rr = idx % kLuNB, cc = idx / kLuNB;
+          s_d[rr][cc] = (rr < jb && cc < jb) ? (double)A[j0 + rr + (int64_t)(j0 + cc) * S.lda] : 0.0;
+        }
+        __syncthreads();
         if (tid < 32) {
           double b[kMaxRhs];
           for (int r = 0; r < nc; ++r) b[r] = (lane < jb) ? sB[(j0 + lane) * nc + r] : 0.0;
           for (int t = jb - 1; t >= 0; --t) {
-            const double d = (double)A[j0 + t + (int64_t)(j0 + t) * S.lda];
-            const double u = (lane < t) ? (double)A[j0 + lane + (int64_t)(j0 + t) * S.lda] : 0.0;
+            const double d = s_d[t][t];
+            const double u = (lane < t) ? s_d[lane][t] : 0.0;
             for (int r = 0; r < nc; ++r) {
               const double xt = __shfl_sync(0xffffffffu, b[r], t) / d;
               if (lane == t) b[r] = xt;
@@ -426,7 +449,7 @@ __global__ void __launch_bounds__(kSolveThreads)
 }
 
 // R = B - A X (FP64) and the backward error max_r ||R_r|| / (||A|| ||X_r|| + ||B_r||)
-// (infinity norms); conv[s] = 1 once it is <= tol, 2 once a sweep no longer halves it
+// (infinity norms); conv[s] = 1 once it is <= tol, 2 once a sweep gains less than 10 %
 __global__ void __launch_bounds__(kSolveThreads)
     batch_residual_kernel(const SysDev* __restrict__ sys, const int* __restrict__ order, int nsys,
                           const double* __restrict__ A, const double* __restrict__ B, const double* __restrict__ X,
@@ -515,7 +538,7 @@ __global__ void __launch_bounds__(kSolveThreads)
       berr[s] = be;
       if (!first) {
         if (be <= tol) conv[s] = 1;
-        else if (be > 0.5 * prev) conv[s] = 2;
+        else if (be > 0.9 * prev) conv[s] = 2;
       }
     }
     __syncthreads();
@@ -934,7 +957,14 @@ namespace {
 
 template <typename T, int NT>
 int launch_lu(bem_batch* b, T* F) {
-  bem::batch_lu_kernel<T, NT><<<std::min((int)b->sys.size(), b->sm_count), NT, 0, b->stream>>>(
+  static bool attr = false;
+  if (!attr) {
+    if (cudaFuncSetAttribute(bem::batch_lu_kernel<T, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)bem::lu_smem<T>()) != cudaSuccess)
+      return BEM_ERR_CUDA;
+    attr = true;
+  }
+  bem::batch_lu_kernel<T, NT><<<std::min((int)b->sys.size(), b->sm_count), NT, bem::lu_smem<T>(), b->stream>>>(
       b->dsys.p, b->ord.p, (int)b->sys.size(), F, b->piv.p, b->info.p, b->counters.p + 0);
   return cudaGetLastError() == cudaSuccess ? BEM_OK : BEM_ERR_CUDA;
 }

@@ -190,7 +190,7 @@ int bem_batch_add(bem_batch* batch, int n, int ne, const double* x, const double
 int bem_batch_assemble(bem_batch* batch);
 /* solve every system for all its load cases: BEM_PREC_FP64 (FP64 LU) or
  * BEM_PREC_FP32_IR (FP32 LU, then max_iter FP64 refinement sweeps; a system stops
- * once its backward error is <= tol or stops halving).  Order <= 25,600. */
+ * once its backward error is <= tol or a sweep gains less than 10 %).  Order <= 25,600. */
 int bem_batch_solve(bem_batch* batch, int precision, double tol, int max_iter,
                     bem_batch_info* info);
 /* system i: its solution x (3n x nrhs, column-major), its A (3n x 3n) and FI (3n x nrhs) */
