@@ -40,7 +40,7 @@ EXPORTS = [
     "bem_set_mesh",
     "bem_set_material", "bem_set_bc", "bem_set_pins", "bem_precompute_geometry",
     "bem_get_geometry", "bem_ghmat8", "bem_get_hg", "bem_solve", "bem_dgesv",
-    "bem_reorganize", "bem_boundary_stresses", "bem_internal_points", "bem_device_state",
+    "bem_reorganize", "bem_boundary_stresses", "bem_solve_transposed", "bem_adjoint_gradient", "bem_internal_points", "bem_device_state",
     "bem_internal_points_device", "bem_profile_begin", "bem_profile_end",
     "bem_dgesv_noalloc", "bem_batch_create", "bem_batch_destroy", "bem_batch_last_error",
     "bem_batch_add", "bem_batch_assemble", "bem_batch_solve", "bem_batch_get_solution",
@@ -131,6 +131,8 @@ def load(build_if_needed: bool = True):
     L.bem_dgesv_noalloc.argtypes = [C.c_int, C.c_int, _vp, C.c_int, _vp, _vp, C.c_int, _ip, _vp]
     L.bem_reorganize.argtypes = [_vp, _vp, _vp]
     L.bem_boundary_stresses.argtypes = [_vp, _vp, _vp, _vp, _vp]
+    L.bem_solve_transposed.argtypes = [_vp, _vp]
+    L.bem_adjoint_gradient.argtypes = [_vp, _vp, _vp, _vp]
     L.bem_internal_points.argtypes = [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int]
     L.bem_device_state.argtypes = [_vp, C.POINTER(C.c_void_p), C.POINTER(C.c_int64),
                                    C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]

@@ -40,6 +40,12 @@ class Quadesth:
         mesh.validate()
         self.mesh = mesh
         self.ctx = ctx or _lib.Context(device)
+        self.load_mesh()
+        self.solve_info: Optional[dict] = None
+
+    # input_data (io_mod.f90:36-146): the mesh's current arrays to the device
+    def load_mesh(self) -> None:
+        mesh = self.mesh
         L, h = self.ctx.L, self.ctx.h
         self._keep = [mesh.x, mesh.y, mesh.z, mesh.nconec, mesh.kconec, mesh.kode, mesh.bc, mesh.pins]
         c = self.ctx.check
@@ -49,7 +55,6 @@ class Quadesth:
         c(L.bem_set_bc(h, _lib.ptr(mesh.kode), _lib.ptr(mesh.bc)), "set_bc")
         c(L.bem_set_pins(h, int(mesh.pins.size), _lib.ptr(mesh.pins) if mesh.pins.size else None),
           "set_pins")
-        self.solve_info: Optional[dict] = None
 
     # assembly_mod.f90:28
     def precompute_element_geometry(self) -> None:

@@ -178,10 +178,13 @@ int launch_hg(bem_ctx* c, int in0, int in1, double* dH, int64_t ldh, double* dG,
 int lu_factor_fp64(bem_ctx* c, double* A, int64_t lda, int n, int* d_piv, int* info,
                    double* seconds);
 int lu_solve_fp64(bem_ctx* c, const double* LU, int64_t lda, int n, double* b);
+// the transposed system A^T y = b with the factors of lu_factor_fp64
+int lu_solve_t_fp64(bem_ctx* c, const double* LU, int64_t lda, int n, double* b);
 int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter,
                 bem_solve_info* stats, int* info);
 int launch_reorganize(bem_ctx* c);
 int launch_boundary_stresses(bem_ctx* c, double* se, double* sn, double* pr, double* vm);
+int launch_adjoint_gradient(bem_ctx* c, double* lam, double* grad, double* gmat);
 int launch_internal_points(bem_ctx* c, int l, const double* cx, const double* cy,
                            const double* cz, double* u, double* s, double* pr, double* vm,
                            int flags);

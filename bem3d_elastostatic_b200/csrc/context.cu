@@ -406,6 +406,39 @@ int bem_boundary_stresses(bem_ctx* c, double* sigma_elem, double* sigma_node, do
   return BEM_OK;
 }
 
+int bem_solve_transposed(bem_ctx* c, double* g) {
+  if (!c || !g) return BEM_ERR_ARG;
+  if (!c->factored_fp64 || !c->have_solution)
+    return bem_fail(c, BEM_ERR_STATE, "solve_transposed needs a solve with BEM_PREC_FP64 first");
+  BEM_CUDA(c, cudaSetDevice(c->device));
+  const size_t N = 3 * (size_t)c->n;
+  bem::DBuf<double> d;
+  BEM_CUDA(c, d.alloc(N));
+  BEM_CUDA(c, cudaMemcpyAsync(d.p, g, N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  int rc = bem::lu_solve_t_fp64(c, c->A.p, c->lda, (int)N, d.p);
+  if (rc) return rc;
+  BEM_CUDA(c, cudaMemcpyAsync(g, d.p, N * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  BEM_CUDA(c, cudaStreamSynchronize(c->stream));
+  return BEM_OK;
+}
+
+int bem_adjoint_gradient(bem_ctx* c, const double* lambda, double* grad_xyz, double* grad_mat) {
+  if (!c || !lambda || !grad_xyz || !grad_mat) return BEM_ERR_ARG;
+  if (!c->have_solution || !c->have_geometry) return bem_fail(c, BEM_ERR_STATE, "adjoint_gradient before solve");
+  BEM_CUDA(c, cudaSetDevice(c->device));
+  int rc = bem::launch_reorganize(c);  // u and t of the current solution
+  if (rc) return rc;
+  const size_t N = 3 * (size_t)c->n;
+  bem::DBuf<double> d;
+  BEM_CUDA(c, d.alloc(2 * N + 2));
+  BEM_CUDA(c, cudaMemcpyAsync(d.p, lambda, N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  if ((rc = bem::launch_adjoint_gradient(c, d.p, d.p + N, d.p + 2 * N))) return rc;
+  BEM_CUDA(c, cudaMemcpyAsync(grad_xyz, d.p + N, N * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  BEM_CUDA(c, cudaMemcpyAsync(grad_mat, d.p + 2 * N, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  BEM_CUDA(c, cudaStreamSynchronize(c->stream));
+  return BEM_OK;
+}
+
 int bem_internal_points_device(bem_ctx* c, int l, const double* cx, const double* cy, const double* cz,
                                double* u, double* s, double* pr, double* vm, int flags) {
   if (!c || l < 0) return BEM_ERR_ARG;

@@ -895,6 +895,181 @@ __global__ void permute_kernel(int n, const int* __restrict__ perm, const double
   if (i < n) x[i] = v[perm[i]];
 }
 
+// ---- the transposed solve: S^T x = b with the same factors --------------------------
+// S^T = T = P L U, so x = U^{-1} L^{-1} P^T b, where L_T(i, j) = S(j, i) (j < i, unit)
+// and U_T(i, j) = S(j, i) (j >= i).  The sweeps read the factor transposed: a solved
+// block j contributes S(block j rows, column i) . y_j to every target column i, one
+// warp per column (coalesced 32-row segments); diagonal blocks are staged transposed
+// with a padded leading dimension.
+constexpr int kLdT = kSolveBlock + 1;
+
+template <typename T>
+__device__ void warp_lower_unit_solve_t(const T* D, int jb, double* w) {
+  const int lane = threadIdx.x & 31;
+  double x[kSolveBlock / 32];
+#pragma unroll
+  for (int q = 0; q < kSolveBlock / 32; ++q) x[q] = (lane + 32 * q < jb) ? w[lane + 32 * q] : 0.0;
+#pragma unroll
+  for (int slot = 0; slot < kSolveBlock / 32; ++slot) {
+#pragma unroll
+    for (int o = 0; o < 32; ++o) {
+      const int cidx = slot * 32 + o;
+      if (cidx < jb) {
+        const double xc = __shfl_sync(0xffffffffu, x[slot], o);
+#pragma unroll
+        for (int q = slot; q < kSolveBlock / 32; ++q) {
+          const int r = lane + 32 * q;
+          if (r > cidx) x[q] = fma(-(double)D[r + cidx * kLdT], xc, x[q]);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < kSolveBlock / 32; ++q)
+    if (lane + 32 * q < jb) w[lane + 32 * q] = x[q];
+}
+
+template <typename T>
+__device__ void warp_upper_solve_t(const T* D, const double* rdiag, int jb, double* w) {
+  const int lane = threadIdx.x & 31;
+  double x[kSolveBlock / 32];
+#pragma unroll
+  for (int q = 0; q < kSolveBlock / 32; ++q) x[q] = (lane + 32 * q < jb) ? w[lane + 32 * q] : 0.0;
+#pragma unroll
+  for (int slot = kSolveBlock / 32 - 1; slot >= 0; --slot) {
+#pragma unroll
+    for (int o = 31; o >= 0; --o) {
+      const int cidx = slot * 32 + o;
+      if (cidx < jb) {
+        const double xc = __shfl_sync(0xffffffffu, x[slot], o) * rdiag[cidx];
+        if (lane == o) x[slot] = xc;
+#pragma unroll
+        for (int q = 0; q <= slot; ++q) {
+          const int r = lane + 32 * q;
+          if (r < cidx) x[q] = fma(-(double)D[r + cidx * kLdT], xc, x[q]);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < kSolveBlock / 32; ++q)
+    if (lane + 32 * q < jb) w[lane + 32 * q] = x[q];
+}
+
+// UPPER = false: forward with L_T (blocks first to last); true: backward with U_T
+template <typename T, bool UPPER>
+__global__ void __launch_bounds__(kSweepThreads, 1)
+    sweep_t_kernel(const T* __restrict__ S, int64_t lda, int n, double* b, unsigned* flags, unsigned tag,
+                   int* status) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* D = reinterpret_cast<T*>(smem_raw);  // [kSolveBlock][kLdT]: D[r + c * kLdT] = T(k0 + r, k0 + c)
+  __shared__ double ys[kSolveBlock];
+  __shared__ double wn[kSolveBlock];
+  __shared__ double rdiag[kSolveBlock];
+  __shared__ int s_abort;
+  const int t = threadIdx.x, G = gridDim.x, g = blockIdx.x, lane = t & 31, wp = t >> 5;
+  const int nblk = (n + kSolveBlock - 1) / kSolveBlock;
+  auto blk0 = [&](int s) { return (UPPER ? nblk - 1 - s : s) * kSolveBlock; };
+  auto stage_diag = [&](int s) {
+    const int k0 = blk0(s), kb = min(kSolveBlock, n - k0);
+    for (int idx = t; idx < kSolveBlock * kSolveBlock; idx += kSweepThreads) {
+      const int a = idx % kSolveBlock, c = idx / kSolveBlock;  // S(k0 + a, k0 + c) = T(k0 + c, k0 + a)
+      const bool in = a < kb && c < kb && (UPPER ? (c <= a) : (c > a));
+      D[c + a * kLdT] = in ? S[(k0 + a) + (int64_t)(k0 + c) * lda] : T(0);
+    }
+  };
+  auto solve = [&](int s) {
+    const int k0 = blk0(s), kb = min(kSolveBlock, n - k0);
+    if (t < kb) wn[t] = b[k0 + t];
+    if (UPPER && t < kSolveBlock) rdiag[t] = (t < kb) ? 1.0 / (double)D[t + t * kLdT] : 0.0;
+    __syncthreads();
+    if (t < 32) {
+      if (UPPER)
+        warp_upper_solve_t<T>(D, rdiag, kb, wn);
+      else
+        warp_lower_unit_solve_t<T>(D, kb, wn);
+    }
+    __syncthreads();
+    if (t < kb) b[k0 + t] = wn[t];
+    __syncthreads();
+    if (t == 0) {
+      __threadfence();
+      st_release_u32(flags + s, tag);
+    }
+    if (s + G < nblk) stage_diag(s + G);
+  };
+
+  if (t == 0) s_abort = 0;
+  if (g < nblk) stage_diag(g);
+  __syncthreads();
+  if (g == 0) solve(0);
+  for (int s = 0; s + 1 < nblk; ++s) {
+    int s2 = s + 1 + ((g - (s + 1)) % G + G) % G;
+    if (s2 >= nblk) break;
+    if (t == 0 && s % G != g) {
+      const unsigned long long t0 = globaltimer_ns();
+      unsigned it = 0;
+      while (ld_acquire_u32(flags + s) != tag) {
+        if ((++it & 255u) == 0 && globaltimer_ns() - t0 > 2000000000ull) {
+          atomicExch(status, BEM_ERR_TIMEOUT);
+          s_abort = 1;
+          break;
+        }
+      }
+      __threadfence();
+    }
+    __syncthreads();
+    if (s_abort) return;
+    const int c0 = blk0(s), cb = min(kSolveBlock, n - c0);
+    if (t < kSolveBlock) ys[t] = (t < cb) ? __ldcg(b + c0 + t) : 0.0;
+    __syncthreads();
+    for (; s2 < nblk; s2 += G) {
+      const int r0 = blk0(s2), rb = min(kSolveBlock, n - r0);
+      // warp wp takes target columns r0 + wp, r0 + wp + 16, ...: dot of the solved rows
+      for (int i = wp; i < rb; i += kSweepThreads / 32) {
+        const T* p = S + c0 + (int64_t)(r0 + i) * lda;
+        double acc = 0.0;
+#pragma unroll
+        for (int u = 0; u < kSolveBlock / 32; ++u) {
+          const int j = lane + 32 * u;
+          if (j < cb) acc = fma((double)p[j], ys[j], acc);
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+        if (lane == 0) b[r0 + i] -= acc;
+      }
+      __syncthreads();
+      if (s2 == s + 1) solve(s2);
+    }
+  }
+}
+
+__global__ void scatter_kernel(int n, const int* __restrict__ perm, const double* __restrict__ v,
+                               double* __restrict__ x) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) x[perm[i]] = v[i];
+}
+
+template <typename T, bool UPPER>
+int sweep_t_launch(bem_ctx* c, const T* S, int64_t lda, int n, double* b, unsigned* flags, unsigned tag,
+                   int* status) {
+  static int ok[2][2] = {{0, 0}, {0, 0}};
+  const size_t dsm = (size_t)kSolveBlock * kLdT * sizeof(T);
+  int& per_sm = ok[sizeof(T) == 8][UPPER ? 1 : 0];
+  if (per_sm == 0) {
+    BEM_CUDA(c, cudaFuncSetAttribute(sweep_t_kernel<T, UPPER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm));
+    BEM_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_t_kernel<T, UPPER>, kSweepThreads, dsm));
+    if (per_sm < 1) return bem_fail(c, BEM_ERR_CUDA, "transposed sweep kernel does not fit on an SM");
+  }
+  const int nblk = (n + kSolveBlock - 1) / kSolveBlock;
+  const int G = std::min(nblk, c->sm_count);
+  void* args[] = {(void*)&S, (void*)&lda, (void*)&n, (void*)&b, (void*)&flags, (void*)&tag, (void*)&status};
+  BEM_CUDA(c, cudaLaunchCooperativeKernel((void*)sweep_t_kernel<T, UPPER>, dim3(G), dim3(kSweepThreads), args, dsm,
+                                          c->stream));
+  ++c->launches;
+  return BEM_OK;
+}
+
 template <typename T, bool UPPER>
 int sweep_launch(bem_ctx* c, const T* S, int64_t lda, int n, double* b, unsigned* flags, unsigned tag,
                  int* status) {
@@ -933,6 +1108,35 @@ int lu_solve_ws(bem_ctx* c, const T* S, int64_t lda, int n, const int* perm, dou
   BEM_CUDA(c, cudaStreamSynchronize(c->stream));
   if (st != 0) return bem_fail(c, st, "triangular solve: a wait for a solved block timed out");
   return BEM_OK;
+}
+
+// b := S^{-T} b with the factors of lu_factor (the transposed system, same factors)
+template <typename T>
+int lu_solve_t_ws(bem_ctx* c, const T* S, int64_t lda, int n, const int* perm, double* b, double* work) {
+  const int nblk = (n + kSolveBlock - 1) / kSolveBlock;
+  unsigned* flags = reinterpret_cast<unsigned*>(work + n);
+  int* status = reinterpret_cast<int*>(flags + nblk);
+  BEM_CUDA(c, cudaMemsetAsync(flags, 0, (nblk + 1) * sizeof(unsigned), c->stream));
+  scatter_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(n, perm, b, work);  // P^T b
+  BEM_LAUNCH_CHECK(c);
+  int rc;
+  if ((rc = sweep_t_launch<T, false>(c, S, lda, n, work, flags, 1u, status))) return rc;
+  if ((rc = sweep_t_launch<T, true>(c, S, lda, n, work, flags, 2u, status))) return rc;
+  BEM_CUDA(c, cudaMemcpyAsync(b, work, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  int st = 0;
+  BEM_CUDA(c, cudaMemcpyAsync(&st, status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  BEM_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (st != 0) return bem_fail(c, st, "transposed solve: a wait for a solved block timed out");
+  return BEM_OK;
+}
+
+int lu_solve_t_fp64(bem_ctx* c, const double* LU, int64_t lda, int n, double* b) {
+  const size_t need = lu_solve_work_count(n);
+  if (c->work.count < need) {
+    c->work.release();
+    BEM_CUDA(c, c->work.alloc(need));
+  }
+  return lu_solve_t_ws<double>(c, LU, lda, n, c->perm.p, b, c->work.p);
 }
 
 template <typename T>

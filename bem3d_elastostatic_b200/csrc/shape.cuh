@@ -8,7 +8,7 @@ namespace bem {
 // quad9 node order: 1:(-1,-1) 2:(0,-1) 3:(1,-1) 4:(1,0) 5:(1,1) 6:(0,1) 7:(-1,1)
 // 8:(-1,0) 9:(0,0); tri6: 1:(1,0,0) 2:(0,1,0) 3:(0,0,1) 4..6 mid-sides.
 template <typename T>
-__device__ __forceinline__ void shape_fn(int ncone, T g1, T g2, T* f, T* fd1, T* fd2) {
+__host__ __device__ __forceinline__ void shape_fn(int ncone, T g1, T g2, T* f, T* fd1, T* fd2) {
   const T one = T(1), two = T(2), half = T(0.5), qtr = T(0.25), four = T(4);
   if (ncone == 9) {
     f[0] = qtr * g1 * g2 * (g1 - one) * (g2 - one);

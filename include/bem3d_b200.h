@@ -142,6 +142,17 @@ int bem_dgesv_noalloc(int n, int nrhs, double* dA, int lda, int* d_ipiv, double*
  * DFI (27, ne) element-nodal tractions.  Host outputs nullable. */
 int bem_reorganize(bem_ctx* ctx, double* FI_out, double* DFI_out);
 
+/* Adjoint (no counterpart in the reference).  bem_solve_transposed solves A^T y = g
+ * (g: host, 3n, overwritten by y) with the factors of the last BEM_PREC_FP64 bem_solve.
+ * bem_adjoint_gradient returns, for lambda (host, 3n), the derivative of
+ * R = lambda^T (FI - A x) at the current solution x with respect to the node
+ * coordinates, grad_xyz (3n: x, y, z of node 1, ...), and to the material, grad_mat
+ * ([d/dmu, d/dnu]), without forming dA/dX.  With lambda = A^{-T} dJ/dx this is the
+ * implicit part of dJ/dX for any objective J(x, X); pinned rows carry no geometry and
+ * their lambda is ignored.  9-node elements. */
+int bem_solve_transposed(bem_ctx* ctx, double* g);
+int bem_adjoint_gradient(bem_ctx* ctx, const double* lambda, double* grad_xyz, double* grad_mat);
+
 /* compute_boundary_stresses (stress_mod.f90:119-406): traction-recovery stresses at
  * every node of every element, sigma_elem (6, 9, ne) (nullable), their average over
  * each node's elements, sigma_node (6, n), and the nodal principal (3, n) and von
