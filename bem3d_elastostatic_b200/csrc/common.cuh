@@ -81,6 +81,29 @@ struct DBuf {
   size_t bytes() const { return count * sizeof(T); }
 };
 
+// A factorisation's launch sequence captured as a CUDA graph and replayed while every
+// pointer and size it was captured with (the key) is unchanged, so that the ~10^4
+// launches of a large factorisation neither wait on the host nor pay per-launch costs.
+// The profile events the capture recorded are kept to be read after each replay.
+struct LUGraph {
+  cudaGraphExec_t exec = nullptr;
+  std::vector<long long> key;
+  struct Ev {
+    int phase, a, b;
+    double flops, bytes;
+  };
+  std::vector<Ev> ev;
+  long long launches = 0;  // kernels per replay
+  void reset() {
+    if (exec) cudaGraphExecDestroy(exec);
+    exec = nullptr;
+    key.clear();
+    ev.clear();
+    launches = 0;
+  }
+  ~LUGraph() { reset(); }
+};
+
 }  // namespace bem
 
 // The opaque context behind bem_ctx*.
@@ -131,6 +154,24 @@ struct bem_ctx {
   bem::DBuf<unsigned int> sync;
   bem::DBuf<int> status;
   bem::DBuf<double> rowscale, colscale;
+  // refinement vectors (residual, correction) and timing events, kept: allocation and
+  // release next to a 10^10-byte system stalled the host for up to 0.7 s per solve
+  bem::DBuf<double> ir_r, ir_d;
+  cudaEvent_t solve_ev[3] = {nullptr, nullptr, nullptr};
+  // FP64 inverses of the 128 x 128 diagonal blocks of the latest factorisation (for the
+  // block-inverse sweeps) and the sweeps' publication slots; dinv_src/n/lda/elem name
+  // the factors the inverses belong to (cleared by every new factorisation)
+  bem::DBuf<double> dinv;
+  bem::DBuf<unsigned long long> slots;
+  const void* dinv_src = nullptr;
+  int dinv_n = 0, dinv_elem = 0;
+  int64_t dinv_lda = 0;
+  // factorisation workspace (kept, so that captured factorisations can be replayed)
+  // and the captured factorisations, one per factor type (0 FP32, 1 FP64)
+  bem::DBuf<unsigned char> lu_scratch[2];
+  bem::LUGraph lu_graph[2][4];  // up to four captured variants per factor type
+  int lu_graph_next[2] = {0, 0};  // the slot a new capture replaces when all are taken
+  bool lu_graph_off = false;  // set when capture is unavailable (or BEM_LU_GRAPH=0)
   // GEMM flavour of the LU trailing update: f64_gemm 1 = DMMA tensor path, 0 = SIMT;
   // f32_gemm 4 = BF16 x3 split on tcgen05 for the trailing update (mma.sync elsewhere),
   // 3 = BF16 x3 split on mma.sync, 1 = plain BF16 (mma.sync), 0 = SIMT FP32
@@ -146,7 +187,11 @@ struct bem_ctx {
   bem_profile prof{};
   std::vector<cudaEvent_t> ev_pool;  // timing events of the LU phase profile, reused
   ~bem_ctx() {
+    for (auto& t : lu_graph)
+      for (auto& g : t) g.reset();
     for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
+    for (cudaEvent_t e : solve_ev)
+      if (e) cudaEventDestroy(e);
   }
 };
 

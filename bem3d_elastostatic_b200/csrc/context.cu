@@ -261,6 +261,7 @@ int bem_ghmat8(bem_ctx* c, int asm_precision, double* A_out, int64_t lda_out, do
   BEM_CUDA(c, cudaSetDevice(c->device));
   const int64_t N = 3 * (int64_t)c->n;
   if (A_out && lda_out < N) return bem_fail(c, BEM_ERR_ARG, "ghmat8: lda < 3n");
+  c->dinv_src = nullptr;  // A is overwritten: inverses of earlier factors are stale
   int rc = bem::launch_ghmat8(c, asm_precision);
   if (rc) return rc;
   if (A_out)

@@ -410,6 +410,7 @@ int gemm_bf16(bem_ctx* c, int M, int N, int K, const float* A, int64_t lda, cons
               int64_t ldc, int mode, int split);
 bool gemm_tc_ok(const void* A, int64_t lda, const void* B, int64_t ldb, int elem);
 bool umma_supported(int K);
+int umma_reserve(bem_ctx* c, int M, int N, int K);
 int gemm_umma_bf16x3(bem_ctx* c, int M, int N, int K, const float* A, int64_t lda, const float* B, int64_t ldb,
                      float* C, int64_t ldc);
 
@@ -498,11 +499,7 @@ int panel_launch(bem_ctx* c, const LUWorkspace& ws, T* S, int64_t lda, int n, in
 struct LUProfile {
   bool on = false;
   bem_ctx* c = nullptr;
-  struct Ev {
-    int phase;
-    int a, b;  // indices into c->ev_pool
-    double flops, bytes;
-  };
+  using Ev = LUGraph::Ev;  // phase, then indices a, b into c->ev_pool, then flops, bytes
   std::vector<Ev> ev;
   size_t used = 0;
   int cur = -1, start = -1;
@@ -513,7 +510,9 @@ struct LUProfile {
       if (cudaEventCreate(&e) != cudaSuccess) return -1;
       c->ev_pool.push_back(e);
     }
-    cudaEventRecord(c->ev_pool[used], s);
+    // External: inside a stream capture the record becomes a graph node (a plain
+    // record there is only a capture dependency and cannot be timed)
+    if (cudaEventRecordWithFlags(c->ev_pool[used], s, cudaEventRecordExternal) != cudaSuccess) return -1;
     return (int)used++;
   }
   // trailing-only mode times the trailing update of every 16th panel (events between
@@ -537,8 +536,12 @@ struct LUProfile {
     long long cnt = 0;
     for (auto& e : ev) {
       float ms = 0.f;
-      cudaEventSynchronize(c->ev_pool[e.b]);
-      cudaEventElapsedTime(&ms, c->ev_pool[e.a], c->ev_pool[e.b]);
+      // a failed query costs the sample only, never a later launch check
+      if (cudaEventSynchronize(c->ev_pool[e.b]) != cudaSuccess ||
+          cudaEventElapsedTime(&ms, c->ev_pool[e.a], c->ev_pool[e.b]) != cudaSuccess) {
+        cudaGetLastError();
+        ms = 0.f;
+      }
       t[e.phase] += ms;
       if (e.phase == 4) {
         ++cnt;
@@ -596,13 +599,7 @@ LUWorkspace lu_workspace_carve(void* base, int n, int nb, int gmax, int elem) {
 size_t lu_solve_work_count(int n) { return ((size_t)n + 127) / 128 * 256 + 256; }
 
 template <typename T>
-int lu_factor(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int* perm, int nb, int* info) {
-  DBuf<unsigned char> scratch;
-  const int gmax = c->sm_count;
-  BEM_CUDA(c, scratch.alloc(lu_workspace_bytes(n, nb, gmax, sizeof(T))));
-  const LUWorkspace ws = lu_workspace_carve(scratch.p, n, nb, gmax, sizeof(T));
-  return lu_factor_ws<T>(c, S, lda, n, piv, perm, nb, info, ws);
-}
+int lu_prepare_inverses(bem_ctx* c, const T* S, int64_t lda, int n);
 
 // x = P v with P = tau_0 tau_1 ... tau_{n-1} (tau_i swaps i and piv[i]) as a gather
 // x[i] = v[perm[i]]; composed on the host once per factorisation
@@ -617,27 +614,29 @@ static int make_perm(bem_ctx* c, const int* d_piv, int n, int* d_perm) {
   return BEM_OK;
 }
 
+static LUProfile make_profile(bem_ctx* c) {
+  LUProfile prof;
+  prof.c = c;
+  prof.on = getenv("BEM_LU_PROFILE") != nullptr || c->prof_timing != BEM_PROF_COUNT;
+  prof.trailing_only = c->prof_timing == BEM_PROF_TRAILING && getenv("BEM_LU_PROFILE") == nullptr;
+  return prof;
+}
+
+// The factorisation's launches, in stream order with no host synchronisation (so that
+// they can be captured as a graph).
 template <typename T>
-int lu_factor_ws(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int* perm, int nb, int* info,
-                 const LUWorkspace& ws) {
-  *info = 0;
+static int lu_factor_enqueue(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int nb, const LUWorkspace& ws,
+                             LUProfile& prof) {
   // barrier counter (offset 0) and status words (offset 8) of the workspace's sync slot
   BEM_CUDA(c, cudaMemsetAsync(ws.barrier, 0, 16, c->stream));
   unsigned bar_base = 0;
-  if (sizeof(T) == 4 && c->f32_gemm == 4) {
-    if (c->umma_err.count < 1) BEM_CUDA(c, c->umma_err.alloc(1));
-    BEM_CUDA(c, cudaMemsetAsync(c->umma_err.p, 0, sizeof(int), c->stream));
-  }
+  if (sizeof(T) == 4 && c->f32_gemm == 4) BEM_CUDA(c, cudaMemsetAsync(c->umma_err.p, 0, sizeof(int), c->stream));
   T* V = reinterpret_cast<T*>(ws.inv);
   T* Y = reinterpret_cast<T*>(ws.ybuf);
   const int64_t ldy = ws.ldy;
   const size_t inv_smem = (size_t)kInvBlock * kInvBlock * sizeof(T);
   cudaFuncSetAttribute(inv_unit_upper_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inv_smem);
   int rc;
-  LUProfile prof;
-  prof.c = c;
-  prof.on = getenv("BEM_LU_PROFILE") != nullptr || c->prof_timing != BEM_PROF_COUNT;
-  prof.trailing_only = c->prof_timing == BEM_PROF_TRAILING && getenv("BEM_LU_PROFILE") == nullptr;
   for (int j0 = 0; j0 < n; j0 += nb) {
     const int jb = std::min(nb, n - j0);
     prof.panel = j0 / nb;
@@ -695,6 +694,13 @@ int lu_factor_ws(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int* perm, int 
       prof.end(c->stream, 2.0 * m * (double)m * jb, (2.0 * m * (double)m + 2.0 * m * (double)jb) * sizeof(T));
     }
   }
+  return BEM_OK;
+}
+
+// After the launches: the phase profile, the status words and the gather form of P.
+template <typename T>
+static int lu_factor_finish(bem_ctx* c, int n, int* piv, int* perm, int* info, const LUWorkspace& ws,
+                            LUProfile& prof) {
   prof.report(c, n);
   int st[2];
   BEM_CUDA(c, cudaMemcpyAsync(st, ws.status, sizeof(st), cudaMemcpyDeviceToHost, c->stream));
@@ -708,6 +714,104 @@ int lu_factor_ws(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int* perm, int 
   *info = st[1];
   if (*info == 0 && perm) return make_perm(c, piv, n, perm);
   return BEM_OK;
+}
+
+template <typename T>
+int lu_factor_ws(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int* perm, int nb, int* info,
+                 const LUWorkspace& ws) {
+  *info = 0;
+  c->dinv_src = nullptr;  // the diagonal-block inverses belong to earlier factors
+  if (sizeof(T) == 4 && c->f32_gemm == 4 && c->umma_err.count < 1) BEM_CUDA(c, c->umma_err.alloc(1));
+  LUProfile prof = make_profile(c);
+  const int rc = lu_factor_enqueue<T>(c, S, lda, n, piv, nb, ws, prof);
+  if (rc) return rc;
+  return lu_factor_finish<T>(c, n, piv, perm, info, ws, prof);
+}
+
+// The context's factorisation: workspace kept in the context, the launch sequence
+// captured once per (factors, order, panel width, workspace, GEMM buffers, profile mode)
+// and replayed, then the diagonal-block inverses of the solve.  Capture that the
+// runtime refuses (or BEM_LU_GRAPH=0) leaves plain launches.
+template <typename T>
+int lu_factor(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int* perm, int nb, int* info) {
+  *info = 0;
+  c->dinv_src = nullptr;
+  const int ti = sizeof(T) == 8 ? 1 : 0;
+  const int gmax = c->sm_count;
+  const size_t bytes = lu_workspace_bytes(n, nb, gmax, sizeof(T));
+  if (c->lu_scratch[ti].count < bytes) {
+    c->lu_scratch[ti].release();
+    BEM_CUDA(c, c->lu_scratch[ti].alloc(bytes));
+  }
+  const LUWorkspace ws = lu_workspace_carve(c->lu_scratch[ti].p, n, nb, gmax, sizeof(T));
+  if (sizeof(T) == 4 && c->f32_gemm == 4) {
+    int rc0;
+    if (n > nb && (rc0 = umma_reserve(c, n - nb, n - nb, nb))) return rc0;
+    if (c->umma_err.count < 1) BEM_CUDA(c, c->umma_err.alloc(1));
+  }
+  if (const char* e = getenv("BEM_LU_GRAPH"))
+    if (atoi(e) == 0) c->lu_graph_off = true;
+  LUProfile prof = make_profile(c);
+  auto make_key = [&]() {
+    return std::vector<long long>{(long long)(uintptr_t)S,  lda, n, nb, (long long)(uintptr_t)piv,
+                                  (long long)(uintptr_t)ws.cand_val, (long long)(uintptr_t)c->umma_buf.p,
+                                  (long long)c->umma_buf.count, (long long)(uintptr_t)c->umma_err.p,
+                                  c->f32_gemm, c->f64_gemm, prof.on, prof.trailing_only, c->sm_count};
+  };
+  int rc = BEM_OK;
+  if (c->lu_graph_off) {
+    rc = lu_factor_enqueue<T>(c, S, lda, n, piv, nb, ws, prof);
+  } else {
+    const std::vector<long long> key = make_key();
+    LUGraph* hit = nullptr;
+    for (auto& g : c->lu_graph[ti])
+      if (g.exec && g.key == key) hit = &g;
+    if (hit) {
+      BEM_CUDA(c, cudaGraphLaunch(hit->exec, c->stream));
+      c->launches += hit->launches;
+      prof.ev = hit->ev;
+    } else {
+      LUGraph* slot = nullptr;
+      for (auto& g : c->lu_graph[ti])
+        if (!slot && !g.exec) slot = &g;
+      if (!slot) {
+        slot = &c->lu_graph[ti][c->lu_graph_next[ti]];
+        c->lu_graph_next[ti] = (c->lu_graph_next[ti] + 1) % 4;
+      }
+      LUGraph& gr = *slot;
+      gr.reset();
+      const long long l0 = c->launches;
+      cudaGraph_t g = nullptr;
+      BEM_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
+      rc = lu_factor_enqueue<T>(c, S, lda, n, piv, nb, ws, prof);
+      cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+      cudaGraphExec_t ex = nullptr;
+      if (rc == BEM_OK && e == cudaSuccess) e = cudaGraphInstantiate(&ex, g, 0);
+      if (g) cudaGraphDestroy(g);
+      if (rc == BEM_OK && e == cudaSuccess) {
+        gr.exec = ex;
+        gr.key = make_key();  // the trailing update may have grown its buffers while captured
+        gr.ev = prof.ev;
+        gr.launches = c->launches - l0;
+        BEM_CUDA(c, cudaGraphLaunch(ex, c->stream));
+      } else {
+        // no capture: plain launches from now on
+        if (getenv("BEM_LU_PROFILE"))
+          fprintf(stderr, "[lu] graph capture unavailable (%s; %s): plain launches\n", cudaGetErrorString(e),
+                  rc ? c->last_error.c_str() : "");
+        if (ex) cudaGraphExecDestroy(ex);
+        cudaGetLastError();
+        c->lu_graph_off = true;
+        c->launches = l0;
+        prof = make_profile(c);
+        rc = lu_factor_enqueue<T>(c, S, lda, n, piv, nb, ws, prof);
+      }
+    }
+  }
+  if (rc) return rc;
+  rc = lu_factor_finish<T>(c, n, piv, perm, info, ws, prof);
+  if (rc || *info != 0) return rc;
+  return lu_prepare_inverses<T>(c, S, lda, n);
 }
 
 template int lu_factor<double>(bem_ctx*, double*, int64_t, int, int*, int*, int, int*);
@@ -893,6 +997,242 @@ __global__ void permute_kernel(int n, const int* __restrict__ perm, const double
                                double* __restrict__ x) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) x[i] = v[perm[i]];
+}
+
+// ---- block-inverse sweeps ------------------------------------------------------------
+// The substitution of a 128 x 128 diagonal block is the sweeps' only sequential work.
+// With the blocks' inverses computed once per factorisation it becomes one 128 x 128
+// product, and the dependent chain per block is one publication, one tile product
+// (its loads issued before the wait) and one inverse product.
+
+constexpr int kInvPitch = kSolveBlock + 1;  // shared-memory pitch of the staged triangle
+
+// Dinv[2 blk] = inverse of the lower triangle (diagonal included) of the diagonal block
+// blk of S, Dinv[2 blk + 1] = inverse of its strict upper triangle plus the identity;
+// each 128 x 128, column-major, FP64, zero outside the block's order.  Both are the
+// inverse W of a unit upper triangle, blocked by 32 (the 32 x 32 diagonal blocks by
+// back substitution in registers, then W_ij = -W_ii sum_{k=i+1..j} U_ik W_kj by
+// distance from the diagonal): the upper one directly; for the lower one,
+// D = N diag(D) with N unit lower, so D^{-1} = diag(D)^{-1} N^{-1} and N^{-1} = W^T
+// for W = (N^T)^{-1}.  Grid (blocks, 2), blockIdx.y = 0 lower, 1 upper.
+template <typename T>
+__global__ void __launch_bounds__(256) diag_inv_kernel(const T* __restrict__ S, int64_t lda, int n,
+                                                       double* __restrict__ Dinv) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* U = reinterpret_cast<double*>(smem_raw);  // [128][kInvPitch], the strict upper part
+  __shared__ double dg[kSolveBlock];
+  __shared__ double tmp[32 * 33];
+  constexpr int B = 32, NB = kSolveBlock, P = kInvPitch;
+  const int blk = blockIdx.x;
+  const bool lower = blockIdx.y == 0;
+  const int k0 = blk * NB, jb = min(NB, n - k0);
+  const T* D = S + k0 + (int64_t)k0 * lda;
+  double* V = Dinv + ((size_t)blk * 2 + blockIdx.y) * (NB * NB);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid < NB) dg[tid] = (tid < jb) ? (double)D[tid + (int64_t)tid * lda] : 1.0;
+  __syncthreads();
+  // U(a, b), a < b: S(a, b) for the upper inverse, S(b, a) / S(a, a) for the lower one;
+  // the index runs along S's columns (contiguous) in both cases
+  for (int idx = tid; idx < NB * NB; idx += blockDim.x) {
+    const int i = idx % NB, j = idx / NB;  // S(k0 + i, k0 + j)
+    const double v = (i < jb && j < jb) ? (double)D[i + (int64_t)j * lda] : 0.0;
+    if (lower) {
+      if (j < i) U[j + i * P] = v / dg[j];
+      else U[j + i * P] = 0.0;
+    } else {
+      U[i + j * P] = (i < j) ? v : 0.0;
+    }
+  }
+  __syncthreads();
+  const int nb32 = (jb + B - 1) / B;
+  if (warp < nb32) {
+    const int o = warp * B;
+    double x[B];
+#pragma unroll
+    for (int i = 0; i < B; ++i) x[i] = (i == lane) ? 1.0 : 0.0;
+#pragma unroll
+    for (int i = B - 2; i >= 0; --i) {
+      double s = x[i];
+#pragma unroll
+      for (int k = i + 1; k < B; ++k) s = fma(-U[(o + i) + (o + k) * P], x[k], s);
+      x[i] = (i < lane) ? s : x[i];
+    }
+#pragma unroll
+    for (int i = 0; i < B; ++i)
+      if (o + i < jb && o + lane < jb) V[(o + i) + (o + lane) * NB] = x[i];
+  }
+  for (int idx = tid; idx < NB * NB; idx += blockDim.x) {
+    const int r = idx % NB, cc = idx / NB;
+    if (r >= jb || cc >= jb || r / B > cc / B) V[idx] = 0.0;
+  }
+  __syncthreads();
+  for (int d = 1; d < nb32; ++d)
+    for (int bi = 0; bi + d < nb32; ++bi) {
+      const int oi = bi * B, oj = (bi + d) * B;
+      for (int e = tid; e < B * B; e += blockDim.x) {
+        const int r = e % B, cc = e / B;
+        double acc = 0.0;
+        for (int k = oi + B; k < oj + B && k < jb; ++k) acc = fma(U[(oi + r) + k * P], V[k + (oj + cc) * NB], acc);
+        tmp[r + cc * 33] = acc;
+      }
+      __syncthreads();
+      for (int e = tid; e < B * B; e += blockDim.x) {
+        const int r = e % B, cc = e / B;
+        double acc = 0.0;
+#pragma unroll 8
+        for (int k = 0; k < B; ++k) acc = fma(V[(oi + r) + (oi + k) * NB], tmp[k + cc * 33], acc);
+        if (oi + r < jb && oj + cc < jb) V[(oi + r) + (oj + cc) * NB] = -acc;
+      }
+      __syncthreads();
+    }
+  if (lower) {
+    // V := diag(D)^{-1} W^T, pairwise in place
+    for (int idx = tid; idx < NB * NB; idx += blockDim.x) {
+      const int i = idx % NB, j = idx / NB;
+      if (i < j) {
+        const double wij = V[i + j * NB], wji = V[j + i * NB];
+        V[i + j * NB] = wji / dg[i];
+        V[j + i * NB] = wij / dg[j];
+      } else if (i == j) {
+        V[i + i * NB] = (i < jb) ? 1.0 / dg[i] : 0.0;
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void st_volatile_v2(unsigned long long* p, unsigned long long a, unsigned long long b) {
+  asm volatile("st.volatile.global.v2.u64 [%0], {%1, %2};" ::"l"(p), "l"(a), "l"(b) : "memory");
+}
+
+__device__ __forceinline__ void ld_volatile_v2(const unsigned long long* p, unsigned long long& a,
+                                               unsigned long long& b) {
+  asm volatile("ld.volatile.global.v2.u64 {%0, %1}, [%2];" : "=l"(a), "=l"(b) : "l"(p) : "memory");
+}
+
+// One sweep over the 128-row blocks with the diagonal blocks' inverses.  UPPER as in
+// sweep_kernel.  Step s solves block k(s) and is owned by CTA s % G, which keeps the
+// partial right-hand sides w of its blocks in shared memory (w = b - the tiles of the
+// blocks solved so far).  A solved block is published as 256 words {tag, 32 data bits}
+// (two per unknown) in slots[256 s ..]: a reader polls the words themselves, so one
+// L2 round trip both signals and delivers the block.  Every CTA loads its first tile of
+// step s before it waits for y_s; the owner of step s+1 handles that tile first and
+// then solves x = Dinv w from the inverse staged in shared memory one owned step ahead.
+// A wait that exceeds 2 s records BEM_ERR_TIMEOUT in *status and ends the CTA.
+template <typename T, bool UPPER>
+__global__ void __launch_bounds__(kSweepThreads, 1)
+    sweep_inv_kernel(const T* __restrict__ S, int64_t lda, int n, const double* __restrict__ Dinv, double* b,
+                     unsigned long long* slots, unsigned tag, int* status) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int NB = kSolveBlock;
+  constexpr bool kPrefetch = sizeof(T) == 4;  // double-buffered tile registers for FP32 factors
+  double* Di = reinterpret_cast<double*>(smem_raw);  // [NB * NB] inverse of the next owned block
+  double* wacc = Di + NB * NB;                        // [owned blocks][NB]
+  __shared__ double ys[NB];
+  __shared__ double red[4][NB];
+  __shared__ int s_abort;
+  const int t = threadIdx.x, G = gridDim.x, g = blockIdx.x;
+  const int nblk = (n + NB - 1) / NB;
+  const int rl = t & (NB - 1), q = t >> 7;
+  auto bidx = [&](int s) { return UPPER ? nblk - 1 - s : s; };
+  auto stage_inv = [&](int s) {
+    const double2* src = reinterpret_cast<const double2*>(Dinv + ((size_t)bidx(s) * 2 + (UPPER ? 1 : 0)) * (NB * NB));
+    double2* dst = reinterpret_cast<double2*>(Di);
+    for (int i0 = 0; i0 < NB * NB / 2; i0 += 8 * kSweepThreads) {
+      double2 v[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) v[u] = __ldcg(src + i0 + u * kSweepThreads + t);
+#pragma unroll
+      for (int u = 0; u < 8; ++u) dst[i0 + u * kSweepThreads + t] = v[u];
+    }
+  };
+  auto load_tile = [&](T* a, int sx, int c0, int cb) {
+    const int r0 = bidx(sx) * NB, rb = min(NB, n - r0);
+    const int cq = 32 * q;
+    const T* p = S + (r0 + rl) + (int64_t)(c0 + cq) * lda;
+#pragma unroll
+    for (int u = 0; u < 32; ++u) a[u] = (rl < rb && cq + u < cb) ? p[(int64_t)u * lda] : T(0);
+  };
+  const int nown = (g < nblk) ? (nblk - 1 - g) / G + 1 : 0;
+  for (int i = t; i < nown * NB; i += blockDim.x) {
+    const int k0 = bidx(g + (i / NB) * G) * NB, r = i % NB;
+    wacc[i] = (k0 + r < n) ? b[k0 + r] : 0.0;
+  }
+  if (t == 0) s_abort = 0;
+  if (nown > 0) stage_inv(g);
+  __syncthreads();
+
+  auto solve = [&](int s) {  // all threads; Di holds the inverse of block k(s)
+    const int k0 = bidx(s) * NB, kb = min(NB, n - k0);
+    const double* w = wacc + ((s - g) / G) * NB;
+    double acc = 0.0;
+#pragma unroll 8
+    for (int u = 0; u < 32; ++u) acc = fma(Di[rl + (32 * q + u) * NB], w[32 * q + u], acc);
+    red[q][rl] = acc;
+    __syncthreads();
+    if (t < kb) {
+      const double x = (red[0][t] + red[1][t]) + (red[2][t] + red[3][t]);
+      const unsigned long long hi = (unsigned long long)tag << 32;
+      const unsigned long long bits = (unsigned long long)__double_as_longlong(x);
+      st_volatile_v2(slots + (size_t)s * 256 + 2 * t, hi | (bits & 0xffffffffull), hi | (bits >> 32));
+      b[k0 + t] = x;
+    }
+    __syncthreads();  // Di and red are free again
+    if (s + G < nblk) stage_inv(s + G);
+  };
+
+  if (g == 0) solve(0);
+  for (int s = 0; s + 1 < nblk; ++s) {
+    const int s2 = s + 1 + ((g - (s + 1)) % G + G) % G;  // this CTA's first step after s
+    if (s2 >= nblk) break;                                // no rows left to update
+    const int c0 = bidx(s) * NB, cb = min(NB, n - c0);
+    T a[32];
+    load_tile(a, s2, c0, cb);
+    if (t < NB) {
+      double y = 0.0;
+      if (t < cb) {
+        const unsigned long long* p = slots + (size_t)s * 256 + 2 * t;
+        const unsigned long long t0 = globaltimer_ns();
+        unsigned it = 0;
+        unsigned long long w0, w1;
+        for (;;) {
+          ld_volatile_v2(p, w0, w1);
+          if ((unsigned)(w0 >> 32) == tag && (unsigned)(w1 >> 32) == tag) break;
+          if ((++it & 63u) == 0 &&
+              (globaltimer_ns() - t0 > 2000000000ull || *((volatile int*)status) != 0)) {
+            atomicCAS(status, 0, BEM_ERR_TIMEOUT);
+            s_abort = 1;
+            w0 = w1 = 0;
+            break;
+          }
+        }
+        y = __longlong_as_double((long long)((w1 << 32) | (w0 & 0xffffffffull)));
+      }
+      ys[t] = y;
+    }
+    __syncthreads();
+    if (s_abort) return;
+    for (int sx = s2; sx < nblk; sx += G) {
+      const bool more = sx + G < nblk;
+      T nx[32];
+      if (kPrefetch && more) load_tile(nx, sx + G, c0, cb);
+      double acc = 0.0;
+#pragma unroll
+      for (int u = 0; u < 32; ++u) acc = fma((double)a[u], ys[32 * q + u], acc);
+      red[q][rl] = acc;
+      __syncthreads();
+      if (t < NB) wacc[((sx - g) / G) * NB + t] -= (red[0][t] + red[1][t]) + (red[2][t] + red[3][t]);
+      __syncthreads();
+      if (sx == s + 1) solve(sx);
+      if (more) {
+        if (kPrefetch) {
+#pragma unroll
+          for (int u = 0; u < 32; ++u) a[u] = nx[u];
+        } else {
+          load_tile(a, sx + G, c0, cb);
+        }
+      }
+    }
+  }
 }
 
 // ---- the transposed solve: S^T x = b with the same factors --------------------------
@@ -1139,6 +1479,62 @@ int lu_solve_t_fp64(bem_ctx* c, const double* LU, int64_t lda, int n, double* b)
   return lu_solve_t_ws<double>(c, LU, lda, n, c->perm.p, b, c->work.p);
 }
 
+// Inverses of the diagonal blocks of freshly computed factors, kept in the context for
+// the block-inverse sweeps of lu_solve (2 x 128 KB per 128-row block).
+template <typename T>
+int lu_prepare_inverses(bem_ctx* c, const T* S, int64_t lda, int n) {
+  c->dinv_src = nullptr;
+  if (const char* e = getenv("BEM_SWEEP_INV"))  // 0: keep the substitution sweeps
+    if (atoi(e) == 0) return BEM_OK;
+  const int nblk = (n + kSolveBlock - 1) / kSolveBlock;
+  const size_t need = (size_t)nblk * 2 * kSolveBlock * kSolveBlock;
+  if (c->dinv.count < need) {
+    c->dinv.release();
+    BEM_CUDA(c, c->dinv.alloc(need));
+  }
+  const int smem = kSolveBlock * kInvPitch * (int)sizeof(double);
+  static bool attr[2] = {false, false};
+  if (!attr[sizeof(T) == 8]) {
+    BEM_CUDA(c, cudaFuncSetAttribute(diag_inv_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    attr[sizeof(T) == 8] = true;
+  }
+  diag_inv_kernel<T><<<dim3(nblk, 2), 256, smem, c->stream>>>(S, lda, n, c->dinv.p);
+  BEM_LAUNCH_CHECK(c);
+  c->dinv_src = S;
+  c->dinv_n = n;
+  c->dinv_lda = lda;
+  c->dinv_elem = (int)sizeof(T);
+  return BEM_OK;
+}
+
+template <typename T, bool UPPER>
+int sweep_inv_launch(bem_ctx* c, const T* S, int64_t lda, int n, double* b, unsigned long long* slots,
+                     unsigned tag, int* status) {
+  static int attr_bytes[2][2] = {{0, 0}, {0, 0}};
+  const int nblk = (n + kSolveBlock - 1) / kSolveBlock;
+  const int G = std::min(nblk, c->sm_count);
+  const int nown = (nblk + G - 1) / G;
+  const size_t dsm = ((size_t)kSolveBlock * kSolveBlock + (size_t)nown * kSolveBlock) * sizeof(double);
+  if (dsm > 227 * 1024) return bem_fail(c, BEM_ERR_ARG, "block-inverse sweep: too many blocks per SM");
+  int& set = attr_bytes[sizeof(T) == 8][UPPER ? 1 : 0];
+  if ((int)dsm > set) {
+    BEM_CUDA(c, cudaFuncSetAttribute(sweep_inv_kernel<T, UPPER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)dsm));
+    int per_sm = 0;
+    BEM_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_inv_kernel<T, UPPER>, kSweepThreads,
+                                                              dsm));
+    if (per_sm < 1) return bem_fail(c, BEM_ERR_CUDA, "block-inverse sweep kernel does not fit on an SM");
+    set = (int)dsm;
+  }
+  const double* dinv = c->dinv.p;
+  void* args[] = {(void*)&S, (void*)&lda, (void*)&n, (void*)&dinv, (void*)&b, (void*)&slots, (void*)&tag,
+                  (void*)&status};
+  BEM_CUDA(c, cudaLaunchCooperativeKernel((void*)sweep_inv_kernel<T, UPPER>, dim3(G), dim3(kSweepThreads), args,
+                                          dsm, c->stream));
+  ++c->launches;
+  return BEM_OK;
+}
+
 template <typename T>
 int lu_solve(bem_ctx* c, const T* S, int64_t lda, int n, const int* perm, double* b) {
   const size_t need = lu_solve_work_count(n);
@@ -1146,7 +1542,30 @@ int lu_solve(bem_ctx* c, const T* S, int64_t lda, int n, const int* perm, double
     c->work.release();
     BEM_CUDA(c, c->work.alloc(need));
   }
-  return lu_solve_ws<T>(c, S, lda, n, perm, b, c->work.p);
+  if (c->dinv_src != S || c->dinv_n != n || c->dinv_lda != lda || c->dinv_elem != (int)sizeof(T))
+    return lu_solve_ws<T>(c, S, lda, n, perm, b, c->work.p);
+  // block-inverse sweeps: slots [nblk][256] words, then the status word
+  const int nblk = (n + kSolveBlock - 1) / kSolveBlock;
+  const size_t words = (size_t)nblk * 256 + 2;
+  if (c->slots.count < words) {
+    c->slots.release();
+    BEM_CUDA(c, c->slots.alloc(words));
+  }
+  unsigned long long* slots = c->slots.p;
+  int* status = reinterpret_cast<int*>(slots + (size_t)nblk * 256);
+  BEM_CUDA(c, cudaMemsetAsync(slots, 0, words * sizeof(unsigned long long), c->stream));
+  int rc;
+  if ((rc = sweep_inv_launch<T, false>(c, S, lda, n, b, slots, 1u, status))) return rc;
+  if ((rc = sweep_inv_launch<T, true>(c, S, lda, n, b, slots, 2u, status))) return rc;
+  double* work = c->work.p;
+  permute_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(n, perm, b, work);
+  BEM_LAUNCH_CHECK(c);
+  BEM_CUDA(c, cudaMemcpyAsync(b, work, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  int st = 0;
+  BEM_CUDA(c, cudaMemcpyAsync(&st, status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  BEM_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (st != 0) return bem_fail(c, st, "triangular solve: a wait for a solved block timed out");
+  return BEM_OK;
 }
 
 template int lu_solve<double>(bem_ctx*, const double*, int64_t, int, const int*, double*);

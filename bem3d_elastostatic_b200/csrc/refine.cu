@@ -1,6 +1,7 @@
 // Mixed-precision solve (FP32 factors + FP64 iterative refinement against the FP64
 // A) and reorganize_solution (io_mod.f90:148-183).
 #include <cmath>
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <algorithm>
@@ -87,6 +88,14 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
   const int64_t lda = c->lda;
   *info = 0;
   if (c->factored_fp64) return bem_fail(c, BEM_ERR_STATE, "A was overwritten by an FP64 factorisation");
+  // BEM_IR_PROFILE: host time stamps of the solve's stages (stderr)
+  const bool host_prof = getenv("BEM_IR_PROFILE") != nullptr;
+  const auto h0 = std::chrono::steady_clock::now();
+  auto stamp = [&](const char* what) {
+    if (host_prof)
+      fprintf(stderr, "[solve host] %-14s %9.3f ms\n", what,
+              std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - h0).count());
+  };
   if (c->A32.count != (size_t)(lda * n)) {
     c->A32.release();
     cudaError_t e = c->A32.alloc((size_t)(lda * n));
@@ -94,9 +103,10 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
   }
   BEM_CUDA(c, c->piv.alloc(n));
   BEM_CUDA(c, c->perm.alloc(n));
-  DBuf<double> r, d;
-  BEM_CUDA(c, r.alloc(n));
-  BEM_CUDA(c, d.alloc(n));
+  DBuf<double>& r = c->ir_r;
+  DBuf<double>& d = c->ir_d;
+  if (r.count != (size_t)n) BEM_CUDA(c, r.alloc(n));
+  if (d.count != (size_t)n) BEM_CUDA(c, d.alloc(n));
   {
     // one workspace for the triangular solves and the residual, sized once
     const size_t nchunk = ((size_t)n + 511) / 512;
@@ -106,10 +116,9 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
       BEM_CUDA(c, c->work.alloc(need));
     }
   }
-  cudaEvent_t e0, e1, e2;
-  BEM_CUDA(c, cudaEventCreate(&e0));
-  BEM_CUDA(c, cudaEventCreate(&e1));
-  BEM_CUDA(c, cudaEventCreate(&e2));
+  for (auto& e : c->solve_ev)
+    if (!e) BEM_CUDA(c, cudaEventCreate(&e));
+  cudaEvent_t e0 = c->solve_ev[0], e1 = c->solve_ev[1], e2 = c->solve_ev[2];
   BEM_CUDA(c, cudaEventRecord(e0, c->stream));
   to_fp32_kernel<<<c->sm_count * 8, 256, 0, c->stream>>>(c->A.p, lda, n, c->A32.p);
   BEM_LAUNCH_CHECK(c);
@@ -123,9 +132,11 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
     const int v = atoi(e);
     if (v >= 128 && v <= 512 && v % 128 == 0) nb = v;
   }
+  stamp("enqueued");
   int rc = lu_factor<float>(c, c->A32.p, lda, n, c->piv.p, c->perm.p, nb, info);
   c->f32_gemm = saved;
   if (rc) return rc;
+  stamp("factored");
   BEM_CUDA(c, cudaEventRecord(e1, c->stream));
   if (*info != 0) return BEM_OK;
   // x0 = LU^{-1} b, then x += LU^{-1} (b - A x)   (plain refinement), or
@@ -276,14 +287,13 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
       BEM_CUDA(c, cudaStreamSynchronize(c->stream));
     }
   }
+  stamp("refined");
   BEM_CUDA(c, cudaEventRecord(e2, c->stream));
   BEM_CUDA(c, cudaEventSynchronize(e2));
+  stamp("synchronised");
   float f_ms = 0.f, r_ms = 0.f;
   cudaEventElapsedTime(&f_ms, e0, e1);
   cudaEventElapsedTime(&r_ms, e1, e2);
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  cudaEventDestroy(e2);
   if (st) {
     st->iterations = use_gmres ? it : std::min(it, max_iter);
     st->restarts = restarts;

@@ -370,6 +370,18 @@ bool make_map(CUtensorMap* map, const void* ptr, int rows, int K, int box_rows) 
 
 bool umma_supported(int K) { return K > 0 && K <= kMaxK && K % UK == 0; }
 
+// Grows the BF16 operand buffer to what an M x N x K update needs (before a captured
+// factorisation, whose first trailing update is its largest).
+int umma_reserve(bem_ctx* c, int M, int N, int K) {
+  const size_t need = 2 * ((size_t)M * K + (size_t)N * K) * sizeof(__nv_bfloat16) + 256;
+  if (c->umma_buf.count < need) {
+    c->umma_buf.release();
+    BEM_CUDA(c, c->umma_buf.alloc(need));
+  }
+  if (c->umma_err.count < 1) BEM_CUDA(c, c->umma_err.alloc(1));
+  return BEM_OK;
+}
+
 // C (M x N) -= A (M x K) * B (K x N) on tcgen05 with the three-term BF16 split.
 int gemm_umma_bf16x3(bem_ctx* c, int M, int N, int K, const float* A, int64_t lda, const float* B, int64_t ldb,
                      float* C, int64_t ldc) {

@@ -220,6 +220,11 @@ def run_gpu(args, ws, rank, local):
 
     for _ in range(args.warmup):
         step(args.precision)
+    # one more untimed step in the timed region's profile mode: the factorisation's
+    # launch sequence is captured per profile mode, so that capture happens here
+    q.ctx.profile_begin(timing=_lib.BEM_PROF_TRAILING)
+    step(args.precision)
+    q.ctx.profile_end()
     barrier(ws)
     torch.cuda.synchronize()
     q.ctx.sync()

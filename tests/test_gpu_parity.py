@@ -162,6 +162,29 @@ def test_dgesv_dropin_random():
         assert ipiv.min() >= 1 and ipiv.max() <= n
 
 
+def test_block_inverse_sweeps_match_substitution(monkeypatch):
+    """The solve with the diagonal blocks' FP64 inverses agrees with block substitution
+    at an order where CTAs own several 128-row blocks and the last block is ragged
+    (20,037 = 156 x 128 + 69)."""
+    from bem3d_elastostatic_b200.api import dgesv
+
+    rng = np.random.default_rng(11)
+    n = 20037
+    A = rng.standard_normal((n, n)) / np.sqrt(n)
+    A[np.diag_indices(n)] += 1.0
+    B = rng.standard_normal((n, 1))
+    _, ipiv_inv, X_inv, info = dgesv(A, B)
+    assert info == 0
+    monkeypatch.setenv("BEM_SWEEP_INV", "0")
+    _, ipiv_sub, X_sub, info = dgesv(A, B)
+    assert info == 0
+    assert np.array_equal(ipiv_inv, ipiv_sub)
+    scale = np.abs(X_sub).max()
+    assert np.abs(X_inv - X_sub).max() / scale < 1e-12
+    res = np.abs(A @ X_inv - B).max() / (np.abs(A).sum(1).max() * scale)
+    assert res < 1e-14, res
+
+
 def test_dgesv_singular_reports_info():
     from bem3d_elastostatic_b200.api import dgesv
 
