@@ -243,17 +243,22 @@ __global__ void trsm_small_kernel(T* S, int64_t lda, int k0, int w, int r_lo, in
   auto U = [&](int a, int b) { return Ucm[a + b * (kPanelW + 1)]; };
   const int r = r_lo + blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= r_hi) return;
+  // every load of the row before its first store (a store to S may alias later loads)
   T y[kPanelW];
+#pragma unroll
+  for (int b = 0; b < kPanelW; ++b) y[b] = (b < w) ? S[r + (int64_t)(k0 + b) * lda] : T(0);
 #pragma unroll
   for (int b = 0; b < kPanelW; ++b) {
     if (b < w) {
-      T v = S[r + (int64_t)(k0 + b) * lda];
+      T v = y[b];
 #pragma unroll
       for (int a = 0; a < b; ++a) v -= y[a] * U(a, b);
       y[b] = v;
-      S[r + (int64_t)(k0 + b) * lda] = v;
     }
   }
+#pragma unroll
+  for (int b = 0; b < kPanelW; ++b)
+    if (b < w) S[r + (int64_t)(k0 + b) * lda] = y[b];
 }
 
 // V = U^{-1} for the unit upper triangle U of S11 (jb x jb, jb <= 128); V column-major
@@ -318,6 +323,65 @@ __global__ void __launch_bounds__(256) inv_unit_upper_kernel(const T* S11, int64
       }
       __syncthreads();
     }
+}
+
+// The same inverse for FP32 factors with U and V both in shared memory (2 x 64 KB) and
+// the off-diagonal blocks of one distance from the diagonal computed together (two
+// barriers per distance); V is written to global memory once at the end.
+constexpr int kInvThreads = 512;
+__global__ void __launch_bounds__(kInvThreads) inv_unit_upper_f32_kernel(const float* S11, int64_t lda, int jb,
+                                                                         float* Vout, int ldv) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int B = 32, NB = 128, NBLK = NB / B;
+  float* U = reinterpret_cast<float*>(smem_raw);  // [NB][NB] column-major, the strict upper part
+  float* V = U + NB * NB;                         // [NB][NB] column-major
+  __shared__ float tmp[NBLK - 1][B * 33];
+  stage_block<float>(U, NB, S11, lda, jb, jb, NB, NB, [](int a, int b) { return a < b; });
+  for (int i = threadIdx.x; i < NB * NB; i += kInvThreads) V[i] = 0.f;
+  __syncthreads();
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nblk = (jb + B - 1) / B;
+  if (warp < nblk) {
+    const int o = warp * B;
+    float x[B];
+#pragma unroll
+    for (int i = 0; i < B; ++i) x[i] = (i == lane) ? 1.f : 0.f;
+#pragma unroll
+    for (int i = B - 2; i >= 0; --i) {
+      float sacc = x[i];
+#pragma unroll
+      for (int k = i + 1; k < B; ++k) sacc -= U[(o + i) + (o + k) * NB] * x[k];
+      x[i] = (i < lane) ? sacc : x[i];
+    }
+#pragma unroll
+    for (int i = 0; i < B; ++i)
+      if (o + i < jb && o + lane < jb) V[(o + i) + (o + lane) * NB] = x[i];
+  }
+  __syncthreads();
+  for (int d = 1; d < nblk; ++d) {
+    const int nb_d = nblk - d;  // blocks (bi, bi + d)
+    for (int e = tid; e < nb_d * B * B; e += kInvThreads) {
+      const int bi = e / (B * B), r = e % B, cc = (e / B) % B;
+      const int oi = bi * B, oj = (bi + d) * B;
+      float acc = 0.f;
+      for (int k = oi + B; k <= oj + B - 1 && k < jb; ++k) acc += U[(oi + r) + k * NB] * V[k + (oj + cc) * NB];
+      tmp[bi][r + cc * 33] = acc;
+    }
+    __syncthreads();
+    for (int e = tid; e < nb_d * B * B; e += kInvThreads) {
+      const int bi = e / (B * B), r = e % B, cc = (e / B) % B;
+      const int oi = bi * B, oj = (bi + d) * B;
+      float acc = 0.f;
+#pragma unroll 8
+      for (int k = 0; k < B; ++k) acc += V[(oi + r) + (oi + k) * NB] * tmp[bi][k + cc * 33];
+      if (oi + r < jb && oj + cc < jb) V[(oi + r) + (oj + cc) * NB] = -acc;
+    }
+    __syncthreads();
+  }
+  for (int i = tid; i < jb * jb; i += kInvThreads) {
+    const int r = i % jb, cc = i / jb;
+    Vout[r + (int64_t)cc * ldv] = V[r + cc * NB];
+  }
 }
 
 // ---------------------------------------------------------------------------------
@@ -636,6 +700,8 @@ static int lu_factor_enqueue(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int
   const int64_t ldy = ws.ldy;
   const size_t inv_smem = (size_t)kInvBlock * kInvBlock * sizeof(T);
   cudaFuncSetAttribute(inv_unit_upper_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inv_smem);
+  cudaFuncSetAttribute(inv_unit_upper_f32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)(2 * kInvBlock * kInvBlock * sizeof(float)));
   int rc;
   for (int j0 = 0; j0 < n; j0 += nb) {
     const int jb = std::min(nb, n - j0);
@@ -680,8 +746,13 @@ static int lu_factor_enqueue(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int
         if (b0 > 0 &&
             (rc = gemm<T>(c, m, bb, b0, Y, ldy, S + j0 + (int64_t)(j0 + b0) * lda, lda, Xb, lda, 0)))
           return rc;
-        inv_unit_upper_kernel<T><<<1, 256, inv_smem, c->stream>>>(
-            S + (j0 + b0) + (int64_t)(j0 + b0) * lda, lda, bb, V, kInvBlock);
+        if (sizeof(T) == 4)
+          inv_unit_upper_f32_kernel<<<1, kInvThreads, 2 * kInvBlock * kInvBlock * sizeof(float), c->stream>>>(
+              reinterpret_cast<const float*>(S + (j0 + b0) + (int64_t)(j0 + b0) * lda), lda, bb,
+              reinterpret_cast<float*>(V), kInvBlock);
+        else
+          inv_unit_upper_kernel<T><<<1, 256, inv_smem, c->stream>>>(
+              S + (j0 + b0) + (int64_t)(j0 + b0) * lda, lda, bb, V, kInvBlock);
         BEM_LAUNCH_CHECK(c);
         if ((rc = gemm<T>(c, m, bb, bb, Xb, lda, V, kInvBlock, Y + (int64_t)b0 * ldy, ldy, 1))) return rc;
       }
