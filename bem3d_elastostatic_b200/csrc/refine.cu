@@ -11,7 +11,10 @@
 
 namespace bem {
 
-constexpr int kNbMixed = 256;  // panel width of the FP32 factorisation (halves the trailing C traffic)
+// panel width of the FP32 factorisation: at 512 the tcgen05 trailing update has as much
+// tensor work per tile as C traffic (measured at 73,734 DOF: 1.79 s per bench step at 256,
+// 1.61 s at 384, 1.58 s at 512)
+constexpr int kNbMixed = 512;
 
 __global__ void to_fp32_kernel(const double* A, int64_t lda, int n, float* A32) {
   const int64_t total = (int64_t)lda * n;
