@@ -40,13 +40,13 @@ __device__ __forceinline__ int sym_idx(int a, int b) {
 
 // fi_acc (3) and d1_acc (9) are this lane's running sums over its elements, kept in
 // shared memory so the 9 x NC accumulators below have the register file to themselves.
+// T: the element's packed quadrature table, staged in shared memory by the caller.
 template <int NC, int MODE, typename R>
-__device__ __forceinline__ void regular_pair(const AsmArgs& P, int e, const int* kc, double xi0,
+__device__ __forceinline__ void regular_pair(const AsmArgs& P, int e, const double* T, const int* kc, double xi0,
                                              double xi1, double xi2, int64_t row,
                                              double* fi_acc, double* d1) {
   double fi[3] = {0.0, 0.0, 0.0};
   constexpr int NG = (NC == 9) ? 36 : 16;
-  const double* T = P.tab + (int64_t)e * kTabStride;
   const double c3 = P.mat.c3, c4 = P.mat.c4, c5 = P.mat.c5, c6 = P.mat.c6;
 
   // ---- G: U* (symmetric, 6 values) x p12 -------------------------------------------
@@ -60,9 +60,9 @@ __device__ __forceinline__ void regular_pair(const AsmArgs& P, int e, const int*
 #pragma unroll 2
     for (int q = 0; q < NG; ++q) {
       // the coordinate difference is always formed in FP64 (no cancellation in R)
-      const R r0 = (R)(__ldg(T + 6 * q + 0) - xi0);
-      const R r1 = (R)(__ldg(T + 6 * q + 1) - xi1);
-      const R r2 = (R)(__ldg(T + 6 * q + 2) - xi2);
+      const R r0 = (R)(T[6 * q + 0] - xi0);
+      const R r1 = (R)(T[6 * q + 1] - xi1);
+      const R r2 = (R)(T[6 * q + 2] - xi2);
       const R ri = rsqrt(r0 * r0 + r1 * r1 + r2 * r2);
       const R a0 = r0 * ri, a1 = r1 * ri, a2 = r2 * ri;
       const R c3r = rc3 * ri;
@@ -76,7 +76,7 @@ __device__ __forceinline__ void regular_pair(const AsmArgs& P, int e, const int*
       const double* W = T + kTabGeo + 9 * q;
 #pragma unroll
       for (int k = 0; k < NC; ++k) {
-        const R w = (R)__ldg(W + k);
+        const R w = (R)W[k];
 #pragma unroll
         for (int p = 0; p < 6; ++p) g[k][p] = fma(u[p], w, g[k][p]);
       }
@@ -138,10 +138,10 @@ __device__ __forceinline__ void regular_pair(const AsmArgs& P, int e, const int*
     const R rc5 = (R)c5, rc6 = (R)c6;
 #pragma unroll 1
     for (int q = 0; q < NG; ++q) {
-      const R r0 = (R)(__ldg(T + 6 * q + 0) - xi0);
-      const R r1 = (R)(__ldg(T + 6 * q + 1) - xi1);
-      const R r2 = (R)(__ldg(T + 6 * q + 2) - xi2);
-      const R n[3] = {(R)__ldg(T + 6 * q + 3), (R)__ldg(T + 6 * q + 4), (R)__ldg(T + 6 * q + 5)};
+      const R r0 = (R)(T[6 * q + 0] - xi0);
+      const R r1 = (R)(T[6 * q + 1] - xi1);
+      const R r2 = (R)(T[6 * q + 2] - xi2);
+      const R n[3] = {(R)T[6 * q + 3], (R)T[6 * q + 4], (R)T[6 * q + 5]};
       const R ri = rsqrt(r0 * r0 + r1 * r1 + r2 * r2);
       const R a[3] = {r0 * ri, r1 * ri, r2 * ri};
       const R rdn = a[0] * n[0] + a[1] * n[1] + a[2] * n[2];
@@ -158,7 +158,7 @@ __device__ __forceinline__ void regular_pair(const AsmArgs& P, int e, const int*
       const double* W = T + kTabGeo + 9 * q;
 #pragma unroll
       for (int k = 0; k < NC; ++k) {
-        const R w = (R)__ldg(W + k);
+        const R w = (R)W[k];
 #pragma unroll
         for (int p = 0; p < 9; ++p) h[k][p] = fma(t[p], w, h[k][p]);
       }
@@ -245,11 +245,35 @@ __device__ __forceinline__ void regular_pair(const AsmArgs& P, int e, const int*
 // PREC 0: every regular pair in FP64.  PREC 1: pairs farther than 3.5 element radii
 // from the element centroid (the near-field radius of stress_mod.f90:603-604) evaluate
 // and accumulate the Kelvin kernels in FP32; nearer pairs stay in FP64.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(smem)),
+               "l"(gmem)
+               : "memory");
+}
+
+// Dynamic shared memory of the regular tile: two buffers of one quadrature table per
+// warp (the batch being integrated and the next one, copied in meanwhile).
+constexpr int kTabSmem = 2 * kBatch * kTabStride * (int)sizeof(double);
+
 template <int MODE, int PREC>
 __device__ __forceinline__ void regular_tile(const AsmArgs& P, int tile) {
   __shared__ double s_red[kBatch][32][12];
+  extern __shared__ __align__(16) double s_tab[];  // [2][kBatch][kTabStride]
   const int w = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
+  // each warp copies its own next element's table (16-byte cp.async, 270 per table)
+  // while it integrates the current one: the table loads leave the dependent chain
+  auto prefetch = [&](int b) {
+    if (b < P.nbatches) {
+      const int e = __ldg(P.batches + kBatch * b + w);
+      if (e >= 0) {
+        const char* src = reinterpret_cast<const char*>(P.tab + (int64_t)e * kTabStride);
+        char* dst = reinterpret_cast<char*>(s_tab + ((b & 1) * kBatch + w) * kTabStride);
+        for (int i = lane; i < kTabStride * 8 / 16; i += 32) cp_async16(dst + 16 * i, src + 16 * i);
+      }
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
   const int local = tile * 32 + lane;  // node offset inside the row range
   const bool active = local < P.nrows_nodes;
   const int in = P.in0 + (active ? local : 0);
@@ -260,8 +284,13 @@ __device__ __forceinline__ void regular_tile(const AsmArgs& P, int tile) {
 #pragma unroll
   for (int p = 0; p < 12; ++p) s_red[w][lane][p] = 0.0;
 
+  prefetch(0);
   for (int b = 0; b < P.nbatches; ++b) {
     const int e = __ldg(P.batches + kBatch * b + w);
+    prefetch(b + 1);
+    asm volatile("cp.async.wait_group 1;" ::: "memory");  // this batch's table is in
+    __syncwarp();
+    const double* T = s_tab + ((b & 1) * kBatch + w) * kTabStride;
     if (e >= 0) {
       const int ncone = __ldg(P.nconec + e);
       int kc[9];
@@ -293,19 +322,20 @@ __device__ __forceinline__ void regular_tile(const AsmArgs& P, int tile) {
       if (active && !sing) {
         if (ncone == 9) {
           if (far32)
-            regular_pair<9, MODE, float>(P, e, kc, xi0, xi1, xi2, row, fi, d1);
+            regular_pair<9, MODE, float>(P, e, T, kc, xi0, xi1, xi2, row, fi, d1);
           else
-            regular_pair<9, MODE, double>(P, e, kc, xi0, xi1, xi2, row, fi, d1);
+            regular_pair<9, MODE, double>(P, e, T, kc, xi0, xi1, xi2, row, fi, d1);
         } else {
           if (far32)
-            regular_pair<6, MODE, float>(P, e, kc, xi0, xi1, xi2, row, fi, d1);
+            regular_pair<6, MODE, float>(P, e, T, kc, xi0, xi1, xi2, row, fi, d1);
           else
-            regular_pair<6, MODE, double>(P, e, kc, xi0, xi1, xi2, row, fi, d1);
+            regular_pair<6, MODE, double>(P, e, T, kc, xi0, xi1, xi2, row, fi, d1);
         }
       }
     }
     __syncthreads();
   }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
 
   __syncthreads();
   if (w == 0 && active) {
@@ -647,10 +677,18 @@ int launch_ghmat8(bem_ctx* c, int precision) {
   P.lda = lda;
   P.FI = c->FI.p;
   const int tiles = (c->n + 31) / 32;
+  static bool attr = false;  // the tables' double buffer is above the 48 KB default
+  if (!attr) {
+    BEM_CUDA(c, cudaFuncSetAttribute(ghmat_regular_kernel<kModeA, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     kTabSmem));
+    BEM_CUDA(c, cudaFuncSetAttribute(ghmat_regular_kernel<kModeA, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     kTabSmem));
+    attr = true;
+  }
   if (precision == BEM_ASM_FP32_FAR)
-    ghmat_regular_kernel<kModeA, 1><<<tiles, 256, 0, c->stream>>>(P);
+    ghmat_regular_kernel<kModeA, 1><<<tiles, 256, kTabSmem, c->stream>>>(P);
   else
-    ghmat_regular_kernel<kModeA, 0><<<tiles, 256, 0, c->stream>>>(P);
+    ghmat_regular_kernel<kModeA, 0><<<tiles, 256, kTabSmem, c->stream>>>(P);
   BEM_LAUNCH_CHECK(c);
   ghmat_singular_kernel<kModeA><<<(c->n + 3) / 4, 128, 0, c->stream>>>(P);
   BEM_LAUNCH_CHECK(c);
@@ -678,7 +716,13 @@ int launch_hg(bem_ctx* c, int in0, int in1, double* dH, int64_t ldh, double* dG,
   P.G = dG;
   P.ldg = ldg;
   const int tiles = (P.nrows_nodes + 31) / 32;
-  ghmat_regular_kernel<kModeHG, 0><<<tiles, 256, 0, c->stream>>>(P);
+  static bool attr = false;
+  if (!attr) {
+    BEM_CUDA(c, cudaFuncSetAttribute(ghmat_regular_kernel<kModeHG, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     kTabSmem));
+    attr = true;
+  }
+  ghmat_regular_kernel<kModeHG, 0><<<tiles, 256, kTabSmem, c->stream>>>(P);
   BEM_LAUNCH_CHECK(c);
   ghmat_singular_kernel<kModeHG><<<(P.nrows_nodes + 3) / 4, 128, 0, c->stream>>>(P);
   BEM_LAUNCH_CHECK(c);
@@ -743,8 +787,15 @@ int launch_batch_hg(cudaStream_t stream, int sm_count, const AsmArgs* d_args, co
     constants = true;
   }
   if (cudaMemsetAsync(counter, 0, sizeof(unsigned), stream) != cudaSuccess) return BEM_ERR_CUDA;
-  batch_regular_kernel<<<std::max(1, std::min(ntiles, sm_count)), 256, 0, stream>>>(d_args, d_tiles, ntiles,
-                                                                                     counter);
+  static bool attr = false;  // the tables' double buffer is above the 48 KB default
+  if (!attr) {
+    if (cudaFuncSetAttribute(batch_regular_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTabSmem) !=
+        cudaSuccess)
+      return BEM_ERR_CUDA;
+    attr = true;
+  }
+  batch_regular_kernel<<<std::max(1, std::min(ntiles, sm_count)), 256, kTabSmem, stream>>>(d_args, d_tiles,
+                                                                                            ntiles, counter);
   if (cudaGetLastError() != cudaSuccess) return BEM_ERR_CUDA;
   batch_singular_kernel<<<(total_nodes + 3) / 4, 128, 0, stream>>>(d_args, d_node_off, nsys, total_nodes);
   if (cudaGetLastError() != cudaSuccess) return BEM_ERR_CUDA;

@@ -185,6 +185,32 @@ def test_block_inverse_sweeps_match_substitution(monkeypatch):
     assert res < 1e-14, res
 
 
+def test_factorisation_graph_replay_is_bitwise_plain(cube8_mesh, monkeypatch):
+    """The factorisation's launch sequence is captured as a CUDA graph on first use and
+    replayed afterwards; every stage is deterministic, so the first (captured) solve, a
+    replayed solve and a context with plain launches give bitwise the same solutions,
+    for the FP32 refinement and for the FP64 LU."""
+    from bem3d_elastostatic_b200.api import Quadesth
+
+    def solves(q):
+        q.precompute_element_geometry()
+        q.ghmat8()
+        a = q.solve_linear_system("fp32-ir", tol=1e-15, max_iter=60)
+        b = q.solve_linear_system("fp32-ir", tol=1e-15, max_iter=60)
+        q.ghmat8()
+        c = q.solve_linear_system("fp64")
+        q.ghmat8()
+        d = q.solve_linear_system("fp64")
+        q.close()
+        return a, b, c, d
+
+    g32a, g32b, g64a, g64b = solves(Quadesth(cube8_mesh))
+    monkeypatch.setenv("BEM_LU_GRAPH", "0")
+    p32, _, p64, _ = solves(Quadesth(cube8_mesh))
+    assert np.array_equal(g32a, g32b) and np.array_equal(g32a, p32)
+    assert np.array_equal(g64a, g64b) and np.array_equal(g64a, p64)
+
+
 def test_dgesv_singular_reports_info():
     from bem3d_elastostatic_b200.api import dgesv
 
