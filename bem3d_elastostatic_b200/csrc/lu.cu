@@ -84,16 +84,24 @@ __device__ __forceinline__ void stage_block(T* dst, int ldd, const T* src, int64
   }
 }
 
+// threads of a panel CTA: one slice row per thread for FP32 factors (measured: the
+// local candidate scan and update per pivot shrink with the rows per thread); FP64
+// keeps 256 (its 176 registers per thread would spill at 512)
 template <typename T>
-__global__ void __launch_bounds__(256, 1)
+constexpr int panel_threads() {
+  return sizeof(T) == 4 ? 512 : 256;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(panel_threads<T>(), 1)
     panel_kernel(T* S, int64_t lda, int n, int r0, int w, int chunk, int* piv, double* cand_val,
                  int* cand_idx, T* cand_col, T* diag_col, unsigned* barrier, unsigned bar_base, int* status) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* col = reinterpret_cast<T*>(smem_raw);  // [chunk][kPitch]
   __shared__ T s_pv[kPanelW];  // the winning candidate column
   __shared__ T s_dc[kPanelW];  // the diagonal column of the pivot step
-  __shared__ double red_v[8];
-  __shared__ int red_c[8];
+  __shared__ double red_v[panel_threads<T>() / 32];
+  __shared__ int red_c[panel_threads<T>() / 32];
   __shared__ int s_local_c, s_abort, s_win[2];
   const int G = gridDim.x, g = blockIdx.x, tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
   const int c_beg = r0 + g * chunk;
@@ -529,7 +537,11 @@ int panel_launch(bem_ctx* c, const LUWorkspace& ws, T* S, int64_t lda, int n, in
                  unsigned& bar_base) {
   static int checked = 0;  // bit 0: double, bit 1: float
   const int cols = n - r0;
-  int G = std::min(std::min(c->sm_count, ws.gmax), std::max(1, (cols + 63) / 64));
+  static const int cap = [] {  // BEM_PANEL_CTAS: at most this many CTAs per panel launch
+    const char* e = getenv("BEM_PANEL_CTAS");
+    return e ? std::max(1, atoi(e)) : INT_MAX;
+  }();
+  int G = std::min(std::min(std::min(c->sm_count, ws.gmax), cap), std::max(1, (cols + 63) / 64));
   int chunk = (cols + G - 1) / G;
   size_t smem = (size_t)chunk * kPitch * sizeof(T);
   if (smem > kPanelSmemMax) return bem_fail(c, BEM_ERR_ARG, "panel slice exceeds shared memory (matrix too large)");
@@ -538,7 +550,7 @@ int panel_launch(bem_ctx* c, const LUWorkspace& ws, T* S, int64_t lda, int n, in
     // one CTA per SM at the largest slice guarantees co-residency of every launch
     BEM_CUDA(c, cudaFuncSetAttribute(panel_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, kPanelSmemMax));
     int occ = 0;
-    BEM_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, panel_kernel<T>, 256, kPanelSmemMax));
+    BEM_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, panel_kernel<T>, panel_threads<T>(), kPanelSmemMax));
     if (occ < 1) return bem_fail(c, BEM_ERR_CUDA, "panel kernel cannot be resident");
     checked |= bit;
   }
@@ -550,7 +562,8 @@ int panel_launch(bem_ctx* c, const LUWorkspace& ws, T* S, int64_t lda, int n, in
   int* st = ws.status;
   unsigned bb = bar_base;
   void* args[] = {&S, &lda, &n, &r0, &w, &chunk, &piv, &cv, &ci, &cc, &dc, &bar, &bb, &st};
-  BEM_CUDA(c, cudaLaunchCooperativeKernel((void*)panel_kernel<T>, dim3(G), dim3(256), args, smem, c->stream));
+  BEM_CUDA(c, cudaLaunchCooperativeKernel((void*)panel_kernel<T>, dim3(G), dim3(panel_threads<T>()), args, smem,
+                                          c->stream));
   ++c->launches;
   bar_base += (unsigned)w * (unsigned)G;
   return BEM_OK;
