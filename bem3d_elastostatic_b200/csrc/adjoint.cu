@@ -329,8 +329,8 @@ __global__ void zero_pins_kernel(const int* pins, int npins, double* lam) {
 }
 
 int upload_tables() {
-  static bool done = false;
-  if (done) return BEM_OK;
+  static DeviceOnce done;  // per device: __constant__ tables
+  if (!done.pending()) return BEM_OK;
   double f[36][9], d1[36][9], d2[36][9], w[36];
   for (int i = 0; i < 6; ++i)
     for (int j = 0; j < 6; ++j) {
@@ -343,7 +343,7 @@ int upload_tables() {
       cudaMemcpyToSymbol(c_gi6, kGiQuad, sizeof(kGiQuad)) != cudaSuccess ||
       cudaMemcpyToSymbol(c_om6, kOmeQuad, sizeof(kOmeQuad)) != cudaSuccess)
     return BEM_ERR_CUDA;
-  done = true;
+  done.mark();
   return BEM_OK;
 }
 

@@ -677,13 +677,13 @@ int launch_ghmat8(bem_ctx* c, int precision) {
   P.lda = lda;
   P.FI = c->FI.p;
   const int tiles = (c->n + 31) / 32;
-  static bool attr = false;  // the tables' double buffer is above the 48 KB default
-  if (!attr) {
+  static DeviceOnce attr;  // the tables' double buffer is above the 48 KB default
+  if (attr.pending()) {
     BEM_CUDA(c, cudaFuncSetAttribute(ghmat_regular_kernel<kModeA, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      kTabSmem));
     BEM_CUDA(c, cudaFuncSetAttribute(ghmat_regular_kernel<kModeA, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      kTabSmem));
-    attr = true;
+    attr.mark();
   }
   if (precision == BEM_ASM_FP32_FAR)
     ghmat_regular_kernel<kModeA, 1><<<tiles, 256, kTabSmem, c->stream>>>(P);
@@ -716,11 +716,11 @@ int launch_hg(bem_ctx* c, int in0, int in1, double* dH, int64_t ldh, double* dG,
   P.G = dG;
   P.ldg = ldg;
   const int tiles = (P.nrows_nodes + 31) / 32;
-  static bool attr = false;
-  if (!attr) {
+  static DeviceOnce attr;
+  if (attr.pending()) {
     BEM_CUDA(c, cudaFuncSetAttribute(ghmat_regular_kernel<kModeHG, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      kTabSmem));
-    attr = true;
+    attr.mark();
   }
   ghmat_regular_kernel<kModeHG, 0><<<tiles, 256, kTabSmem, c->stream>>>(P);
   BEM_LAUNCH_CHECK(c);
@@ -779,20 +779,20 @@ __global__ void __launch_bounds__(128)
 
 int launch_batch_hg(cudaStream_t stream, int sm_count, const AsmArgs* d_args, const int2* d_tiles, int ntiles,
                     unsigned* counter, const int* d_node_off, int nsys, int total_nodes, long long* launches) {
-  static bool constants = false;
-  if (!constants) {
+  static DeviceOnce constants;
+  if (constants.pending()) {
     if (cudaMemcpyToSymbol(s_gi, kGiQuad, sizeof(kGiQuad)) != cudaSuccess ||
         cudaMemcpyToSymbol(s_ome, kOmeQuad, sizeof(kOmeQuad)) != cudaSuccess)
       return BEM_ERR_CUDA;
-    constants = true;
+    constants.mark();
   }
   if (cudaMemsetAsync(counter, 0, sizeof(unsigned), stream) != cudaSuccess) return BEM_ERR_CUDA;
-  static bool attr = false;  // the tables' double buffer is above the 48 KB default
-  if (!attr) {
+  static DeviceOnce attr;  // the tables' double buffer is above the 48 KB default
+  if (attr.pending()) {
     if (cudaFuncSetAttribute(batch_regular_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kTabSmem) !=
         cudaSuccess)
       return BEM_ERR_CUDA;
-    attr = true;
+    attr.mark();
   }
   batch_regular_kernel<<<std::max(1, std::min(ntiles, sm_count)), 256, kTabSmem, stream>>>(d_args, d_tiles,
                                                                                             ntiles, counter);

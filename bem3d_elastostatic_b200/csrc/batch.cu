@@ -957,12 +957,12 @@ namespace {
 
 template <typename T, int NT>
 int launch_lu(bem_batch* b, T* F) {
-  static bool attr = false;
-  if (!attr) {
+  static bem::DeviceOnce attr;
+  if (attr.pending()) {
     if (cudaFuncSetAttribute(bem::batch_lu_kernel<T, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)bem::lu_smem<T>()) != cudaSuccess)
       return BEM_ERR_CUDA;
-    attr = true;
+    attr.mark();
   }
   bem::batch_lu_kernel<T, NT><<<std::min((int)b->sys.size(), b->sm_count), NT, bem::lu_smem<T>(), b->stream>>>(
       b->dsys.p, b->ord.p, (int)b->sys.size(), F, b->piv.p, b->info.p, b->counters.p + 0);
@@ -1004,14 +1004,14 @@ int enqueue_solve(bem_batch* b, int precision, double tol, int sweeps, T* F) {
 
 template <typename T>
 int set_smem() {
-  static bool done = false;
-  if (done) return BEM_OK;
+  static bem::DeviceOnce done;
+  if (!done.pending()) return BEM_OK;
   if (cudaFuncSetAttribute(bem::batch_solve_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)bem::kSolveSmem) != cudaSuccess ||
       cudaFuncSetAttribute(bem::batch_residual_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)bem::kSolveSmem) != cudaSuccess)
     return BEM_ERR_CUDA;
-  done = true;
+  done.mark();
   return BEM_OK;
 }
 

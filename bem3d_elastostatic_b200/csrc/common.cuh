@@ -81,6 +81,20 @@ struct DBuf {
   size_t bytes() const { return count * sizeof(T); }
 };
 
+// One-time set-up that CUDA keeps per device (kernel attributes, __constant__ tables),
+// tracked per device so that a process driving several GPUs sets up each of them:
+// `static DeviceOnce s; if (s.pending()) { ...; s.mark(); }` with the device current.
+inline int current_device() {
+  int d = 0;
+  cudaGetDevice(&d);
+  return d & 63;
+}
+struct DeviceOnce {
+  unsigned long long bits = 0;
+  bool pending() const { return ((bits >> current_device()) & 1ull) == 0; }
+  void mark() { bits |= 1ull << current_device(); }
+};
+
 // A factorisation's launch sequence captured as a CUDA graph and replayed while every
 // pointer and size it was captured with (the key) is unchanged, so that the ~10^4
 // launches of a large factorisation neither wait on the host nor pay per-launch costs.

@@ -324,11 +324,11 @@ static bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
 
 int gemm_dmma(bem_ctx* c, int M, int N, int K, const double* A, int64_t lda, const double* B, int64_t ldb, double* C,
               int64_t ldc, int mode) {
-  static bool attr = false;
-  if (!attr) {
+  static DeviceOnce attr;
+  if (attr.pending()) {
     cudaFuncSetAttribute(dgemm_dmma_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDmmaSmem);
     cudaFuncSetAttribute(dgemm_dmma_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDmmaSmem);
-    attr = true;
+    attr.mark();
   }
   dim3 grid((N + DBN - 1) / DBN, (M + DBM - 1) / DBM);
   if (mode == 0)
@@ -341,15 +341,15 @@ int gemm_dmma(bem_ctx* c, int M, int N, int K, const double* A, int64_t lda, con
 
 int gemm_bf16(bem_ctx* c, int M, int N, int K, const float* A, int64_t lda, const float* B, int64_t ldb, float* C,
               int64_t ldc, int mode, int split) {
-  static bool attr = false;
+  static DeviceOnce attr;
   const size_t smem1 = (size_t)(HBK * HPA + HBN * HPB) * sizeof(__nv_bfloat16);
   const size_t smem3 = 2 * smem1;
-  if (!attr) {
+  if (attr.pending()) {
     cudaFuncSetAttribute(sgemm_bf16_kernel<0, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1);
     cudaFuncSetAttribute(sgemm_bf16_kernel<1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem1);
     cudaFuncSetAttribute(sgemm_bf16_kernel<0, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem3);
     cudaFuncSetAttribute(sgemm_bf16_kernel<1, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem3);
-    attr = true;
+    attr.mark();
   }
   dim3 grid((N + HBN - 1) / HBN, (M + HBM_ - 1) / HBM_);
   if (split == 3) {

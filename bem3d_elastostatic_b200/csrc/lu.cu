@@ -535,7 +535,7 @@ namespace {
 template <typename T>
 int panel_launch(bem_ctx* c, const LUWorkspace& ws, T* S, int64_t lda, int n, int r0, int w, int* piv,
                  unsigned& bar_base) {
-  static int checked = 0;  // bit 0: double, bit 1: float
+  static DeviceOnce checked;  // per instantiation (T) and device
   const int cols = n - r0;
   static const int cap = [] {  // BEM_PANEL_CTAS: at most this many CTAs per panel launch
     const char* e = getenv("BEM_PANEL_CTAS");
@@ -545,14 +545,13 @@ int panel_launch(bem_ctx* c, const LUWorkspace& ws, T* S, int64_t lda, int n, in
   int chunk = (cols + G - 1) / G;
   size_t smem = (size_t)chunk * kPitch * sizeof(T);
   if (smem > kPanelSmemMax) return bem_fail(c, BEM_ERR_ARG, "panel slice exceeds shared memory (matrix too large)");
-  const int bit = sizeof(T) == 8 ? 1 : 2;
-  if (!(checked & bit)) {
+  if (checked.pending()) {
     // one CTA per SM at the largest slice guarantees co-residency of every launch
     BEM_CUDA(c, cudaFuncSetAttribute(panel_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, kPanelSmemMax));
     int occ = 0;
     BEM_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, panel_kernel<T>, panel_threads<T>(), kPanelSmemMax));
     if (occ < 1) return bem_fail(c, BEM_ERR_CUDA, "panel kernel cannot be resident");
-    checked |= bit;
+    checked.mark();
   }
   double* cv = ws.cand_val;
   int* ci = ws.cand_idx;
@@ -1477,13 +1476,14 @@ __global__ void scatter_kernel(int n, const int* __restrict__ perm, const double
 template <typename T, bool UPPER>
 int sweep_t_launch(bem_ctx* c, const T* S, int64_t lda, int n, double* b, unsigned* flags, unsigned tag,
                    int* status) {
-  static int ok[2][2] = {{0, 0}, {0, 0}};
+  static DeviceOnce ok;  // per instantiation and device
   const size_t dsm = (size_t)kSolveBlock * kLdT * sizeof(T);
-  int& per_sm = ok[sizeof(T) == 8][UPPER ? 1 : 0];
-  if (per_sm == 0) {
+  if (ok.pending()) {
+    int per_sm = 0;
     BEM_CUDA(c, cudaFuncSetAttribute(sweep_t_kernel<T, UPPER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm));
     BEM_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_t_kernel<T, UPPER>, kSweepThreads, dsm));
     if (per_sm < 1) return bem_fail(c, BEM_ERR_CUDA, "transposed sweep kernel does not fit on an SM");
+    ok.mark();
   }
   const int nblk = (n + kSolveBlock - 1) / kSolveBlock;
   const int G = std::min(nblk, c->sm_count);
@@ -1497,13 +1497,14 @@ int sweep_t_launch(bem_ctx* c, const T* S, int64_t lda, int n, double* b, unsign
 template <typename T, bool UPPER>
 int sweep_launch(bem_ctx* c, const T* S, int64_t lda, int n, double* b, unsigned* flags, unsigned tag,
                  int* status) {
-  static int grid[2][2] = {{0, 0}, {0, 0}};  // CTAs per SM, per (T, direction)
+  static DeviceOnce ok;  // per instantiation and device
   const size_t dsm = (size_t)kSolveBlock * kSolveBlock * sizeof(T);
-  int& per_sm = grid[sizeof(T) == 8][UPPER ? 1 : 0];
-  if (per_sm == 0) {
+  if (ok.pending()) {
+    int per_sm = 0;
     BEM_CUDA(c, cudaFuncSetAttribute(sweep_kernel<T, UPPER>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsm));
     BEM_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_kernel<T, UPPER>, kSweepThreads, dsm));
     if (per_sm < 1) return bem_fail(c, BEM_ERR_CUDA, "triangular sweep kernel does not fit on an SM");
+    ok.mark();
   }
   const int nblk = (n + kSolveBlock - 1) / kSolveBlock;
   const int G = std::min(nblk, c->sm_count);  // one CTA per SM: the whole diagonal block in smem
@@ -1577,10 +1578,10 @@ int lu_prepare_inverses(bem_ctx* c, const T* S, int64_t lda, int n) {
     BEM_CUDA(c, c->dinv.alloc(need));
   }
   const int smem = kSolveBlock * kInvPitch * (int)sizeof(double);
-  static bool attr[2] = {false, false};
-  if (!attr[sizeof(T) == 8]) {
+  static DeviceOnce attr;  // per instantiation and device
+  if (attr.pending()) {
     BEM_CUDA(c, cudaFuncSetAttribute(diag_inv_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    attr[sizeof(T) == 8] = true;
+    attr.mark();
   }
   diag_inv_kernel<T><<<dim3(nblk, 2), 256, smem, c->stream>>>(S, lda, n, c->dinv.p);
   BEM_LAUNCH_CHECK(c);
@@ -1594,13 +1595,13 @@ int lu_prepare_inverses(bem_ctx* c, const T* S, int64_t lda, int n) {
 template <typename T, bool UPPER>
 int sweep_inv_launch(bem_ctx* c, const T* S, int64_t lda, int n, double* b, unsigned long long* slots,
                      unsigned tag, int* status) {
-  static int attr_bytes[2][2] = {{0, 0}, {0, 0}};
+  static int attr_bytes[64] = {};  // per instantiation: the attribute set so far, per device
   const int nblk = (n + kSolveBlock - 1) / kSolveBlock;
   const int G = std::min(nblk, c->sm_count);
   const int nown = (nblk + G - 1) / G;
   const size_t dsm = ((size_t)kSolveBlock * kSolveBlock + (size_t)nown * kSolveBlock) * sizeof(double);
   if (dsm > 227 * 1024) return bem_fail(c, BEM_ERR_ARG, "block-inverse sweep: too many blocks per SM");
-  int& set = attr_bytes[sizeof(T) == 8][UPPER ? 1 : 0];
+  int& set = attr_bytes[current_device()];
   if ((int)dsm > set) {
     BEM_CUDA(c, cudaFuncSetAttribute(sweep_inv_kernel<T, UPPER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)dsm));

@@ -392,7 +392,11 @@ int gemm_umma_bf16x3(bem_ctx* c, int M, int N, int K, const float* A, int64_t ld
     if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess || !fn)
       return bem_fail(c, BEM_ERR_CUDA, "cuTensorMapEncodeTiled not available");
     g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }
+  static DeviceOnce attr;  // the kernel attribute is per device
+  if (attr.pending()) {
     cudaFuncSetAttribute(umma_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem);
+    attr.mark();
   }
   const size_t na = (size_t)M * K, nb_ = (size_t)N * K;
   const size_t need = 2 * (na + nb_) * sizeof(__nv_bfloat16) + 256;
