@@ -33,13 +33,18 @@ BEM_PROF_TRAILING = 2
 BEM_ASM_FP64 = 0
 BEM_ASM_FP32_FAR = 1
 BEM_IP_KELVIN_CONSISTENT = 1
+BEM_PIVOT_PARTIAL = 0
+BEM_PIVOT_WINDOW = 1
+BEM_OPT_PIVOTING = 1
+BEM_OPT_WAIT_LIMIT_MS = 2
+BEM_OPT_WITHHOLD_BLOCK = 3
 
 # every symbol the header declares, for the export check
 EXPORTS = [
     "bem_ctx_create", "bem_ctx_destroy", "bem_last_error", "bem_sync", "bem_get_stream",
-    "bem_set_mesh",
+    "bem_set_option", "bem_set_mesh",
     "bem_set_material", "bem_set_bc", "bem_set_pins", "bem_precompute_geometry",
-    "bem_get_geometry", "bem_ghmat8", "bem_get_hg", "bem_solve", "bem_dgesv",
+    "bem_get_geometry", "bem_ghmat8", "bem_set_system", "bem_get_rows", "bem_get_hg", "bem_solve", "bem_dgesv",
     "bem_reorganize", "bem_boundary_stresses", "bem_solve_transposed", "bem_adjoint_gradient", "bem_internal_points", "bem_device_state",
     "bem_internal_points_device", "bem_profile_begin", "bem_profile_end",
     "bem_dgesv_noalloc", "bem_batch_create", "bem_batch_destroy", "bem_batch_last_error",
@@ -61,7 +66,7 @@ class BemError(RuntimeError):
 class SolveInfo(C.Structure):
     _fields_ = [("iterations", C.c_int), ("restarts", C.c_int), ("rel_residual", C.c_double),
                 ("factor_seconds", C.c_double), ("refine_seconds", C.c_double),
-                ("gflops", C.c_double)]
+                ("gflops", C.c_double), ("pivoting", C.c_int), ("fallbacks", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -118,6 +123,7 @@ def load(build_if_needed: bool = True):
     L.bem_last_error.restype = C.c_char_p
     L.bem_sync.argtypes = [_vp]
     L.bem_get_stream.argtypes = [_vp, C.POINTER(C.c_void_p)]
+    L.bem_set_option.argtypes = [_vp, C.c_int, C.c_int64]
     L.bem_set_mesh.argtypes = [_vp, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp]
     L.bem_set_material.argtypes = [_vp, C.c_double, C.c_double]
     L.bem_set_bc.argtypes = [_vp, _vp, _vp]
@@ -125,6 +131,8 @@ def load(build_if_needed: bool = True):
     L.bem_precompute_geometry.argtypes = [_vp]
     L.bem_get_geometry.argtypes = [_vp] + [_vp] * 8
     L.bem_ghmat8.argtypes = [_vp, C.c_int, _vp, C.c_int64, _vp]
+    L.bem_set_system.argtypes = [_vp, C.c_int, _vp, C.c_int64, _vp]
+    L.bem_get_rows.argtypes = [_vp, C.c_int, C.c_int, _vp, C.c_int64, _vp]
     L.bem_get_hg.argtypes = [_vp, C.c_int, C.c_int, _vp, C.c_int64, _vp, C.c_int64]
     L.bem_solve.argtypes = [_vp, C.c_int, C.c_double, C.c_int, _vp, _ip, C.POINTER(SolveInfo)]
     L.bem_dgesv.argtypes = [_vp, C.c_int, C.c_int, _vp, C.c_int, _vp, _vp, C.c_int, _ip]
@@ -190,6 +198,10 @@ class Context:
 
     def sync(self):
         self.check(self.L.bem_sync(self.h), "sync")
+
+    def set_option(self, option: int, value: int):
+        """bem_set_option: BEM_OPT_PIVOTING, BEM_OPT_WAIT_LIMIT_MS, BEM_OPT_WITHHOLD_BLOCK."""
+        self.check(self.L.bem_set_option(self.h, int(option), int(value)), "set_option")
 
     def profile_begin(self, timing=True):
         """timing: True / BEM_PROF_PHASES (every LU phase), BEM_PROF_TRAILING (the

@@ -76,6 +76,19 @@ class Quadesth:
                                              _lib.ptr(FI)), "ghmat8")
         return (A, FI) if return_system else None
 
+    def system_rows(self, in0: int, in1: int):
+        """Rows of A and FI for collocation nodes [in0, in1) (3 rows per node), read from
+        the device after ghmat8 (before an FP64 factorisation overwrites A)."""
+        r0, r1 = 3 * in0, 3 * in1
+        A = np.zeros((r1 - r0, self.mesh.ndof), order="F")
+        FI = np.zeros(r1 - r0)
+        self.ctx.check(self.ctx.L.bem_get_rows(self.ctx.h, r0, r1, _lib.ptr(A), r1 - r0, _lib.ptr(FI)),
+                       "get_rows")
+        return A, FI
+
+    def set_option(self, option: int, value: int) -> None:
+        self.ctx.set_option(option, value)
+
     def hg(self, in0: int = 0, in1: Optional[int] = None):
         in1 = self.mesh.n if in1 is None else in1
         nr = 3 * (in1 - in0)
@@ -233,6 +246,30 @@ class Batch:
         if self.h:
             self.L.bem_batch_destroy(self.h)
             self.h = None
+
+
+def solve_system(A: np.ndarray, FI: np.ndarray, precision: str = "fp32-ir", tol: float = 1e-13,
+                 max_iter: int = 50, ctx: Optional[_lib.Context] = None,
+                 pivoting: Optional[int] = None):
+    """solve_linear_system (solver_mod.f90:17) for any dense system in any precision
+    mode: A (n x n) and FI (n) go to the device (bem_set_system), bem_solve solves.
+    Returns (x, solve_info)."""
+    ctx = ctx or _lib.Context(0)
+    A = np.asfortranarray(A, dtype=np.float64)
+    FI = np.ascontiguousarray(FI, dtype=np.float64)
+    n = A.shape[0]
+    if pivoting is not None:
+        ctx.set_option(_lib.BEM_OPT_PIVOTING, pivoting)
+    ctx.check(ctx.L.bem_set_system(ctx.h, n, _lib.ptr(A), n, _lib.ptr(FI)), "set_system")
+    x = np.zeros(n)
+    info = _lib.C.c_int(0)
+    st = _lib.SolveInfo()
+    rc = ctx.L.bem_solve(ctx.h, PRECISIONS[precision], tol, max_iter, _lib.ptr(x), _lib.C.byref(info),
+                         _lib.C.byref(st))
+    if rc > 0 or info.value != 0:
+        raise SolverFailure(info.value or rc)
+    ctx.check(rc, "solve")
+    return x, st.as_dict()
 
 
 def dgesv(A: np.ndarray, B: np.ndarray, ctx: Optional[_lib.Context] = None):

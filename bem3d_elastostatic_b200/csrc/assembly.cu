@@ -698,6 +698,8 @@ int launch_ghmat8(bem_ctx* c, int precision) {
     BEM_LAUNCH_CHECK(c);
   }
   c->have_system = true;
+  c->mesh_system = true;
+  c->nsys = N;
   c->have_solution = false;
   c->factored_fp64 = false;
   return BEM_OK;

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <string>
 #include <vector>
 
@@ -89,10 +90,13 @@ inline int current_device() {
   cudaGetDevice(&d);
   return d & 63;
 }
+// The bits are atomic: host threads that set up different devices at the same time
+// each keep their bit (a lost bit would only repeat the set-up, but a plain
+// read-modify-write from several threads is a data race).
 struct DeviceOnce {
-  unsigned long long bits = 0;
-  bool pending() const { return ((bits >> current_device()) & 1ull) == 0; }
-  void mark() { bits |= 1ull << current_device(); }
+  std::atomic<unsigned long long> bits{0};
+  bool pending() const { return ((bits.load(std::memory_order_acquire) >> current_device()) & 1ull) == 0; }
+  void mark() { bits.fetch_or(1ull << current_device(), std::memory_order_acq_rel); }
 };
 
 // A factorisation's launch sequence captured as a CUDA graph and replayed while every
@@ -157,6 +161,8 @@ struct bem_ctx {
   // system
   bem::DBuf<double> A, FI, X, U, DFI;  // FI: rhs; X: solution; U, DFI: reorganized u, t
   int64_t lda = 0;
+  int64_t nsys = 0;          // order of the system in A (3n after ghmat8, any n after set_system)
+  bool mesh_system = false;  // A and FI come from ghmat8 on the current mesh
   bool have_system = false, have_solution = false, factored_fp64 = false;
 
   // LU / refinement workspace
@@ -191,6 +197,15 @@ struct bem_ctx {
   // 3 = BF16 x3 split on mma.sync, 1 = plain BF16 (mma.sync), 0 = SIMT FP32
   int f64_gemm = 1;
   int f32_gemm = 4;
+  // pivoting of the next factorisation: true = the pivot search of each 32-wide
+  // sub-panel restricted to its diagonal block (the mixed-precision modes, with a
+  // fallback to partial pivoting), false = partial pivoting (DGESV)
+  bool lu_window = false;
+  int pivot_pref = BEM_PIVOT_WINDOW;  // BEM_OPT_PIVOTING
+  // bounded device waits (BEM_OPT_WAIT_LIMIT_MS), in ns, and the test-only withheld
+  // sweep block (BEM_OPT_WITHHOLD_BLOCK, -1 = none)
+  unsigned long long wait_ns = 2000000000ull;
+  int withhold_block = -1;
   int f32_gemm_override = -1;  // BEM_F32_GEMM environment override (0, 1, 3)
   // tcgen05 trailing update: BF16 hi/lo operand copies and its error word
   bem::DBuf<unsigned char> umma_buf;

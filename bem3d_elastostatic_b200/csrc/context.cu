@@ -6,6 +6,7 @@
 // recomputes inside its hot loop (assembly_mod.f90:149-161, 194-206), and the
 // conflict-free element schedule of the assembly kernel.  All numerics run on the GPU.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -146,10 +147,34 @@ int bem_get_stream(bem_ctx* c, void** stream) {
   return BEM_OK;
 }
 
+int bem_set_option(bem_ctx* c, int option, int64_t value) {
+  if (!c) return BEM_ERR_ARG;
+  switch (option) {
+    case BEM_OPT_PIVOTING:
+      if (value != BEM_PIVOT_WINDOW && value != BEM_PIVOT_PARTIAL)
+        return bem_fail(c, BEM_ERR_ARG, "set_option: pivoting must be BEM_PIVOT_WINDOW or BEM_PIVOT_PARTIAL");
+      c->pivot_pref = (int)value;
+      return BEM_OK;
+    case BEM_OPT_WAIT_LIMIT_MS:
+      if (value < 1 || value > 60000) return bem_fail(c, BEM_ERR_ARG, "set_option: wait limit must be 1..60000 ms");
+      c->wait_ns = (unsigned long long)value * 1000000ull;
+      return BEM_OK;
+    case BEM_OPT_WITHHOLD_BLOCK:
+      if (value < -1 || value > INT32_MAX) return bem_fail(c, BEM_ERR_ARG, "set_option: bad block index");
+      c->withhold_block = (int)value;
+      return BEM_OK;
+    default:
+      return bem_fail(c, BEM_ERR_ARG, "set_option: unknown option");
+  }
+}
+
 int bem_set_mesh(bem_ctx* c, int n, int ne, const double* x, const double* y, const double* z,
                  const int* nconec, const int* kconec) {
   if (!c || n <= 0 || ne <= 0 || !x || !y || !z || !nconec || !kconec)
     return bem_fail(c, BEM_ERR_ARG, "set_mesh: bad arguments");
+  for (int i = 0; i < n; ++i)
+    if (!std::isfinite(x[i]) || !std::isfinite(y[i]) || !std::isfinite(z[i]))
+      return bem_fail(c, BEM_ERR_ARG, "set_mesh: a node coordinate is not finite");
   BEM_CUDA(c, cudaSetDevice(c->device));
   c->h_nconec.assign(nconec, nconec + ne);
   c->h_kconec.assign(kconec, kconec + 9 * (size_t)ne);
@@ -273,6 +298,46 @@ int bem_ghmat8(bem_ctx* c, int asm_precision, double* A_out, int64_t lda_out, do
   return BEM_OK;
 }
 
+int bem_set_system(bem_ctx* c, int n, const double* A, int64_t lda_in, const double* FI) {
+  if (!c || !A || !FI || n <= 0 || lda_in < n) return bem_fail(c, BEM_ERR_ARG, "set_system: bad arguments");
+  BEM_CUDA(c, cudaSetDevice(c->device));
+  const int64_t lda = ((int64_t)n + 31) / 32 * 32;
+  if (c->A.count != (size_t)(lda * n)) {
+    c->A.release();
+    if (c->A.alloc((size_t)(lda * n)) != cudaSuccess) return bem_fail(c, BEM_ERR_OOM, "set_system: allocating A");
+  }
+  c->lda = lda;
+  BEM_CUDA(c, c->FI.alloc(n));
+  BEM_CUDA(c, cudaMemsetAsync(c->A.p, 0, c->A.bytes(), c->stream));  // the padding rows stay zero
+  BEM_CUDA(c, cudaMemcpy2DAsync(c->A.p, lda * sizeof(double), A, lda_in * sizeof(double), (size_t)n * sizeof(double),
+                                n, cudaMemcpyHostToDevice, c->stream));
+  BEM_CUDA(c, cudaMemcpyAsync(c->FI.p, FI, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  BEM_CUDA(c, cudaStreamSynchronize(c->stream));
+  c->dinv_src = nullptr;
+  c->nsys = n;
+  c->have_system = true;
+  c->mesh_system = false;
+  c->have_solution = false;
+  c->factored_fp64 = false;
+  return BEM_OK;
+}
+
+int bem_get_rows(bem_ctx* c, int r0, int r1, double* A_rows, int64_t ld, double* FI_rows) {
+  if (!c || !A_rows) return bem_fail(c, BEM_ERR_ARG, "get_rows: null argument");
+  const int64_t N = c->nsys;
+  if (r0 < 0 || r1 > N || r1 <= r0 || ld < r1 - r0) return bem_fail(c, BEM_ERR_ARG, "get_rows: bad row range");
+  if (!c->have_system) return bem_fail(c, BEM_ERR_STATE, "get_rows before ghmat8");
+  if (c->factored_fp64) return bem_fail(c, BEM_ERR_STATE, "get_rows: A was overwritten by its FP64 factors");
+  BEM_CUDA(c, cudaSetDevice(c->device));
+  BEM_CUDA(c, cudaMemcpy2DAsync(A_rows, ld * sizeof(double), c->A.p + r0, c->lda * sizeof(double),
+                                (size_t)(r1 - r0) * sizeof(double), N, cudaMemcpyDeviceToHost, c->stream));
+  if (FI_rows)
+    BEM_CUDA(c, cudaMemcpyAsync(FI_rows, c->FI.p + r0, (size_t)(r1 - r0) * sizeof(double), cudaMemcpyDeviceToHost,
+                                c->stream));
+  BEM_CUDA(c, cudaStreamSynchronize(c->stream));
+  return BEM_OK;
+}
+
 int bem_get_hg(bem_ctx* c, int in0, int in1, double* H, int64_t ldh, double* G, int64_t ldg) {
   if (!c || !H || !G || in0 < 0 || in1 > c->n || in1 <= in0)
     return bem_fail(c, BEM_ERR_ARG, "get_hg: bad row range");
@@ -301,7 +366,7 @@ int bem_solve(bem_ctx* c, int precision, double rel_tol, int max_iter, double* F
   if (!c->have_system) return bem_fail(c, BEM_ERR_STATE, "solve before ghmat8");
   BEM_CUDA(c, cudaSetDevice(c->device));
   *info = 0;
-  const int64_t N = 3 * (int64_t)c->n;
+  const int64_t N = c->nsys;
   bem_solve_info st{};
   int rc;
   BEM_CUDA(c, c->X.alloc(N));
@@ -372,6 +437,7 @@ int bem_dgesv(bem_ctx* c, int n, int nrhs, double* A, int lda, int* ipiv, double
 int bem_reorganize(bem_ctx* c, double* FI_out, double* DFI_out) {
   if (!c) return BEM_ERR_ARG;
   if (!c->have_solution) return bem_fail(c, BEM_ERR_STATE, "reorganize before solve");
+  if (!c->mesh_system) return bem_fail(c, BEM_ERR_STATE, "reorganize: the system was not assembled by ghmat8");
   BEM_CUDA(c, cudaSetDevice(c->device));
   int rc = bem::launch_reorganize(c);
   if (rc) return rc;
@@ -389,6 +455,7 @@ int bem_boundary_stresses(bem_ctx* c, double* sigma_elem, double* sigma_node, do
   if (!c) return BEM_ERR_ARG;
   if (!sigma_node || !prin || !vm) return bem_fail(c, BEM_ERR_ARG, "boundary_stresses: null output");
   if (!c->have_solution) return bem_fail(c, BEM_ERR_STATE, "boundary stresses before solve");
+  if (!c->mesh_system) return bem_fail(c, BEM_ERR_STATE, "boundary stresses: the system was not assembled by ghmat8");
   BEM_CUDA(c, cudaSetDevice(c->device));
   // u and t of the current solution (cheap: two small kernels)
   int rc = bem::launch_reorganize(c);
@@ -412,7 +479,7 @@ int bem_solve_transposed(bem_ctx* c, double* g) {
   if (!c->factored_fp64 || !c->have_solution)
     return bem_fail(c, BEM_ERR_STATE, "solve_transposed needs a solve with BEM_PREC_FP64 first");
   BEM_CUDA(c, cudaSetDevice(c->device));
-  const size_t N = 3 * (size_t)c->n;
+  const size_t N = (size_t)c->nsys;
   bem::DBuf<double> d;
   BEM_CUDA(c, d.alloc(N));
   BEM_CUDA(c, cudaMemcpyAsync(d.p, g, N * sizeof(double), cudaMemcpyHostToDevice, c->stream));
@@ -426,6 +493,7 @@ int bem_solve_transposed(bem_ctx* c, double* g) {
 int bem_adjoint_gradient(bem_ctx* c, const double* lambda, double* grad_xyz, double* grad_mat) {
   if (!c || !lambda || !grad_xyz || !grad_mat) return BEM_ERR_ARG;
   if (!c->have_solution || !c->have_geometry) return bem_fail(c, BEM_ERR_STATE, "adjoint_gradient before solve");
+  if (!c->mesh_system) return bem_fail(c, BEM_ERR_STATE, "adjoint_gradient: the system was not assembled by ghmat8");
   BEM_CUDA(c, cudaSetDevice(c->device));
   int rc = bem::launch_reorganize(c);  // u and t of the current solution
   if (rc) return rc;

@@ -20,7 +20,7 @@ __global__ void etaxja_kernel(int ne, const double* __restrict__ x, const double
                               const double* __restrict__ z, const int* __restrict__ nconec,
                               const int* __restrict__ kconec, double* eta1, double* eta2,
                               double* eta3, double* xja, double* xg1, double* xg2, double* xg3,
-                              double* ff, double* tab) {
+                              double* ff, double* tab, int* bad) {
   const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (gid >= (int64_t)ne * kGp) return;
   const int e = (int)(gid / kGp);
@@ -68,6 +68,9 @@ __global__ void etaxja_kernel(int ne, const double* __restrict__ x, const double
   }
   double J, n1, n2, n3;
   jacobian_dc<double>(ncone, fd1, fd2, xj1, xj2, xj3, J, n1, n2, n3);
+  // a zero (or non-finite) Jacobian makes the unit normal a division by zero
+  // (assembly_mod.f90:331-334): the element is degenerate
+  if (bad && !(J > 0.0 && J < INFINITY && a - a == 0.0 && b - b == 0.0 && c - c == 0.0)) atomicExch(bad, 1);
   eta1[kk] = n1;
   eta2[kk] = n2;
   eta3[kk] = n3;
@@ -108,8 +111,11 @@ int upload_quadrature_constants() {
 
 int launch_geometry(bem_ctx* c) {
   if (!c->have_mesh) return bem_fail(c, BEM_ERR_STATE, "precompute_geometry before set_mesh");
-  if (upload_quadrature_constants() != 0)
-    return bem_fail(c, BEM_ERR_CUDA, "uploading quadrature constants");
+  static DeviceOnce constants;  // __constant__ tables are per device
+  if (constants.pending()) {
+    if (upload_quadrature_constants() != 0) return bem_fail(c, BEM_ERR_CUDA, "uploading quadrature constants");
+    constants.mark();
+  }
   const size_t ng = (size_t)kGp * c->ne;
   for (auto* b : {&c->eta1, &c->eta2, &c->eta3, &c->xja, &c->xg1, &c->xg2, &c->xg3})
     BEM_CUDA(c, b->alloc(ng));
@@ -117,10 +123,19 @@ int launch_geometry(bem_ctx* c) {
   BEM_CUDA(c, c->tab.alloc((size_t)kTabStride * c->ne));
   const int threads = 128;
   const int64_t blocks = ((int64_t)ng + threads - 1) / threads;
+  if (c->status.count < 1) BEM_CUDA(c, c->status.alloc(1));
+  BEM_CUDA(c, cudaMemsetAsync(c->status.p, 0, sizeof(int), c->stream));
   etaxja_kernel<<<(unsigned)blocks, threads, 0, c->stream>>>(
       c->ne, c->x.p, c->y.p, c->z.p, c->nconec.p, c->kconec.p, c->eta1.p, c->eta2.p, c->eta3.p,
-      c->xja.p, c->xg1.p, c->xg2.p, c->xg3.p, c->ff.p, c->tab.p);
+      c->xja.p, c->xg1.p, c->xg2.p, c->xg3.p, c->ff.p, c->tab.p, c->status.p);
   BEM_LAUNCH_CHECK(c);
+  int bad = 0;
+  BEM_CUDA(c, cudaMemcpyAsync(&bad, c->status.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  BEM_CUDA(c, cudaStreamSynchronize(c->stream));
+  if (bad) {
+    c->have_geometry = false;
+    return bem_fail(c, BEM_ERR_MESH, "degenerate element: zero or non-finite Jacobian at a Gauss point");
+  }
   c->have_geometry = true;
   return BEM_OK;
 }
@@ -137,7 +152,7 @@ int launch_geometry_arrays(cudaStream_t stream, int ne, const double* x, const d
   const int64_t blocks = ((int64_t)ng + threads - 1) / threads;
   etaxja_kernel<<<(unsigned)blocks, threads, 0, stream>>>(ne, x, y, z, nconec, kconec, ref, ref + ng,
                                                           ref + 2 * ng, ref + 3 * ng, ref + 4 * ng,
-                                                          ref + 5 * ng, ref + 6 * ng, ref + 7 * ng, tab);
+                                                          ref + 5 * ng, ref + 6 * ng, ref + 7 * ng, tab, nullptr);
   return cudaGetLastError() == cudaSuccess ? BEM_OK : BEM_ERR_CUDA;
 }
 

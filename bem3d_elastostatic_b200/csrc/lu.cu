@@ -19,6 +19,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <atomic>
 #include <vector>
 
 #include "lu.cuh"
@@ -29,7 +30,6 @@ constexpr int kPitch = kPanelW + 1;  // shared-memory column pitch (conflict-fre
 constexpr int kInvBlock = 128;       // unit-triangle inverse block of the block-row TRSM
 constexpr int kSolveBlock = 128;     // diagonal block of the triangular solves
 constexpr int kPanelSmemMax = 200 * 1024;  // dynamic shared memory of a panel CTA
-constexpr long long kSpinLimit = 1ll << 24;
 constexpr int kSweepThreads = 512;   // threads of a triangular sweep CTA (4 per row of a block)
 
 __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
@@ -95,7 +95,8 @@ constexpr int panel_threads() {
 template <typename T>
 __global__ void __launch_bounds__(panel_threads<T>(), 1)
     panel_kernel(T* S, int64_t lda, int n, int r0, int w, int chunk, int* piv, double* cand_val,
-                 int* cand_idx, T* cand_col, T* diag_col, unsigned* barrier, unsigned bar_base, int* status) {
+                 int* cand_idx, T* cand_col, T* diag_col, unsigned* barrier, unsigned bar_base, int* status,
+                 unsigned long long wait_ns) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* col = reinterpret_cast<T*>(smem_raw);  // [chunk][kPitch]
   __shared__ T s_pv[kPanelW];  // the winning candidate column
@@ -151,10 +152,11 @@ __global__ void __launch_bounds__(panel_threads<T>(), 1)
     if (tid == 0) {
       red_release_add_u32(barrier, 1u);
       const unsigned target = bar_base + (unsigned)(t + 1) * (unsigned)G;
-      long long spins = 0;
+      const unsigned long long t0 = globaltimer_ns();
+      unsigned spins = 0;
       int abort = 0;
       while (ld_acquire_u32(barrier) < target) {
-        if (++spins > kSpinLimit || *((volatile int*)status) != 0) {
+        if ((++spins & 63u) == 0 && (globaltimer_ns() - t0 > wait_ns || *((volatile int*)status) != 0)) {
           abort = 1;
           break;
         }
@@ -218,12 +220,133 @@ __global__ void __launch_bounds__(panel_threads<T>(), 1)
   }
 }
 
+// Window pivoting: the sub-panel's pivot search is restricted to its w x w diagonal
+// block (T rows r0..r0+w), so the sub-panel needs no grid-wide exchange.  Every CTA
+// factors that block redundantly in shared memory (warp 0: lane c owns column c of the
+// window, one warp argmax per pivot, ties to the smallest index as the partial-pivot
+// kernel), while its other warps load their columns; then each thread eliminates one
+// column c >= r0 + w of the sub-panel (T row c) with the recorded steps, the same
+// operations panel_kernel applies to a non-pivot column.  CTA 0 writes the pivots, the
+// first exact zero pivot (status[1]) and the factored block to `win` (w x w, leading
+// dimension kPanelW): the block is copied into S by the next launch (swap_rows_kernel),
+// since other CTAs of this launch may still be reading it from S.
+template <typename T>
+__global__ void __launch_bounds__(256) window_panel_kernel(T* S, int64_t lda, int n, int r0, int w, int* piv,
+                                                           T* win, int* status) {
+  __shared__ T D[kPanelW][kPanelW + 1];  // D[c][j] = S(r0 + j, r0 + c)
+  __shared__ int s_p[kPanelW];
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int c = r0 + w + blockIdx.x * blockDim.x + tid;  // this thread's column (T row)
+  constexpr int V = 16 / sizeof(T);                       // elements per 16-byte vector
+  const bool vec = ((lda % V) == 0) && ((r0 % V) == 0) && ((reinterpret_cast<uintptr_t>(S) & 15) == 0);
+  // every load of the thread's column before the window's barrier (r0 + 32 <= lda: the
+  // rows up to 32 exist in every column; only rows < w are used or stored)
+  T x[kPanelW];
+  if (c < n) {
+    const T* src = S + r0 + (int64_t)c * lda;
+    if (vec && r0 + kPanelW <= lda) {
+#pragma unroll
+      for (int q = 0; q < kPanelW / V; ++q) {
+        const int4 v = *reinterpret_cast<const int4*>(src + q * V);
+        const T* e = reinterpret_cast<const T*>(&v);
+#pragma unroll
+        for (int u = 0; u < V; ++u) x[q * V + u] = e[u];
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < kPanelW; ++j) x[j] = (j < w) ? src[j] : T(0);
+    }
+  }
+  if (tid < kPanelW) {
+    // warp 0: stage and factor the window
+    for (int cc = 0; cc < kPanelW; ++cc)  // lane = row: one coalesced segment per column
+      D[cc][lane] = (cc < w && lane < w) ? S[r0 + lane + (int64_t)(r0 + cc) * lda] : T(0);
+    __syncwarp();
+    for (int t = 0; t < w; ++t) {
+      double bv = (lane >= t && lane < w) ? fabs((double)D[lane][t]) : -1.0;
+      int bc = (lane >= t && lane < w) ? lane : INT_MAX, bg = 0;
+      for (int off = 16; off > 0; off >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
+        const int oc = __shfl_xor_sync(0xffffffffu, bc, off);
+        better(bv, bc, bg, ov, oc, 0);
+      }
+      const int p = bc;
+      if (lane == 0) s_p[t] = p;
+      if (p != t && lane < w) {
+        const T a = D[t][lane];
+        D[t][lane] = D[p][lane];
+        D[p][lane] = a;
+      }
+      __syncwarp();
+      const T pv = D[t][t];
+      if (pv != T(0) && lane > t && lane < w) {
+        const T l = D[lane][t] / pv;
+        D[lane][t] = l;
+        for (int j = t + 1; j < w; ++j) D[lane][j] -= l * D[t][j];
+      }
+      __syncwarp();
+    }
+    if (blockIdx.x == 0) {
+      if (lane < w) {
+        piv[r0 + lane] = r0 + s_p[lane];
+        for (int j = 0; j < w; ++j) win[j + lane * kPanelW] = D[lane][j];
+      }
+      if (lane == 0) {
+        for (int t = 0; t < w; ++t)
+          if (D[t][t] == T(0)) {
+            if (status[1] == 0) status[1] = r0 + t + 1;
+            break;
+          }
+      }
+    }
+  }
+  __syncthreads();
+  if (c >= n) return;
+  // eliminate: step t scales x[t] by the pivot and updates the entries below it
+#pragma unroll
+  for (int t = 0; t < kPanelW; ++t) {
+    if (t < w) {
+      const T pv = D[t][t];
+      if (pv != T(0)) {
+        const T l = x[t] / pv;
+        x[t] = l;
+#pragma unroll
+        for (int j = t + 1; j < kPanelW; ++j)
+          if (j < w) x[j] -= l * D[t][j];
+      }
+    }
+  }
+  T* dst = S + r0 + (int64_t)c * lda;
+  if (vec && w == kPanelW) {
+#pragma unroll
+    for (int q = 0; q < kPanelW / V; ++q) {
+      int4 v;
+      T* e = reinterpret_cast<T*>(&v);
+#pragma unroll
+      for (int u = 0; u < V; ++u) e[u] = x[q * V + u];
+      *reinterpret_cast<int4*>(dst + q * V) = v;
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < kPanelW; ++j)
+      if (j < w) dst[j] = x[j];
+  }
+}
+
 // Applies swaps k0+t <-> piv[k0+t] (t = 0..w-1 in order) to rows [a0,a1) and [b0,b1).
+// With window pivoting `win` (nullable) holds the factored w x w diagonal block of the
+// sub-panel (leading dimension kPanelW), which CTA 0 copies into S(k0.., k0..) first;
+// the swaps below touch no row of that block.
 template <typename T>
 __global__ void swap_rows_kernel(T* S, int64_t lda, const int* piv, int k0, int w, int a0, int a1, int b0,
-                                 int b1) {
+                                 int b1, const T* win) {
   __shared__ int sp[kPanelW];
   if (threadIdx.x < w) sp[threadIdx.x] = piv[k0 + threadIdx.x];
+  if (win && blockIdx.x == 0)
+    for (int i = threadIdx.x; i < w * w; i += blockDim.x) {
+      const int j = i % w, cc = i / w;
+      S[k0 + j + (int64_t)(k0 + cc) * lda] = win[j + cc * kPanelW];
+    }
   __syncthreads();
   const int na = a1 - a0;
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -560,11 +683,23 @@ int panel_launch(bem_ctx* c, const LUWorkspace& ws, T* S, int64_t lda, int n, in
   unsigned* bar = ws.barrier;
   int* st = ws.status;
   unsigned bb = bar_base;
-  void* args[] = {&S, &lda, &n, &r0, &w, &chunk, &piv, &cv, &ci, &cc, &dc, &bar, &bb, &st};
+  unsigned long long wns = c->wait_ns;
+  void* args[] = {&S, &lda, &n, &r0, &w, &chunk, &piv, &cv, &ci, &cc, &dc, &bar, &bb, &st, &wns};
   BEM_CUDA(c, cudaLaunchCooperativeKernel((void*)panel_kernel<T>, dim3(G), dim3(panel_threads<T>()), args, smem,
                                           c->stream));
   ++c->launches;
   bar_base += (unsigned)w * (unsigned)G;
+  return BEM_OK;
+}
+
+// Window-pivoted sub-panel: one plain launch, one thread per column right of the window.
+template <typename T>
+int window_panel_launch(bem_ctx* c, const LUWorkspace& ws, T* S, int64_t lda, int n, int r0, int w, int* piv) {
+  const int64_t cols = (int64_t)n - r0 - w;
+  const unsigned G = (unsigned)std::max<int64_t>(1, (cols + 255) / 256);
+  window_panel_kernel<T><<<G, 256, 0, c->stream>>>(S, lda, n, r0, w, piv, reinterpret_cast<T*>(ws.cand_col),
+                                                   ws.status);
+  BEM_LAUNCH_CHECK(c);
   return BEM_OK;
 }
 
@@ -710,6 +845,9 @@ static int lu_factor_enqueue(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int
   T* V = reinterpret_cast<T*>(ws.inv);
   T* Y = reinterpret_cast<T*>(ws.ybuf);
   const int64_t ldy = ws.ldy;
+  // window pivoting (pivot search within each sub-panel's diagonal block) or partial
+  // pivoting (over every remaining row of T)
+  const bool window = c->lu_window;
   const size_t inv_smem = (size_t)kInvBlock * kInvBlock * sizeof(T);
   cudaFuncSetAttribute(inv_unit_upper_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inv_smem);
   cudaFuncSetAttribute(inv_unit_upper_f32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -721,16 +859,21 @@ static int lu_factor_enqueue(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int
     for (int r0 = j0; r0 < j0 + jb; r0 += kPanelW) {
       const int w = std::min(kPanelW, j0 + jb - r0);
       prof.begin(0, c->stream);
-      if ((rc = panel_launch<T>(c, ws, S, lda, n, r0, w, piv, bar_base))) return rc;
+      if (window) {
+        if ((rc = window_panel_launch<T>(c, ws, S, lda, n, r0, w, piv))) return rc;
+      } else if ((rc = panel_launch<T>(c, ws, S, lda, n, r0, w, piv, bar_base))) {
+        return rc;
+      }
       prof.end(c->stream);
       prof.begin(1, c->stream);
       // swaps on every other row of S: the earlier panels' multipliers (rows [0, r0),
-      // so that the factors end up as T = P L U) and the trailing rows
+      // so that the factors end up as T = P L U) and the trailing rows; with window
+      // pivoting this launch also stores the factored window block
       const int a0 = 0, a1 = r0, b0 = r0 + w, b1 = n;
       const int64_t rows = (int64_t)(a1 - a0) + (b1 - b0);
-      if (rows > 0) {
-        swap_rows_kernel<T><<<(unsigned)((rows + 255) / 256), 256, 0, c->stream>>>(S, lda, piv, r0, w, a0, a1, b0,
-                                                                                   b1);
+      if (rows > 0 || window) {
+        swap_rows_kernel<T><<<(unsigned)std::max<int64_t>(1, (rows + 255) / 256), 256, 0, c->stream>>>(
+            S, lda, piv, r0, w, a0, a1, b0, b1, window ? reinterpret_cast<const T*>(ws.cand_col) : nullptr);
         BEM_LAUNCH_CHECK(c);
       }
       prof.end(c->stream);
@@ -839,7 +982,8 @@ int lu_factor(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int* perm, int nb,
     return std::vector<long long>{(long long)(uintptr_t)S,  lda, n, nb, (long long)(uintptr_t)piv,
                                   (long long)(uintptr_t)ws.cand_val, (long long)(uintptr_t)c->umma_buf.p,
                                   (long long)c->umma_buf.count, (long long)(uintptr_t)c->umma_err.p,
-                                  c->f32_gemm, c->f64_gemm, prof.on, prof.trailing_only, c->sm_count};
+                                  c->f32_gemm, c->f64_gemm, prof.on, prof.trailing_only, c->sm_count,
+                                  c->lu_window ? 1 : 0};
   };
   int rc = BEM_OK;
   if (c->lu_graph_off) {
@@ -982,12 +1126,12 @@ __device__ void warp_upper_unit_solve(const T* D, int jb, double* w) {
 // of step s+1 first, and that owner then solves and publishes block k(s+1) before it
 // turns to its other blocks.  The dependent chain is one tile GEMV and one warp solve
 // per block; the rest of the factor streams from HBM alongside.  Diagonal blocks are
-// staged into shared memory one owned step ahead.  A wait that exceeds 2 s records
-// BEM_ERR_TIMEOUT in *status and ends the CTA.
+// staged into shared memory one owned step ahead.  A wait that exceeds the context's
+// wait limit (2 s by default) records BEM_ERR_TIMEOUT in *status and ends the CTA.
 template <typename T, bool UPPER>
 __global__ void __launch_bounds__(kSweepThreads, 1)
     sweep_kernel(const T* __restrict__ S, int64_t lda, int n, double* b, unsigned* flags, unsigned tag,
-                 int* status) {
+                 int* status, unsigned long long wait_ns) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* D = reinterpret_cast<T*>(smem_raw);  // [kSolveBlock][kSolveBlock] column-major
   __shared__ double ys[kSolveBlock];
@@ -1040,7 +1184,7 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
       const unsigned long long t0 = globaltimer_ns();
       unsigned it = 0;
       while (ld_acquire_u32(flags + s) != tag) {
-        if ((++it & 255u) == 0 && globaltimer_ns() - t0 > 2000000000ull) {
+        if ((++it & 255u) == 0 && (globaltimer_ns() - t0 > wait_ns || *((volatile int*)status) != 0)) {
           atomicExch(status, BEM_ERR_TIMEOUT);
           s_abort = 1;
           break;
@@ -1200,11 +1344,14 @@ __device__ __forceinline__ void ld_volatile_v2(const unsigned long long* p, unsi
 // L2 round trip both signals and delivers the block.  Every CTA loads its first tile of
 // step s before it waits for y_s; the owner of step s+1 handles that tile first and
 // then solves x = Dinv w from the inverse staged in shared memory one owned step ahead.
-// A wait that exceeds 2 s records BEM_ERR_TIMEOUT in *status and ends the CTA.
+// A wait that exceeds the context's wait limit records BEM_ERR_TIMEOUT in *status and
+// ends the CTA.  `withhold` (failure injection, -1 = none) is a step of the forward
+// sweep that is solved but not published, so that the waits for it run out.
 template <typename T, bool UPPER>
 __global__ void __launch_bounds__(kSweepThreads, 1)
     sweep_inv_kernel(const T* __restrict__ S, int64_t lda, int n, const double* __restrict__ Dinv, double* b,
-                     unsigned long long* slots, unsigned tag, int* status) {
+                     unsigned long long* slots, unsigned tag, int* status, unsigned long long wait_ns,
+                     int withhold) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int NB = kSolveBlock;
   constexpr bool kPrefetch = sizeof(T) == 4;  // double-buffered tile registers for FP32 factors
@@ -1256,7 +1403,8 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
       const double x = (red[0][t] + red[1][t]) + (red[2][t] + red[3][t]);
       const unsigned long long hi = (unsigned long long)tag << 32;
       const unsigned long long bits = (unsigned long long)__double_as_longlong(x);
-      st_volatile_v2(slots + (size_t)s * 256 + 2 * t, hi | (bits & 0xffffffffull), hi | (bits >> 32));
+      if (UPPER || s != withhold)  // a withheld step (failure injection) is never published
+        st_volatile_v2(slots + (size_t)s * 256 + 2 * t, hi | (bits & 0xffffffffull), hi | (bits >> 32));
       b[k0 + t] = x;
     }
     __syncthreads();  // Di and red are free again
@@ -1281,7 +1429,7 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
           ld_volatile_v2(p, w0, w1);
           if ((unsigned)(w0 >> 32) == tag && (unsigned)(w1 >> 32) == tag) break;
           if ((++it & 63u) == 0 &&
-              (globaltimer_ns() - t0 > 2000000000ull || *((volatile int*)status) != 0)) {
+              (globaltimer_ns() - t0 > wait_ns || *((volatile int*)status) != 0)) {
             atomicCAS(status, 0, BEM_ERR_TIMEOUT);
             s_abort = 1;
             w0 = w1 = 0;
@@ -1383,7 +1531,7 @@ __device__ void warp_upper_solve_t(const T* D, const double* rdiag, int jb, doub
 template <typename T, bool UPPER>
 __global__ void __launch_bounds__(kSweepThreads, 1)
     sweep_t_kernel(const T* __restrict__ S, int64_t lda, int n, double* b, unsigned* flags, unsigned tag,
-                   int* status) {
+                   int* status, unsigned long long wait_ns) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* D = reinterpret_cast<T*>(smem_raw);  // [kSolveBlock][kLdT]: D[r + c * kLdT] = T(k0 + r, k0 + c)
   __shared__ double ys[kSolveBlock];
@@ -1433,7 +1581,7 @@ __global__ void __launch_bounds__(kSweepThreads, 1)
       const unsigned long long t0 = globaltimer_ns();
       unsigned it = 0;
       while (ld_acquire_u32(flags + s) != tag) {
-        if ((++it & 255u) == 0 && globaltimer_ns() - t0 > 2000000000ull) {
+        if ((++it & 255u) == 0 && (globaltimer_ns() - t0 > wait_ns || *((volatile int*)status) != 0)) {
           atomicExch(status, BEM_ERR_TIMEOUT);
           s_abort = 1;
           break;
@@ -1487,7 +1635,9 @@ int sweep_t_launch(bem_ctx* c, const T* S, int64_t lda, int n, double* b, unsign
   }
   const int nblk = (n + kSolveBlock - 1) / kSolveBlock;
   const int G = std::min(nblk, c->sm_count);
-  void* args[] = {(void*)&S, (void*)&lda, (void*)&n, (void*)&b, (void*)&flags, (void*)&tag, (void*)&status};
+  unsigned long long wns = c->wait_ns;
+  void* args[] = {(void*)&S, (void*)&lda, (void*)&n, (void*)&b, (void*)&flags, (void*)&tag, (void*)&status,
+                  (void*)&wns};
   BEM_CUDA(c, cudaLaunchCooperativeKernel((void*)sweep_t_kernel<T, UPPER>, dim3(G), dim3(kSweepThreads), args, dsm,
                                           c->stream));
   ++c->launches;
@@ -1508,7 +1658,9 @@ int sweep_launch(bem_ctx* c, const T* S, int64_t lda, int n, double* b, unsigned
   }
   const int nblk = (n + kSolveBlock - 1) / kSolveBlock;
   const int G = std::min(nblk, c->sm_count);  // one CTA per SM: the whole diagonal block in smem
-  void* args[] = {(void*)&S, (void*)&lda, (void*)&n, (void*)&b, (void*)&flags, (void*)&tag, (void*)&status};
+  unsigned long long wns = c->wait_ns;
+  void* args[] = {(void*)&S, (void*)&lda, (void*)&n, (void*)&b, (void*)&flags, (void*)&tag, (void*)&status,
+                  (void*)&wns};
   BEM_CUDA(c, cudaLaunchCooperativeKernel((void*)sweep_kernel<T, UPPER>, dim3(G), dim3(kSweepThreads), args, dsm,
                                           c->stream));
   ++c->launches;
@@ -1595,25 +1747,34 @@ int lu_prepare_inverses(bem_ctx* c, const T* S, int64_t lda, int n) {
 template <typename T, bool UPPER>
 int sweep_inv_launch(bem_ctx* c, const T* S, int64_t lda, int n, double* b, unsigned long long* slots,
                      unsigned tag, int* status) {
-  static int attr_bytes[64] = {};  // per instantiation: the attribute set so far, per device
+  // per instantiation and device: the attribute is set once to the largest dynamic
+  // shared memory the device allows next to the kernel's static arrays, so that no
+  // later launch (of any order) needs to raise it
+  static std::atomic<int> max_dyn[64];
   const int nblk = (n + kSolveBlock - 1) / kSolveBlock;
   const int G = std::min(nblk, c->sm_count);
   const int nown = (nblk + G - 1) / G;
   const size_t dsm = ((size_t)kSolveBlock * kSolveBlock + (size_t)nown * kSolveBlock) * sizeof(double);
-  if (dsm > 227 * 1024) return bem_fail(c, BEM_ERR_ARG, "block-inverse sweep: too many blocks per SM");
-  int& set = attr_bytes[current_device()];
-  if ((int)dsm > set) {
-    BEM_CUDA(c, cudaFuncSetAttribute(sweep_inv_kernel<T, UPPER>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)dsm));
+  std::atomic<int>& lim = max_dyn[current_device()];
+  if (lim.load() == 0) {
+    cudaFuncAttributes fa{};
+    int optin = 0;
+    BEM_CUDA(c, cudaFuncGetAttributes(&fa, sweep_inv_kernel<T, UPPER>));
+    BEM_CUDA(c, cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device));
+    const int mx = optin - (int)fa.sharedSizeBytes;
+    BEM_CUDA(c, cudaFuncSetAttribute(sweep_inv_kernel<T, UPPER>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
     int per_sm = 0;
     BEM_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sweep_inv_kernel<T, UPPER>, kSweepThreads,
-                                                              dsm));
+                                                              (size_t)mx));
     if (per_sm < 1) return bem_fail(c, BEM_ERR_CUDA, "block-inverse sweep kernel does not fit on an SM");
-    set = (int)dsm;
+    lim.store(mx);
   }
+  if (dsm > (size_t)lim.load()) return bem_fail(c, BEM_ERR_ARG, "block-inverse sweep: too many blocks per SM");
   const double* dinv = c->dinv.p;
-  void* args[] = {(void*)&S, (void*)&lda, (void*)&n, (void*)&dinv, (void*)&b, (void*)&slots, (void*)&tag,
-                  (void*)&status};
+  unsigned long long wns = c->wait_ns;
+  int withhold = c->withhold_block;
+  void* args[] = {(void*)&S,     (void*)&lda,    (void*)&n,   (void*)&dinv, (void*)&b,
+                  (void*)&slots, (void*)&tag,    (void*)&status, (void*)&wns, (void*)&withhold};
   BEM_CUDA(c, cudaLaunchCooperativeKernel((void*)sweep_inv_kernel<T, UPPER>, dim3(G), dim3(kSweepThreads), args,
                                           dsm, c->stream));
   ++c->launches;

@@ -21,6 +21,14 @@
 //     counter and status words are cleared by every call, and calls that overlap on
 //     the GPU (different streams or host threads) race on it and must be serialised
 //     by the caller.
+// The call synchronises `stream` (it reads the factorisation's status words and
+// composes the pivot gather on the host).  Like bem_dgesv, the factors are those of
+// A^T in A's storage and d_ipiv is dgetrf's pivot sequence of A^T (see lu.cuh): the
+// solution of A X = B is exact LAPACK semantics, a reuse of dA/d_ipiv with dgetrs is
+// not.  When the factorisation itself fails (a negative status) d_ipiv is undefined;
+// otherwise it is 1-based on return, including an info > 0 return and a failed solve.
+#include <algorithm>
+#include <atomic>
 #include <cstdio>
 
 #include "lu.cuh"
@@ -43,7 +51,9 @@ constexpr size_t kNoAllocBytes = kFactorBytes + up256(kSolveDoubles * sizeof(dou
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
 constexpr int kMaxDevices = 64;
-void* g_scratch_addr[kMaxDevices] = {};
+// the array's device address per device (atomic: host threads may call on different
+// devices at the same time; two threads that race on one device store the same value)
+std::atomic<void*> g_scratch_addr[kMaxDevices];
 
 __global__ void one_based_kernel(int n, int* ipiv) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -60,14 +70,14 @@ extern "C" int bem_dgesv_noalloc(int n, int nrhs, double* dA, int lda, int* d_ip
   *info = 0;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return BEM_ERR_CUDA;
-  if (!g_scratch_addr[dev]) {
+  if (!g_scratch_addr[dev].load(std::memory_order_acquire)) {
     // set-up, once per device with that device current: the host-side symbol is only
     // a stand-in, the kernels need the array's device address
     void* p = nullptr;
     if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return BEM_ERR_CUDA;
-    g_scratch_addr[dev] = p;
+    g_scratch_addr[dev].store(p, std::memory_order_release);
   }
-  unsigned char* base = static_cast<unsigned char*>(g_scratch_addr[dev]);
+  unsigned char* base = static_cast<unsigned char*>(g_scratch_addr[dev].load(std::memory_order_acquire));
   if (bem::lu_workspace_bytes(n, kNoAllocNb, kNoAllocGmax, sizeof(double)) > kFactorBytes) return BEM_ERR_TOO_LARGE;
 
   // a context on the stack: no device memory of its own (its buffers stay empty)
@@ -75,16 +85,19 @@ extern "C" int bem_dgesv_noalloc(int n, int nrhs, double* dA, int lda, int* d_ip
   c.device = dev;
   c.stream = static_cast<cudaStream_t>(stream);
   cudaDeviceGetAttribute(&c.sm_count, cudaDevAttrMultiProcessorCount, dev);
+  // the candidate exchange of the panel launches is carved for kNoAllocGmax CTAs: every
+  // grid sized from the SM count stays within it on a part with more SMs
+  c.sm_count = std::min(c.sm_count, kNoAllocGmax);
   const bem::LUWorkspace ws = bem::lu_workspace_carve(base, n, kNoAllocNb, kNoAllocGmax, sizeof(double));
   double* solve_work = reinterpret_cast<double*>(base + kFactorBytes);
   int* perm = reinterpret_cast<int*>(base + kFactorBytes + up256(kSolveDoubles * sizeof(double)));
   int rc = bem::lu_factor_ws<double>(&c, dA, lda, n, d_ipiv, perm, kNoAllocNb, info, ws);
-  if (rc) return rc;
+  if (rc) return rc;  // the factorisation failed: d_ipiv is undefined
+  // from here on the pivots are complete: they are made 1-based on every return path
   if (*info == 0)
-    for (int j = 0; j < nrhs; ++j)
-      if ((rc = bem::lu_solve_ws<double>(&c, dA, lda, n, perm, dB + (int64_t)j * ldb, solve_work)))
-        return rc;
+    for (int j = 0; j < nrhs && rc == 0; ++j)
+      rc = bem::lu_solve_ws<double>(&c, dA, lda, n, perm, dB + (int64_t)j * ldb, solve_work);
   one_based_kernel<<<(n + 255) / 256, 256, 0, c.stream>>>(n, d_ipiv);
   if (cudaGetLastError() != cudaSuccess) return BEM_ERR_CUDA;
-  return *info;
+  return rc ? rc : *info;
 }

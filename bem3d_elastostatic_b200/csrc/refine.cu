@@ -87,7 +87,7 @@ __global__ void scale_kernel(int n, double a, const double* x, double* y) {
 }
 
 int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_solve_info* st, int* info) {
-  const int n = 3 * c->n;
+  const int n = (int)c->nsys;
   const int64_t lda = c->lda;
   *info = 0;
   if (c->factored_fp64) return bem_fail(c, BEM_ERR_STATE, "A was overwritten by an FP64 factorisation");
@@ -122,6 +122,16 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
   for (auto& e : c->solve_ev)
     if (!e) BEM_CUDA(c, cudaEventCreate(&e));
   cudaEvent_t e0 = c->solve_ev[0], e1 = c->solve_ev[1], e2 = c->solve_ev[2];
+  // Window pivoting first (pivot search within each 32-wide sub-panel's diagonal
+  // block: no grid-wide exchange per pivot); if that factorisation meets a zero pivot or
+  // its refinement does not converge, the solve is repeated with partial pivoting.
+  bool window = c->pivot_pref != BEM_PIVOT_PARTIAL;
+  int fallbacks = 0;
+  double berr = 1.0;
+  int it = 0, restarts = 0;
+  const bool use_gmres = (precision == BEM_PREC_BF16_IR);
+  int rc = BEM_OK;
+  for (;;) {
   BEM_CUDA(c, cudaEventRecord(e0, c->stream));
   to_fp32_kernel<<<c->sm_count * 8, 256, 0, c->stream>>>(c->A.p, lda, n, c->A32.p);
   BEM_LAUNCH_CHECK(c);
@@ -136,21 +146,32 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
     if (v >= 128 && v <= 512 && v % 128 == 0) nb = v;
   }
   stamp("enqueued");
-  int rc = lu_factor<float>(c, c->A32.p, lda, n, c->piv.p, c->perm.p, nb, info);
+  c->lu_window = window;
+  rc = lu_factor<float>(c, c->A32.p, lda, n, c->piv.p, c->perm.p, nb, info);
+  c->lu_window = false;
   c->f32_gemm = saved;
   if (rc) return rc;
   stamp("factored");
   BEM_CUDA(c, cudaEventRecord(e1, c->stream));
-  if (*info != 0) return BEM_OK;
+  if (*info != 0) {
+    if (window) {  // a zero pivot inside a window: partial pivoting may still succeed
+      window = false;
+      ++fallbacks;
+      *info = 0;
+      continue;
+    }
+    return BEM_OK;
+  }
   // x0 = LU^{-1} b, then x += LU^{-1} (b - A x)   (plain refinement), or
   // x += GMRES(M^{-1} A, M^{-1} r) with M = the low-precision LU (GMRES-IR)
   BEM_CUDA(c, cudaMemsetAsync(c->X.p, 0, n * sizeof(double), c->stream));
   BEM_CUDA(c, cudaMemcpyAsync(r.p, c->FI.p, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
   double norms[4] = {0, 0, 0, 0};
-  double anorm = -1.0, berr = 1.0, prev = 1e300;
-  int it = 0, restarts = 0;
+  double anorm = -1.0, prev = 1e300;
+  berr = 1.0;
+  it = 0;
+  restarts = 0;
   const bool ir_prof = getenv("BEM_IR_PROFILE") != nullptr;
-  const bool use_gmres = (precision == BEM_PREC_BF16_IR);
   if (!use_gmres) {
     cudaEvent_t q0, q1, q2;
     if (ir_prof) {
@@ -294,6 +315,13 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
   BEM_CUDA(c, cudaEventRecord(e2, c->stream));
   BEM_CUDA(c, cudaEventSynchronize(e2));
   stamp("synchronised");
+  if (window && !(berr <= std::max(rel_tol, 1e-14))) {  // no convergence: partial pivoting
+    window = false;
+    ++fallbacks;
+    continue;
+  }
+  break;
+  }  // attempts
   float f_ms = 0.f, r_ms = 0.f;
   cudaEventElapsedTime(&f_ms, e0, e1);
   cudaEventElapsedTime(&r_ms, e1, e2);
@@ -304,6 +332,8 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
     st->factor_seconds = f_ms * 1e-3;
     st->refine_seconds = r_ms * 1e-3;
     st->gflops = f_ms > 0 ? (2.0 / 3.0) * (double)n * n * n / (f_ms * 1e-3) * 1e-9 : 0.0;
+    st->pivoting = window ? BEM_PIVOT_WINDOW : BEM_PIVOT_PARTIAL;
+    st->fallbacks = fallbacks;
   }
   // Stagnation at the FP64 working-precision floor counts as converged: a requested
   // tolerance below ~1e-14 is met "to working precision".

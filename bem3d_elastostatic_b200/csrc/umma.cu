@@ -15,7 +15,7 @@
 // receives exactly one addition per call, C + (-acc), the same IEEE operation as
 // C - acc: the result is deterministic.
 //
-// Every mbarrier wait is bounded: on timeout the kernel records an error word, the
+// Every mbarrier wait is bounded (the context's wait limit, 2 s by default): on timeout the kernel records an error word, the
 // other roles stop at their next wait, the producer waits (bounded) for its own copies
 // and the MMA warp for its own MMAs, and the tensor memory is freed.
 #include <cuda.h>
@@ -44,7 +44,6 @@ constexpr int kSmem = kStages * STAGE + 1024 + 256 + kStg;
 constexpr unsigned kTmemCols = 512;     // two 128 x 256 FP32 accumulators
 constexpr int kEpiThreads = 256;        // 8 epilogue warps
 constexpr int kThreads = 64 + kEpiThreads;
-constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s bound on every mbarrier wait
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
   return (unsigned)__cvta_generic_to_shared(p);
@@ -57,7 +56,8 @@ __device__ __forceinline__ unsigned long long globaltimer() {
 }
 
 // bounded wait on an mbarrier phase; gives up early when another role aborted
-__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, volatile int* abort_flag) {
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, volatile int* abort_flag,
+                                          unsigned long long wait_ns) {
   const unsigned long long t0 = globaltimer();
   while (true) {
     unsigned done;
@@ -70,7 +70,7 @@ __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, volatil
         : "memory");
     if (done) return true;
     if (abort_flag && *abort_flag) return false;
-    if (globaltimer() - t0 > kWaitNs) return false;
+    if (globaltimer() - t0 > wait_ns) return false;
   }
 }
 
@@ -92,7 +92,8 @@ __device__ __forceinline__ void umma_commit(unsigned bar) {
 __global__ void __launch_bounds__(kThreads, 1)
     umma_update_kernel(const __grid_constant__ CUtensorMap tAh, const __grid_constant__ CUtensorMap tAl,
                        const __grid_constant__ CUtensorMap tBh, const __grid_constant__ CUtensorMap tBl,
-                       const __grid_constant__ CUtensorMap tC, int M, int N, int K, int* err) {
+                       const __grid_constant__ CUtensorMap tC, int M, int N, int K, int* err,
+                       unsigned long long wait_ns) {
   extern __shared__ __align__(16) unsigned char umma_smem[];
   const unsigned raw = smem_u32(umma_smem);
   const unsigned base = (raw + 1023u) & ~1023u;  // 1024-byte aligned operand tiles
@@ -150,7 +151,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         const int m0 = (t % tiles_m) * UM, n0 = (t / tiles_m) * UN;
         const int row[4] = {m0, m0, n0, n0};
         for (int c = 0; c < nchunk; ++c) {
-          if (!mbar_wait(smem_u32(&empty[stage]), phase ^ 1u, abort_flag)) {
+          if (!mbar_wait(smem_u32(&empty[stage]), phase ^ 1u, abort_flag, wait_ns)) {
             fail();
             break;
           }
@@ -175,7 +176,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
       // this CTA's own copies must have landed before its shared memory goes away
       for (int s = 0; s < kStages; ++s)
-        if (last[s] >= 0) mbar_wait(smem_u32(&full[s]), (unsigned)last[s], nullptr);
+        if (last[s] >= 0) mbar_wait(smem_u32(&full[s]), (unsigned)last[s], nullptr, wait_ns);
     }
   } else if (warp == 1) {
     if (lane == 0) {
@@ -185,7 +186,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       int stage = 0, ab = 0;
       unsigned phase = 0, aphase = 0;
       for (int t = blockIdx.x; t < total && !*abort_flag; t += gridDim.x) {
-        if (!mbar_wait(smem_u32(&tempty[ab]), aphase ^ 1u, abort_flag)) {
+        if (!mbar_wait(smem_u32(&tempty[ab]), aphase ^ 1u, abort_flag, wait_ns)) {
           fail();
           break;
         }
@@ -193,7 +194,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         const unsigned d = tmem + (unsigned)(ab * UN);
         bool ok = true;
         for (int c = 0; c < nchunk; ++c) {
-          if (!mbar_wait(smem_u32(&full[stage]), phase, abort_flag)) {
+          if (!mbar_wait(smem_u32(&full[stage]), phase, abort_flag, wait_ns)) {
             ok = false;
             break;
           }
@@ -233,7 +234,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
       }
       umma_commit(smem_u32(drain));
-      mbar_wait(smem_u32(drain), 0, nullptr);
+      mbar_wait(smem_u32(drain), 0, nullptr, wait_ns);
     }
     __syncwarp();
   } else {
@@ -251,7 +252,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     for (int t = blockIdx.x; t < total && !*abort_flag; t += gridDim.x) {
       const int m0 = (t % tiles_m) * UM, n0 = (t / tiles_m) * UN;
       // the four warps of a half leave together (they meet at named barriers below)
-      const int ok = mbar_wait(smem_u32(&tfull[ab]), aphase, abort_flag) ? 1 : 0;
+      const int ok = mbar_wait(smem_u32(&tfull[ab]), aphase, abort_flag, wait_ns) ? 1 : 0;
       int all_ok;
       asm volatile(
           "{\n\t.reg .pred p, q;\n\tsetp.ne.b32 p, %1, 0;\n\t"
@@ -437,7 +438,8 @@ int gemm_umma_bf16x3(bem_ctx* c, int M, int N, int K, const float* A, int64_t ld
       return bem_fail(c, BEM_ERR_CUDA, "umma: tensor map encoding of C failed");
   }
   const int grid = (int)std::min<int64_t>(tiles, c->sm_count);
-  umma_update_kernel<<<grid, kThreads, kSmem, c->stream>>>(mAh, mAl, mBh, mBl, mC, M, N, K, c->umma_err.p);
+  umma_update_kernel<<<grid, kThreads, kSmem, c->stream>>>(mAh, mAl, mBh, mBl, mC, M, N, K, c->umma_err.p,
+                                                           c->wait_ns);
   BEM_LAUNCH_CHECK(c);
   return BEM_OK;
 }

@@ -4,8 +4,9 @@
  * Every entry point takes plain pointers and sizes and returns an int status.  The
  * reference exposes its hot path as Fortran module procedures working on module
  * globals (data_mod.f90:37-52); each function below names the procedure it stands
- * in for.  A Fortran caller binds them with ISO_C_BINDING (INTEGRATION.md shows the
- * interface block); Python binds them with ctypes (bem3d_elastostatic_b200/_lib.py).
+ * in for.  A Fortran caller binds them with ISO_C_BINDING (include/assembly_gpu_mod.f90
+ * holds the interface block); Python binds them with ctypes
+ * (bem3d_elastostatic_b200/_lib.py).
  *
  * Data contract (identical to the reference's globals):
  *   x, y, z       (n) node coordinates
@@ -62,6 +63,15 @@ typedef struct bem_ctx bem_ctx;
 #define BEM_IP_KELVIN_CONSISTENT 1 /* use T*_ij u_j in the displacement identity; clear =
                                       the reference's stress_mod.f90:838-843 form */
 
+/* Pivoting of the low-precision factorisation of the *_IR modes (BEM_OPT_PIVOTING).
+ * BEM_PREC_FP64 always pivots partially (DGESV). */
+#define BEM_PIVOT_WINDOW 1  /* default: the pivot search of each 32-wide sub-panel is
+                               restricted to its 32 x 32 diagonal block (a warp-level
+                               search, no grid-wide exchange per pivot); a zero pivot or a
+                               refinement that does not converge repeats the solve with
+                               partial pivoting */
+#define BEM_PIVOT_PARTIAL 0 /* partial pivoting over every remaining row */
+
 typedef struct {
   int iterations;        /* refinement sweeps (IR) or GMRES iterations */
   int restarts;          /* GMRES restarts */
@@ -69,6 +79,8 @@ typedef struct {
   double factor_seconds; /* device time of the factorisation */
   double refine_seconds; /* device time of the refinement */
   double gflops;         /* 2/3 N^3 / factor_seconds */
+  int pivoting;          /* BEM_PIVOT_* of the factorisation that produced the solution */
+  int fallbacks;         /* window-pivoted attempts repeated with partial pivoting */
 } bem_solve_info;
 
 /* Context ------------------------------------------------------------------------ */
@@ -79,6 +91,23 @@ const char* bem_last_error(const bem_ctx* ctx);
 int bem_sync(bem_ctx* ctx);
 /* the context's CUDA stream (a cudaStream_t), for callers that time or order work */
 int bem_get_stream(bem_ctx* ctx, void** stream);
+
+/* Context options (no counterpart in the reference).
+ *   BEM_OPT_PIVOTING        BEM_PIVOT_WINDOW (default) or BEM_PIVOT_PARTIAL for the
+ *                           factorisations of the *_IR solve modes
+ *   BEM_OPT_WAIT_LIMIT_MS   limit of every bounded device wait of the context's kernels
+ *                           (grid barriers, triangular-sweep publications, tcgen05
+ *                           mbarriers), 1..60000 ms, default 2000; a wait that runs out
+ *                           ends its kernel and the call returns BEM_ERR_TIMEOUT
+ *   BEM_OPT_WITHHOLD_BLOCK  failure injection for tests: the block-inverse triangular
+ *                           sweep of the next solves does not publish this 128-row block
+ *                           (-1, the default, publishes all), so that the waits for it run
+ *                           out and the solve returns BEM_ERR_TIMEOUT with the context
+ *                           still usable */
+#define BEM_OPT_PIVOTING 1
+#define BEM_OPT_WAIT_LIMIT_MS 2
+#define BEM_OPT_WITHHOLD_BLOCK 3
+int bem_set_option(bem_ctx* ctx, int option, int64_t value);
 
 /* Input: replaces input_data (io_mod.f90:36-146) and update_material_constants
  * (data_mod.f90:97-108).  Node -> element adjacency (io_mod.f90:125-135) is built here;
@@ -102,6 +131,20 @@ int bem_get_geometry(bem_ctx* ctx, double* eta1, double* eta2, double* eta3, dou
 /* ghmat8 (assembly_mod.f90:53-223): assembles A and FI on the device (column swap,
  * rigid-body diagonal).  A_out/FI_out (nullable) receive host copies; lda >= 3n. */
 int bem_ghmat8(bem_ctx* ctx, int asm_precision, double* A_out, int64_t lda, double* FI_out);
+
+/* A dense system of any order n (A column-major with leading dimension lda >= n, and
+ * its right-hand side FI), copied to the device in place of an assembled one, for
+ * bem_solve: the reference's solve_linear_system(A_mat, B_vec, n_size)
+ * (solver_mod.f90:17) takes any system.  The phases that need the mesh's system
+ * (bem_reorganize, stresses, adjoint) refuse it (BEM_ERR_STATE). */
+int bem_set_system(bem_ctx* ctx, int n, const double* A, int64_t lda, const double* FI);
+
+/* Rows [r0, r1) of the assembled A (into A_rows, (r1 - r0) x 3n, leading dimension
+ * ld >= r1 - r0) and of FI (FI_rows, nullable), copied from the device: a slice for
+ * parity checks at orders whose A does not fit in host memory.  No counterpart in the
+ * reference.  A must not have been overwritten by a BEM_PREC_FP64 factorisation (the
+ * *_IR modes factor a copy). */
+int bem_get_rows(bem_ctx* ctx, int r0, int r1, double* A_rows, int64_t ld, double* FI_rows);
 
 /* H (3n x 3n, rigid-body diagonal included) and G (3n x 27ne) for collocation nodes
  * [in0, in1) — the two products ghmat8 combines, for entrywise parity checks. */
@@ -128,13 +171,16 @@ int bem_dgesv(bem_ctx* ctx, int n, int nrhs, double* A, int lda, int* ipiv, doub
  * of the solve (a host that owns all device memory through its own pool, a loop that
  * must not pay for cudaMalloc/cudaFree synchronisation, a fixed memory budget).  Its
  * scratch is one static 4.3 MiB device array per GPU, which limits n to 4096
- * (larger n returns BEM_ERR_TOO_LARGE).  dA (n x n, lda) is overwritten by the factors,
- * dB (n x nrhs, ldb) by the solution, d_ipiv (n ints) by the 1-based pivots; *info
- * (host) follows DGESV.  Work is queued on `stream` (a cudaStream_t, 0 = legacy
- * default stream); the call returns after the factorisation's status is known, the
- * solution is complete once the stream has been synchronised.  The first call on a
- * device sets up the array's device address: make it before any stream capture.  All
- * calls share the array: calls that overlap on the GPU race and must be serialised. */
+ * (larger n returns BEM_ERR_TOO_LARGE).  As in bem_dgesv, dA (n x n, lda) is
+ * overwritten by the factors of A^T in A's storage and d_ipiv (n ints) by dgetrf's
+ * 1-based pivot sequence of A^T (pivoting over the rows of A^T: see the header of
+ * lu.cu), so dA/d_ipiv are not dgetrs input for A; dB (n x nrhs, ldb) receives the
+ * solution of A X = B and *info (host) follows DGESV.  d_ipiv is undefined when the
+ * call returns an error before the factorisation completed.  Work is queued on
+ * `stream` (a cudaStream_t, 0 = legacy default stream); the call synchronises that
+ * stream to read the factorisation's status.  The first call on a device sets up the
+ * array's device address: make it before any stream capture.  All calls share the
+ * array: calls that overlap on the GPU race and must be serialised. */
 int bem_dgesv_noalloc(int n, int nrhs, double* dA, int lda, int* d_ipiv, double* dB, int ldb,
                       int* info, void* stream);
 
