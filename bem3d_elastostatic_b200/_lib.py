@@ -87,7 +87,9 @@ class Profile(C.Structure):
                 ("lu_swap_ms", C.c_double), ("lu_panel_update_ms", C.c_double),
                 ("lu_trsm_ms", C.c_double), ("lu_trailing_ms", C.c_double),
                 ("lu_trailing_launches", C.c_longlong), ("lu_trailing_flops", C.c_double),
-                ("lu_trailing_bytes", C.c_double)]
+                ("lu_trailing_bytes", C.c_double), ("ip_points", C.c_longlong),
+                ("ip_near_points", C.c_longlong), ("ip_far_evals", C.c_double),
+                ("ip_near_evals", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -208,6 +208,7 @@ struct bem_ctx {
   int withhold_block = -1;
   int f32_gemm_override = -1;  // BEM_F32_GEMM environment override (0, 1, 3)
   // tcgen05 trailing update: BF16 hi/lo operand copies and its error word
+  bem::DBuf<unsigned long long> ip_counters;  // internal points: far and near evaluations
   bem::DBuf<unsigned char> umma_buf;
   bem::DBuf<int> umma_err;
   // profiling (bem_profile_begin/end)

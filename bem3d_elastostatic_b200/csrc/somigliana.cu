@@ -7,14 +7,18 @@
 // Kernels
 //   far_table / near_table  pre-weighted Gauss-point tables (:580-726), 12 doubles per
 //                           point: x, y, z, n1, n2, n3, u*w (3), t*w (3)
-//   far_kernel              one thread per internal point walking every element; the
-//                           element tables are staged through shared memory in chunks
-//                           and read as broadcasts; near elements are skipped and the
-//                           point is flagged
+//   far_kernel              persistent: each CTA takes tiles of 256 x P internal points
+//                           (P = 4, 2 or 1 points per thread, whichever keeps every SM
+//                           busy) and streams every element's table through a
+//                           double-buffered shared-memory ring (cp.async, 8 elements per
+//                           chunk) that it reads as broadcasts, so each staged table point
+//                           feeds 256 P points; near elements are skipped and the point
+//                           is flagged
 //   near_kernel             one warp per flagged point: its near elements' 1600 points
 //                           split over the lanes, a fixed-order warp reduction, then the
 //                           principal stresses
 //   finish_kernel           principal stresses of the points with no near element
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -229,42 +233,111 @@ __device__ __forceinline__ void somigliana_point(const SomConst& K, const double
   sa[5] += Dzx - Szx;
 }
 
-__global__ void __launch_bounds__(256) far_kernel(int l, const double* cx, const double* cy, const double* cz,
-                                                  int ne, const int* nconec, const double* einfo,
-                                                  const double* far, SomConst K, double* part, int* nearflag) {
-  __shared__ double s_tab[kChunk][kGp * kRec];
-  __shared__ double s_info[kChunk][4];
-  __shared__ int s_npt[kChunk];
-  const int ip = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool active = ip < l;
-  const double xx = active ? cx[ip] : 0.0, yy = active ? cy[ip] : 0.0, zz = active ? cz[ip] : 0.0;
-  double ua[3] = {0, 0, 0}, sa[6] = {0, 0, 0, 0, 0, 0};
-  int has_near = 0;
-  for (int e0 = 0; e0 < ne; e0 += kChunk) {
-    const int ce = min(kChunk, ne - e0);
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < ce * kGp * kRec; idx += blockDim.x) {
-      const int ee = idx / (kGp * kRec), v = idx % (kGp * kRec);
-      s_tab[ee][v] = far[(int64_t)(e0 + ee) * kGp * kRec + v];
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(smem)),
+               "l"(gmem)
+               : "memory");
+}
+
+constexpr int kFarThreads = 256;
+constexpr int kChunkDoubles = kChunk * kGp * kRec;  // one staged chunk of element tables
+constexpr size_t kFarSmem = 2 * (size_t)(kChunkDoubles + kChunk * 4) * sizeof(double);
+
+// Far pass over tiles of kFarThreads * P points (point p of thread t: tile base +
+// p * kFarThreads + t, so every load of a point array is coalesced).  counters[0]
+// accumulates the table points evaluated (far Gauss points x internal points).
+template <int P>
+__global__ void __launch_bounds__(kFarThreads, 1)
+    far_kernel(int l, const double* __restrict__ cx, const double* __restrict__ cy, const double* __restrict__ cz,
+               int ne, const int* __restrict__ nconec, const double* __restrict__ einfo,
+               const double* __restrict__ far, SomConst K, double* part, int* nearflag,
+               unsigned long long* counters) {
+  extern __shared__ __align__(16) double far_smem[];
+  double* s_tab = far_smem;                      // [2][kChunkDoubles]
+  double* s_info = far_smem + 2 * kChunkDoubles;  // [2][kChunk][4]
+  __shared__ int s_npt[2][kChunk];
+  constexpr int T = kFarThreads * P;
+  const int tid = threadIdx.x;
+  const int ntiles = (l + T - 1) / T;
+  const int nchunks = (ne + kChunk - 1) / kChunk;
+  unsigned long long evals = 0;
+  auto stage = [&](int ch, int buf) {  // issue the copies of chunk ch into buffer buf
+    const int e0 = ch * kChunk, ce = min(kChunk, ne - e0);
+    const double* src = far + (int64_t)e0 * kGp * kRec;
+    double* dst = s_tab + buf * kChunkDoubles;
+    for (int i = tid; i < ce * kGp * kRec / 2; i += kFarThreads) cp_async16(dst + 2 * i, src + 2 * i);
+    const double* isrc = einfo + 4 * (int64_t)e0;
+    double* idst = s_info + buf * kChunk * 4;
+    for (int i = tid; i < ce * 2; i += kFarThreads) cp_async16(idst + 2 * i, isrc + 2 * i);
+    if (tid < ce) s_npt[buf][tid] = (nconec[e0 + tid] == 9) ? 36 : 16;
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    double xx[P], yy[P], zz[P], ua[P][3], sa[P][6];
+    bool act[P];
+    int has_near[P];
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      const int ip = tile * T + p * kFarThreads + tid;
+      act[p] = ip < l;
+      xx[p] = act[p] ? cx[ip] : 0.0;
+      yy[p] = act[p] ? cy[ip] : 0.0;
+      zz[p] = act[p] ? cz[ip] : 0.0;
+      has_near[p] = 0;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) ua[p][c] = 0.0;
+#pragma unroll
+      for (int c = 0; c < 6; ++c) sa[p][c] = 0.0;
     }
-    for (int idx = threadIdx.x; idx < ce * 4; idx += blockDim.x) s_info[idx / 4][idx % 4] = einfo[4 * (int64_t)e0 + idx];
-    if (threadIdx.x < ce) s_npt[threadIdx.x] = (nconec[e0 + threadIdx.x] == 9) ? 36 : 16;
-    __syncthreads();
-    if (!active) continue;
-    for (int ee = 0; ee < ce; ++ee) {
-      const double dx = xx - s_info[ee][0], dy = yy - s_info[ee][1], dz = zz - s_info[ee][2];
-      if (dx * dx + dy * dy + dz * dz > s_info[ee][3]) {
-        const int np = s_npt[ee];
-        for (int q = 0; q < np; ++q) somigliana_point(K, &s_tab[ee][q * kRec], xx, yy, zz, ua, sa);
+    __syncthreads();  // the previous tile's last chunk is no longer read
+    stage(0, 0);
+    for (int ch = 0; ch < nchunks; ++ch) {
+      const int buf = ch & 1;
+      if (ch + 1 < nchunks) {
+        stage(ch + 1, buf ^ 1);
+        asm volatile("cp.async.wait_group 1;" ::: "memory");
       } else {
-        has_near = 1;
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
       }
+      __syncthreads();
+      const int ce = min(kChunk, ne - ch * kChunk);
+      const double* tab = s_tab + buf * kChunkDoubles;
+      const double* inf = s_info + buf * kChunk * 4;
+      for (int ee = 0; ee < ce; ++ee) {
+        bool farp[P];
+        bool any = false;
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+          const double dx = xx[p] - inf[4 * ee], dy = yy[p] - inf[4 * ee + 1], dz = zz[p] - inf[4 * ee + 2];
+          farp[p] = act[p] && (dx * dx + dy * dy + dz * dz > inf[4 * ee + 3]);
+          if (act[p] && !farp[p]) has_near[p] = 1;
+          any |= farp[p];
+        }
+        if (!any) continue;
+        const int np = s_npt[buf][ee];
+        const double* Pt = tab + ee * kGp * kRec;
+        for (int q = 0; q < np; ++q) {
+#pragma unroll
+          for (int p = 0; p < P; ++p)
+            if (farp[p]) somigliana_point(K, Pt + q * kRec, xx[p], yy[p], zz[p], ua[p], sa[p]);
+        }
+#pragma unroll
+        for (int p = 0; p < P; ++p) evals += farp[p] ? (unsigned long long)np : 0ull;
+      }
+      __syncthreads();  // buffer buf is refilled by the next iteration's stage
+    }
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      if (!act[p]) continue;
+      const int64_t ip = (int64_t)tile * T + p * kFarThreads + tid;
+      for (int c = 0; c < 3; ++c) part[9 * ip + c] = ua[p][c];
+      for (int c = 0; c < 6; ++c) part[9 * ip + 3 + c] = sa[p][c];
+      nearflag[ip] = has_near[p];
     }
   }
-  if (!active) return;
-  for (int c = 0; c < 3; ++c) part[9 * (int64_t)ip + c] = ua[c];
-  for (int c = 0; c < 6; ++c) part[9 * (int64_t)ip + 3 + c] = sa[c];
-  nearflag[ip] = has_near;
+  // one addition per warp
+  for (int off = 16; off > 0; off >>= 1) evals += __shfl_xor_sync(0xffffffffu, evals, off);
+  if ((tid & 31) == 0 && evals) atomicAdd(counters, evals);
 }
 
 __global__ void near_list_kernel(int l, const int* nearflag, int* list, int* count) {
@@ -275,19 +348,22 @@ __global__ void near_list_kernel(int l, const int* nearflag, int* list, int* cou
 __global__ void __launch_bounds__(128) near_kernel(int nlist, const int* list, const double* cx, const double* cy,
                                                    const double* cz, int ne, const double* einfo, const double* near,
                                                    SomConst K, const double* part, double* u, double* s, double* pr,
-                                                   double* vm) {
+                                                   double* vm, unsigned long long* counters) {
   const int wid = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (wid >= nlist) return;
   const int ip = list[wid];
   const double xx = cx[ip], yy = cy[ip], zz = cz[ip];
   double ua[3] = {0, 0, 0}, sa[6] = {0, 0, 0, 0, 0, 0};
+  unsigned long long evals = 0;
   for (int e = 0; e < ne; ++e) {
     const double dx = xx - einfo[4 * e], dy = yy - einfo[4 * e + 1], dz = zz - einfo[4 * e + 2];
     if (dx * dx + dy * dy + dz * dz > einfo[4 * e + 3]) continue;
     const double* T = near + (int64_t)e * kNear * kRec;
     for (int q = lane; q < kNear; q += 32) somigliana_point(K, T + (int64_t)q * kRec, xx, yy, zz, ua, sa);
+    evals += kNear;
   }
+  if (lane == 0 && evals) atomicAdd(counters + 1, evals);
   for (int off = 16; off > 0; off >>= 1) {
     for (int c = 0; c < 3; ++c) ua[c] += __shfl_xor_sync(0xffffffffu, ua[c], off);
     for (int c = 0; c < 6; ++c) sa[c] += __shfl_xor_sync(0xffffffffu, sa[c], off);
@@ -358,9 +434,32 @@ int launch_internal_points(bem_ctx* c, int l, const double* cx, const double* cy
   K.cD = 1.0 / (8.0 * kPi * (1.0 - nu));
   K.cS = mu / (4.0 * kPi * (1.0 - nu));
   K.asg = (flags & BEM_IP_KELVIN_CONSISTENT) ? -1.0 : 1.0;
-  far_kernel<<<(l + 255) / 256, 256, 0, c->stream>>>(l, cx, cy, cz, ne, c->nconec.p, einfo.p, far.p, K, part.p,
-                                                     flag.p);
-  BEM_LAUNCH_CHECK(c);
+  if (c->ip_counters.count < 2) BEM_CUDA(c, c->ip_counters.alloc(2));
+  BEM_CUDA(c, cudaMemsetAsync(c->ip_counters.p, 0, 2 * sizeof(unsigned long long), c->stream));
+  {
+    static DeviceOnce attr;  // the double-buffered chunk ring is above the 48 KB default
+    if (attr.pending()) {
+      BEM_CUDA(c, cudaFuncSetAttribute(far_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFarSmem));
+      BEM_CUDA(c, cudaFuncSetAttribute(far_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFarSmem));
+      BEM_CUDA(c, cudaFuncSetAttribute(far_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFarSmem));
+      attr.mark();
+    }
+    // the most points per thread that still gives every SM at least four tiles
+    const int grid = c->sm_count;
+    const int P = ((int64_t)l >= 4LL * grid * 4 * kFarThreads) ? 4 : ((int64_t)l >= 4LL * grid * 2 * kFarThreads) ? 2 : 1;
+    const int ntiles = (int)((l + (int64_t)P * kFarThreads - 1) / ((int64_t)P * kFarThreads));
+    const int G = std::min(grid, ntiles);
+    if (P == 4)
+      far_kernel<4><<<G, kFarThreads, kFarSmem, c->stream>>>(l, cx, cy, cz, ne, c->nconec.p, einfo.p, far.p, K,
+                                                             part.p, flag.p, c->ip_counters.p);
+    else if (P == 2)
+      far_kernel<2><<<G, kFarThreads, kFarSmem, c->stream>>>(l, cx, cy, cz, ne, c->nconec.p, einfo.p, far.p, K,
+                                                             part.p, flag.p, c->ip_counters.p);
+    else
+      far_kernel<1><<<G, kFarThreads, kFarSmem, c->stream>>>(l, cx, cy, cz, ne, c->nconec.p, einfo.p, far.p, K,
+                                                             part.p, flag.p, c->ip_counters.p);
+    BEM_LAUNCH_CHECK(c);
+  }
   int* count = flag.p + l;
   BEM_CUDA(c, cudaMemsetAsync(count, 0, sizeof(int), c->stream));
   near_list_kernel<<<(l + 255) / 256, 256, 0, c->stream>>>(l, flag.p, list.p, count);
@@ -370,12 +469,18 @@ int launch_internal_points(bem_ctx* c, int l, const double* cx, const double* cy
   BEM_CUDA(c, cudaStreamSynchronize(c->stream));
   if (nlist > 0) {
     near_kernel<<<(nlist + 3) / 4, 128, 0, c->stream>>>(nlist, list.p, cx, cy, cz, ne, einfo.p, near.p, K, part.p, u,
-                                                        s, pr, vm);
+                                                        s, pr, vm, c->ip_counters.p);
     BEM_LAUNCH_CHECK(c);
   }
   finish_kernel<<<(l + 255) / 256, 256, 0, c->stream>>>(l, flag.p, part.p, u, s, pr, vm);
   BEM_LAUNCH_CHECK(c);
+  unsigned long long cnt[2] = {0, 0};
+  BEM_CUDA(c, cudaMemcpyAsync(cnt, c->ip_counters.p, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream));
   BEM_CUDA(c, cudaStreamSynchronize(c->stream));
+  c->prof.ip_points += l;
+  c->prof.ip_near_points += nlist;
+  c->prof.ip_far_evals += (double)cnt[0];
+  c->prof.ip_near_evals += (double)cnt[1];
   return BEM_OK;
 }
 

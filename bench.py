@@ -1,25 +1,43 @@
 #!/usr/bin/env python
 """Benchmark: assembly + solve of the 73,734-DOF unit cube on one B200.
 
-Workload (BASELINE config "mixed precision"): unit cube [0,1]^3, 32 x 32 quad9
-elements per face (6,144 elements, 24,578 nodes, 73,734 DOF; the FP64 matrix is
+Workload (the mixed-precision benchmark configuration): unit cube [0,1]^3, 32 x 32
+quad9 elements per face (6,144 elements, 24,578 nodes, 73,734 DOF; the FP64 matrix is
 43.5 GB), E = 1, nu = 0.3, u_z = 0 on z = 0 with three pinned DOFs, t_z = 1 on z = 1.
 
 A step is one pass of the hot path on that mesh with the inputs resident in HBM:
 element geometry, ghmat8 assembly of A x = FI (FP64), and the mixed-precision solve
-(FP32 LU whose trailing updates run on the tensor cores as a three-term BF16 split,
-FP64 iterative refinement against the FP64 A).  ``value`` is seconds per solved
-system (lower is better).  The same step with the plain FP64 LU is timed once for
-the "vs plain FP64" comparison, and its solution is the accuracy reference.
+(FP32 LU with window pivoting whose trailing updates run on the tensor cores as a
+three-term BF16 split, FP64 iterative refinement against the FP64 A).  ``value`` is
+seconds per solved system (lower is better).  The same step with the plain FP64 LU is
+timed once for the "vs plain FP64" comparison; its solution is the accuracy reference.
 
-``e2e`` times the same work through the public API from pinned host buffers: mesh,
+``e2e`` times the same work through the public C ABI from pinned host buffers: mesh,
 material, supports and pins copied in, then geometry, assembly, solve, and the
 solution copied back.
 
+Further legs of the default run (config.legs; each untimed by the headline, each
+reporting its own device times; a leg that fails records its error and the line is
+still printed):
+  nu_sweep      the same cube at nu = 0.0 and 0.49: mixed step, plain FP64 step,
+                refinement iterations, relative error against FP64, analytic error
+  somigliana    1,000,000 internal points uniform in [0.05, 0.95]^3 on the nu = 0.3
+                solution: points/s, kernel evaluations/s and FP64 TFLOP/s at ~280 flops
+                per (point, Gauss point)
+  plate         the clamped plate (10 x 10 x 1, 3,840 quad9, 46,086 DOF, E = 210e3):
+                assembly + plain FP64 LU (GFLOP/s) + 200 x 200 x 5 internal points
+  batch         512 boxes of 78..2,598 DOF with 8 load cases each: one assembly, FP32
+                LU + FP64 refinement against plain FP64 LU
+  adjoint       hollow sphere (3,072 quad9, 36,876 DOF): forward solve, adjoint
+                gradient, Lame error, central differences at a few coordinates
+
 ``cpu_baseline`` / ``--impl reference``: the reference's algorithm restated in C++
-(oracle/, OpenMP on every host core) with LAPACK dgesv from scipy's OpenBLAS, on a
-bounded sample: assembly of a slice of collocation rows and dgesv at a reduced
-order, extrapolated linearly in rows and cubically in order (labelled so).
+(oracle/, OpenMP on every host core) with LAPACK dgesv from scipy's OpenBLAS.  Its
+whole pipeline (geometry, assembly, dgesv) is timed on cubes of 8, 12 and 16 elements
+per face edge (4,614 / 10,374 / 18,438 DOF); assembly is fitted as a + b N^2 and
+dgesv as c + d N^3 and both are extrapolated to 73,734 DOF (labelled so).  The GPU
+arm's leg also assembles sampled row blocks of the 73,734-DOF matrix with the oracle
+and checks the GPU's rows against them (config.parity).
 
 Multi-GPU: the dense LU does not shard; --gpus N runs N independent replicas (one
 process per GPU under torchrun) and value = max-over-ranks step time / N.
@@ -33,6 +51,7 @@ import statistics
 import subprocess
 import sys
 import time
+import traceback
 
 import numpy as np
 
@@ -42,6 +61,9 @@ sys.path.insert(0, HERE)
 METRIC = "assembly+solve s at 73.7k DOF: mixed-prec+IR vs plain FP64, rel err<=1e-10"
 WORKLOAD = ("unit cube [0,1]^3, 32x32 quad9 per face: 6,144 elements, 24,578 nodes, "
             "73,734 DOF, E=1, nu=0.3, u_z=0 on z=0 + 3 pins, t_z=1 on z=1")
+FP64_PEAK_NOMINAL = 37.0  # TFLOP/s, B200 FP64 (no FP64 figure is measured on this pool)
+SOMIGLIANA_FLOPS = 280.0  # per (internal point, table point): stress_mod.f90:807-885
+CPU_FIT_SIZES = (8, 12, 16)
 
 
 def measured_peaks():
@@ -135,49 +157,109 @@ def barrier(ws: int):
         dist.barrier()
 
 
-# ------------------------------------------------------------------------------------
-# CPU leg (oracle: the reference's algorithm restated in C++, OpenMP, + OpenBLAS dgesv)
-# ------------------------------------------------------------------------------------
-
-def cpu_sample(mesh, rows: int = 256, n_lu: int = 10240):
-    sys.path.insert(0, os.path.join(HERE, "oracle"))
-    import oracle as O
-    from scipy.linalg import lapack
-
-    orc = O.Oracle(mesh)
-    t0 = time.perf_counter()
-    orc.geometry()
-    orc.ghmat8(0, rows, pins=False)
-    t_asm = time.perf_counter() - t0
-    rng = np.random.default_rng(20261203)
-    A = np.asfortranarray(rng.standard_normal((n_lu, n_lu)))
-    A[np.diag_indices(n_lu)] += n_lu ** 0.5
-    b = rng.standard_normal(n_lu)
-    t0 = time.perf_counter()
-    lapack.dgesv(A, b, overwrite_a=True, overwrite_b=True)
-    t_lu = time.perf_counter() - t0
-    N = mesh.ndof
-    est = t_asm * (mesh.n / rows) + t_lu * (N / n_lu) ** 3
-    sample = (f"assembly of collocation rows 0..{rows} of {mesh.n} (x{mesh.n / rows:.1f}) and "
-              f"dgesv at N={n_lu} (x(N/{n_lu})^3 = {(N / n_lu) ** 3:.0f}); extrapolated")
-    return est, sample, {"assembly_sample_s": t_asm, "dgesv_sample_s": t_lu}
-
-
 def host_cores() -> int:
     return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
 
 
-def run_reference(args, ws, rank):
-    if rank != 0:
-        return 0
+def _leg(name, fn, out: dict):
+    """Run one extra leg; its failure is recorded, never fatal to the bench line."""
+    t0 = time.perf_counter()
+    try:
+        out[name] = fn()
+    except Exception as ex:  # noqa: BLE001 - a leg of the report only
+        out[name] = {"error": f"{type(ex).__name__}: {ex}"[:300],
+                     "trace": traceback.format_exc(limit=3)[-600:]}
+    if isinstance(out[name], dict):
+        out[name]["leg_wall_s"] = time.perf_counter() - t0
+
+
+# ------------------------------------------------------------------------------------
+# CPU leg: the oracle (the reference's algorithm restated in C++, OpenMP, + OpenBLAS)
+# ------------------------------------------------------------------------------------
+
+def _oracle():
+    sys.path.insert(0, os.path.join(HERE, "oracle"))
+    import oracle as O
+
+    return O
+
+
+def cpu_pipeline(m: int):
+    """The reference's pipeline on the m x m-per-face uniaxial cube on the host cores:
+    geometry + ghmat8 (assembly_mod.f90:28-223) and dgesv (solver_mod.f90:28)."""
+    from scipy.linalg import lapack
+
     from bem3d_elastostatic_b200.mesh import uniaxial_cube
 
-    mesh = uniaxial_cube(32, young=1.0, nu=0.3)
-    for _ in range(args.warmup):
-        cpu_sample(mesh, rows=64, n_lu=4096)
-    vals, extra = [], {}
+    O = _oracle()
+    mesh = uniaxial_cube(m, young=1.0, nu=0.3)
+    orc = O.Oracle(mesh)
+    t0 = time.perf_counter()
+    orc.geometry()
+    A, F = orc.ghmat8()
+    t1 = time.perf_counter()
+    _, _, x, info = lapack.dgesv(A, F, overwrite_a=True, overwrite_b=True)
+    t2 = time.perf_counter()
+    if info != 0:
+        raise RuntimeError(f"dgesv info {info}")
+    return mesh.ndof, t1 - t0, t2 - t1
+
+
+def cpu_fit(times: dict, N: int):
+    """Least-squares fits assembly = a + b N^2, dgesv = c + d N^3 over the measured
+    sizes, extrapolated to order N; returns (seconds, details)."""
+    Ns = np.array(sorted(times))
+    ta = np.array([times[n][0] for n in Ns])
+    tl = np.array([times[n][1] for n in Ns])
+    Ma = np.stack([np.ones_like(Ns, dtype=float), Ns.astype(float) ** 2], 1)
+    Ml = np.stack([np.ones_like(Ns, dtype=float), Ns.astype(float) ** 3], 1)
+    ca, *_ = np.linalg.lstsq(Ma, ta, rcond=None)
+    cl, *_ = np.linalg.lstsq(Ml, tl, rcond=None)
+    res_a = (ta - Ma @ ca) / ta
+    res_l = (tl - Ml @ cl) / tl
+    est_a = float(ca[0] + ca[1] * N ** 2)
+    est_l = float(cl[0] + cl[1] * float(N) ** 3)
+    det = {"sizes_dof": [int(n) for n in Ns], "assembly_s": [float(v) for v in ta],
+           "dgesv_s": [float(v) for v in tl], "assembly_fit": [float(v) for v in ca],
+           "dgesv_fit": [float(v) for v in cl],
+           "assembly_fit_rel_residuals": [float(v) for v in res_a],
+           "dgesv_fit_rel_residuals": [float(v) for v in res_l],
+           "extrapolated_assembly_s": est_a, "extrapolated_dgesv_s": est_l}
+    return est_a + est_l, det
+
+
+def cpu_sample_label(N):
+    return (f"oracle pipeline (geometry + ghmat8 + dgesv) timed on cubes of "
+            f"{'/'.join(str(m) for m in CPU_FIT_SIZES)} quad9 per face edge, fitted "
+            f"(assembly a+bN^2, dgesv c+dN^3) and extrapolated to N={N}")
+
+
+def run_reference(args, ws, rank):
+    """--impl reference: the CPU restatement of the reference on the host cores.  Each
+    step times one size of the fit (in rotation) and reports the fit over the latest
+    measurement of every size; the warm-up steps fill the table."""
+    if rank != 0:
+        return 0
+    N = 73734
+    times = {}
+    sizes = list(CPU_FIT_SIZES)
+    k = 0
+    for _ in range(max(args.warmup, len(sizes))):
+        m = sizes[k % len(sizes)]
+        n, ta, tl = cpu_pipeline(m)
+        times[n] = (ta, tl)
+        k += 1
+    vals = []
+    det = {}
+    measured = []
     for _ in range(args.steps):
-        v, sample, extra = cpu_sample(mesh)
+        m = sizes[k % len(sizes)]
+        t0 = time.perf_counter()
+        n, ta, tl = cpu_pipeline(m)
+        measured.append({"m": m, "dof": n, "wall_s": time.perf_counter() - t0})
+        times[n] = (ta, tl)
+        k += 1
+        v, det = cpu_fit(times, N)
         vals.append(v)
     value = float(statistics.median(vals))
     cores = host_cores()
@@ -186,11 +268,11 @@ def run_reference(args, ws, rank):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": value * 1e3, "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "path": "CPU restatement of the reference (oracle/)"},
+        "config": {"workload": WORKLOAD, "path": "CPU restatement of the reference (oracle/)",
+                   "extrapolated": True, "fit": det, "measured_steps": measured},
         "cpu_baseline": {"value": value, "unit": "s", "cores": cores, "kind": "port",
-                         "sample": sample},
+                         "sample": cpu_sample_label(N)},
         "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "extra": extra,
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -199,6 +281,249 @@ def run_reference(args, ws, rank):
 # ------------------------------------------------------------------------------------
 # GPU arm
 # ------------------------------------------------------------------------------------
+
+class Timer:
+    """CUDA events on the library's stream."""
+
+    def __init__(self, stream):
+        import torch
+
+        self.stream = stream
+        self.a = torch.cuda.Event(enable_timing=True)
+        self.b = torch.cuda.Event(enable_timing=True)
+
+    def __enter__(self):
+        self.a.record(self.stream)
+        return self
+
+    def __exit__(self, *exc):
+        self.b.record(self.stream)
+        self.b.synchronize()
+        self.s = self.a.elapsed_time(self.b) / 1e3
+
+
+def leg_nu_sweep(q, mesh, args, stream, x_ref_by_nu):
+    """Mixed step, plain FP64 step and accuracy at the configuration's other nu."""
+    from bem3d_elastostatic_b200 import _lib
+
+    out = {}
+    for nu in (0.0, 0.49):
+        q.ctx.check(q.ctx.L.bem_set_material(q.ctx.h, float(mesh.young / (2 * (1 + nu))), float(nu)),
+                    "set_material")
+        r = {}
+        # first mixed step: the factorisation graph exists for this order already
+        with Timer(stream) as t:
+            q.precompute_element_geometry()
+            q.ghmat8()
+            x = q.solve_linear_system("fp32-ir", tol=args.tol, max_iter=60)
+        r["mixed_s"] = t.s
+        r.update({k: q.solve_info[k] for k in ("iterations", "rel_residual", "pivoting", "fallbacks")})
+        u, _ = q.reorganize_solution()
+        with Timer(stream) as t:
+            q.precompute_element_geometry()
+            q.ghmat8()
+            x64 = q.solve_linear_system("fp64")
+        r["fp64_s"] = t.s
+        r["speedup_vs_fp64"] = r["fp64_s"] / r["mixed_s"]
+        r["rel_err_vs_fp64"] = float(np.abs(x - x64).max() / np.abs(x64).max())
+        P = mesh.node_coords()
+        young = mesh.young
+        ua = np.stack([-nu * P[:, 0], -nu * P[:, 1], P[:, 2]], 1) / young
+        r["u_vs_analytic"] = float(np.abs(u.reshape(-1, 3) - ua).max() / np.abs(ua).max())
+        out[f"nu={nu}"] = r
+    q.ctx.check(q.ctx.L.bem_set_material(q.ctx.h, float(mesh.mu), float(mesh.nu)), "set_material")
+    out["nu=0.3"] = x_ref_by_nu
+    _ = _lib
+    return out
+
+
+def leg_somigliana(q, mesh, stream, npts=1_000_000):
+    """1M internal points uniform in [0.05, 0.95]^3 (seed 20261203) on the current
+    solution, device-resident points and results."""
+    import torch
+
+    from bem3d_elastostatic_b200 import _lib
+    from bem3d_elastostatic_b200.mesh import uniform_points
+
+    q.reorganize_solution()  # u and t of the context's latest (nu = 0.3, mixed) solution
+    pts = uniform_points(npts, 0.05, 0.95, 20261203)
+    dev = torch.device("cuda", q.ctx.device)
+    P = torch.from_numpy(np.ascontiguousarray(pts.T)).to(dev)
+    out = torch.empty((13, npts), dtype=torch.float64, device=dev)
+    u, s, pr, vm = out[0:3], out[3:9], out[9:12], out[12]
+    L, h = q.ctx.L, q.ctx.h
+
+    def call():
+        q.ctx.check(L.bem_internal_points_device(h, npts, P[0].data_ptr(), P[1].data_ptr(), P[2].data_ptr(),
+                                                 u.data_ptr(), s.data_ptr(), pr.data_ptr(), vm.data_ptr(), 0),
+                    "internal_points")
+
+    call()  # warm-up (tables, constants)
+    q.ctx.profile_begin(_lib.BEM_PROF_COUNT)
+    with Timer(stream) as t:
+        call()
+    prof = q.ctx.profile_end()
+    evals = prof["ip_far_evals"] + prof["ip_near_evals"]
+    flops = SOMIGLIANA_FLOPS * evals
+    sig = s.cpu().numpy()
+    # the uniaxial stress state: sigma_zz = 1, all else 0 (discretisation error only)
+    err = float(max(np.abs(sig[2] - 1.0).max(), np.abs(sig[[0, 1, 3, 4, 5]]).max()))
+    return {"points": npts, "seconds": t.s, "points_per_s": npts / t.s,
+            "near_points": prof["ip_near_points"], "far_evals": prof["ip_far_evals"],
+            "near_evals": prof["ip_near_evals"], "evals_per_s": evals / t.s,
+            "fp64_tflops": flops / t.s / 1e12, "fp64_peak_tflops_nominal": FP64_PEAK_NOMINAL,
+            "frac_of_nominal_fp64": flops / t.s / 1e12 / FP64_PEAK_NOMINAL,
+            "flops_per_eval": SOMIGLIANA_FLOPS, "sigma_vs_analytic_max_abs": err}
+
+
+def leg_plate(device, stream_of):
+    """The clamped plate: assembly + plain FP64 LU + 200 x 200 x 5 internal points."""
+    from bem3d_elastostatic_b200.api import Quadesth
+    from bem3d_elastostatic_b200.mesh import clamped_plate, plate_grid_points
+
+    mesh = clamped_plate(points=plate_grid_points())
+    q = Quadesth(mesh, device=device)
+    stream = stream_of(q)
+    try:
+        q.precompute_element_geometry()  # warm-up of geometry and assembly
+        q.ghmat8()
+        with Timer(stream) as ta:
+            q.precompute_element_geometry()
+            q.ghmat8()
+        q.solve_linear_system("fp64")  # warm-up (workspace, graph capture)
+        q.ghmat8()
+        with Timer(stream) as tl:
+            x = q.solve_linear_system("fp64")
+        info = dict(q.solve_info)
+        q.reorganize_solution()
+        with Timer(stream) as ti:
+            _, s, _, _ = q.compute_internal_points()
+        N = mesh.ndof
+        gflops = (2.0 / 3.0) * N ** 3 / info["factor_seconds"] / 1e9
+        return {"workload": f"clamped plate 10x10x1, {mesh.ne} quad9, {N} DOF, E=210e3, nu=0.3",
+                "assembly_s": ta.s, "fp64_solve_s": tl.s, "fp64_factor_s": info["factor_seconds"],
+                "lu_gflops": gflops, "lu_frac_of_nominal_fp64": gflops / 1e3 / FP64_PEAK_NOMINAL,
+                "internal_points": mesh.l, "internal_points_s_host_buffers": ti.s,
+                "assembly_plus_solve_s": ta.s + tl.s, "max_abs_u": float(np.abs(x).max())}
+    finally:
+        q.close()
+
+
+def leg_batch(device):
+    """512 boxes with 8 load cases each: assembly, FP32 LU + FP64 refinement and FP64."""
+    from bem3d_elastostatic_b200.api import Batch
+    from bem3d_elastostatic_b200.mesh import box_batch
+
+    systems = box_batch(512, loads=8)
+    N = np.array([m.ndof for m, _ in systems])
+    b = Batch(device)
+    try:
+        for m, bcs in systems:
+            b.add(m, bcs)
+        b.assemble()
+        t0 = time.perf_counter()
+        b.assemble()
+        t_asm = time.perf_counter() - t0
+        b.solve("fp32-ir", tol=1e-15, max_iter=10)  # warm-up: autotune + graph capture
+        ir = b.solve("fp32-ir", tol=1e-15, max_iter=10)
+        x_ir = [b.solution(i) for i in range(len(systems))]
+        b.solve("fp64")
+        f64 = b.solve("fp64")
+        x64 = [b.solution(i) for i in range(len(systems))]
+        diff = max(float(np.abs(a - c).max() / np.abs(c).max()) for a, c in zip(x_ir, x64))
+        return {"systems": len(systems), "loads": 8, "dof_min": int(N.min()), "dof_max": int(N.max()),
+                "assemble_s_wall": t_asm, "fp32_ir": ir, "fp64": f64,
+                "systems_per_s_fp32_ir": len(systems) / ir["solve_seconds"],
+                "systems_per_s_fp64": len(systems) / f64["solve_seconds"],
+                "speedup_fp32_ir_vs_fp64": f64["solve_seconds"] / ir["solve_seconds"],
+                "rel_diff_ir_vs_fp64": diff}
+    finally:
+        b.close()
+
+
+def leg_adjoint(device, fd_coords=2, m=16):
+    """Hollow sphere: forward (FP64), adjoint gradient of the compliance, Lame, FD."""
+    import torch
+
+    from bem3d_elastostatic_b200.adjoint import BEMSolve, compliance, reorganize
+    from bem3d_elastostatic_b200.api import Quadesth
+    from bem3d_elastostatic_b200.mesh import hollow_sphere, lame_sphere_displacement
+
+    mesh = hollow_sphere(m, nu=0.3)
+    inner = list(range(mesh.ne // 2, mesh.ne))
+    q = Quadesth(mesh, device=device)
+    X0 = np.stack([mesh.x, mesh.y, mesh.z], 1).copy()
+    mu0, nu0 = float(mesh.mu), float(mesh.nu)
+
+    def forward(Xv, mu, nu, grad=False):
+        X = torch.tensor(Xv, dtype=torch.float64, requires_grad=grad)
+        m_ = torch.tensor(mu, dtype=torch.float64, requires_grad=grad)
+        n_ = torch.tensor(nu, dtype=torch.float64, requires_grad=grad)
+        x = BEMSolve.apply(X, m_, n_, q)
+        u, t = reorganize(mesh, x, m_)
+        return compliance(mesh, X, u, t, inner), X, m_, n_, x
+
+    try:
+        forward(X0, mu0, nu0)  # warm-up
+        t0 = time.perf_counter()
+        J, X, mu, nu, x = forward(X0, mu0, nu0, grad=True)
+        t1 = time.perf_counter()
+        J.backward()
+        t2 = time.perf_counter()
+        g = X.grad.numpy().copy()
+        gnu = float(nu.grad)
+        r = np.linalg.norm(X0, axis=1)
+        ur = (x.detach().numpy().reshape(-1, 3) * X0).sum(1) / r
+        exact = lame_sphere_displacement(r, 1.0, 2.0, 1.0, 2 * mu0 * (1 + nu0), nu0)
+        rng = np.random.default_rng(20261203)
+        nodes = np.unique(mesh.kconec[:, inner].ravel() - 1)
+        h = 1e-6
+        errs = []
+        with torch.no_grad():
+            for _ in range(fd_coords):
+                i, d = int(rng.choice(nodes)), int(rng.integers(0, 3))
+                Xp, Xm = X0.copy(), X0.copy()
+                Xp[i, d] += h
+                Xm[i, d] -= h
+                fd = (float(forward(Xp, mu0, nu0)[0]) - float(forward(Xm, mu0, nu0)[0])) / (2 * h)
+                errs.append(abs(fd - g[i, d]) / max(abs(fd), 1e-300))
+            fdn = (float(forward(X0, mu0, nu0 + h)[0]) - float(forward(X0, mu0, nu0 - h)[0])) / (2 * h)
+        return {"workload": f"hollow sphere a=1 b=2, m={m}: {mesh.ne} quad9, {mesh.ndof} DOF",
+                "forward_s_wall": t1 - t0, "backward_s_wall": t2 - t1,
+                "lame_ur_max_rel_err": float(np.abs(ur - exact).max() / np.abs(exact).max()),
+                "fd_coordinates": fd_coords, "fd_rel_err_max": float(max(errs)) if errs else None,
+                "fd_nu_rel_err": abs(fdn - gnu) / abs(fdn)}
+    finally:
+        q.close()
+
+
+def run_case(args):
+    """--case m: one pass of the hot path on the m x m-per-face cube (geometry, ghmat8,
+    the solve, and --case-points uniform internal points), a small self-contained
+    workload for profilers; prints what ran, no timing claims."""
+    from bem3d_elastostatic_b200 import _lib
+    from bem3d_elastostatic_b200.api import Quadesth
+    from bem3d_elastostatic_b200.mesh import uniaxial_cube, uniform_points
+
+    pts = uniform_points(args.case_points, 0.05, 0.95, 20261203) if args.case_points else None
+    mesh = uniaxial_cube(args.case, young=1.0, nu=0.3, points=pts)
+    q = Quadesth(mesh)
+    if args.pivoting == "partial":
+        q.set_option(_lib.BEM_OPT_PIVOTING, _lib.BEM_PIVOT_PARTIAL)
+    q.precompute_element_geometry()
+    q.ghmat8()
+    x = q.solve_linear_system(args.case_precision, tol=1e-15, max_iter=60)
+    out = {"case": f"cube {args.case}x{args.case} per face", "dof": mesh.ndof,
+           "precision": args.case_precision, "solve_info": q.solve_info, "max_x": float(np.abs(x).max())}
+    if args.case_points:
+        q.reorganize_solution()
+        _, s, _, _ = q.compute_internal_points()
+        out["points"] = int(args.case_points)
+        out["sigma_zz_range"] = [float(s[2].min()), float(s[2].max())]
+    print(json.dumps(out), flush=True)
+    q.close()
+    return 0
+
 
 def run_gpu(args, ws, rank, local):
     import torch
@@ -211,6 +536,8 @@ def run_gpu(args, ws, rank, local):
     torch.cuda.set_device(local)
     mesh = uniaxial_cube(32, young=1.0, nu=0.3)
     q = Quadesth(mesh, device=local)
+    if args.pivoting == "partial":
+        q.set_option(_lib.BEM_OPT_PIVOTING, _lib.BEM_PIVOT_PARTIAL)
     stream = torch.cuda.ExternalStream(q.ctx.stream(), device=local)
 
     def step(precision):
@@ -258,6 +585,7 @@ def run_gpu(args, ws, rank, local):
     q.ctx.profile_begin(timing=_lib.BEM_PROF_PHASES)
     step(args.precision)
     phases = q.ctx.profile_end()
+    u_mixed, _ = q.reorganize_solution()
 
     # the assembly alone (geometry + ghmat8, regular and singular pairs), untimed step:
     # regular quad9 pairs at 36 Gauss points x ~470 flops = 16,920 flops each
@@ -265,34 +593,39 @@ def run_gpu(args, ws, rank, local):
     assembly = None
     try:
         q.ctx.sync()
-        a0 = torch.cuda.Event(enable_timing=True)
-        a1 = torch.cuda.Event(enable_timing=True)
-        a0.record(stream)
-        q.precompute_element_geometry()
-        q.ghmat8()
-        a1.record(stream)
-        a1.synchronize()
-        t_asm = a0.elapsed_time(a1) / 1e3
+        with Timer(stream) as ta:
+            q.precompute_element_geometry()
+            q.ghmat8()
+        t_asm = ta.s
         pairs = int(mesh.n) * int(mesh.ne) - int(np.sum(mesh.nconec))
         tflops = pairs * 16920.0 / t_asm / 1e12
         assembly = {"seconds": t_asm, "regular_pairs": pairs, "pairs_per_s": pairs / t_asm,
-                    "fp64_tflops": tflops, "fp64_peak_tflops_nominal": 37.0, "frac": tflops / 37.0}
+                    "fp64_tflops": tflops, "fp64_peak_tflops_nominal": FP64_PEAK_NOMINAL,
+                    "frac": tflops / FP64_PEAK_NOMINAL}
     except Exception as ex:  # a measurement of the report only: never lose the bench line
         assembly = {"error": str(ex)[:200]}
+
+    # rows of the assembled matrix for the CPU leg's parity check (before FP64 factors A)
+    row_blocks = [(0, 96), (mesh.n // 2, mesh.n // 2 + 64), (mesh.n - 64, mesh.n)]
+    gpu_rows = {}
+    try:
+        for b0, b1 in row_blocks:
+            gpu_rows[(b0, b1)] = q.system_rows(b0, b1)
+    except Exception:
+        gpu_rows = {}
 
     # plain FP64 comparison step (also the accuracy reference at this size)
     fp64_s = None
     rel_err = None
     if not args.skip_fp64:
         q.ctx.sync()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        x64 = step("fp64")
-        e1.record(stream)
-        e1.synchronize()
-        fp64_s = allreduce_max(e0.elapsed_time(e1) / 1e3, ws)
+        with Timer(stream) as t64:
+            x64 = step("fp64")
+        fp64_s = allreduce_max(t64.s, ws)
         rel_err = float(np.abs(x_mixed - x64).max() / np.abs(x64).max())
+    P = mesh.node_coords()
+    ua = np.stack([-mesh.nu * P[:, 0], -mesh.nu * P[:, 1], P[:, 2]], 1) / mesh.young
+    u_analytic = float(np.abs(u_mixed.reshape(-1, 3) - ua).max() / np.abs(ua).max())
 
     # end to end through the public API from pinned host memory
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
@@ -327,8 +660,28 @@ def run_gpu(args, ws, rank, local):
     e2e_s = allreduce_max(e0.elapsed_time(e1) / 1e3 / e2e_steps, ws)
     e2e_err = float(np.abs(hsol - x_mixed).max() / np.abs(x_mixed).max())
 
+    legs = {}
+    nu03 = {"mixed_s": t_step, "fp64_s": fp64_s, "speedup_vs_fp64": (fp64_s / t_step) if fp64_s else None,
+            "rel_err_vs_fp64": rel_err, "iterations": infos[-1]["iterations"],
+            "rel_residual": infos[-1]["rel_residual"], "pivoting": infos[-1]["pivoting"],
+            "fallbacks": infos[-1]["fallbacks"], "u_vs_analytic": u_analytic}
+    want = set(args.legs.split(",")) if args.legs else set()
+    if rank == 0 and "somigliana" in want:
+        _leg("somigliana", lambda: leg_somigliana(q, mesh, stream), legs)
+    if "nu_sweep" in want and not args.skip_fp64:
+        _leg("nu_sweep", lambda: leg_nu_sweep(q, mesh, args, stream, nu03), legs)
+    else:
+        legs["nu_sweep"] = {"nu=0.3": nu03}
+    q.close()
+    stream_of = lambda qq: torch.cuda.ExternalStream(qq.ctx.stream(), device=local)
+    if rank == 0 and "plate" in want:
+        _leg("plate", lambda: leg_plate(local, stream_of), legs)
+    if rank == 0 and "batch" in want:
+        _leg("batch", lambda: leg_batch(local), legs)
+    if rank == 0 and "adjoint" in want:
+        _leg("adjoint", lambda: leg_adjoint(local), legs)
+
     if rank != 0:
-        q.close()
         return 0
 
     peaks, src = measured_peaks()
@@ -346,7 +699,7 @@ def run_gpu(args, ws, rank, local):
     roofline = {
         "kernel": ("umma_update_kernel + its BF16 split kernels (LU trailing update: C -= A B, "
                    "tcgen05 BF16x3 into TMEM, TMA-reduce epilogue)" if args.precision == "fp32-ir" else
-                   "sgemm_bf16_kernel<0,1> (LU trailing update, BF16 mma.sync)"),
+                   "umma_update_kernel, one BF16 product (LU trailing update)"),
         "traffic": None,
         "algorithmic_bytes_per_launch": prof["lu_trailing_bytes"] / n_launch,
         "algorithmic_fp32_flops_per_launch": prof["lu_trailing_flops"] / n_launch,
@@ -370,9 +723,33 @@ def run_gpu(args, ws, rank, local):
             roofline["traffic_source"] = "ncu dram__bytes ratio, profiles/trailing_gemm_traffic.json"
 
     cpu = None
+    parity = {"rel_err_vs_fp64": rel_err, "u_vs_analytic": u_analytic}
     if ws == 1 and not args.skip_cpu:
-        v, sample, extra = cpu_sample(mesh)
-        cpu = {"value": v, "unit": "s", "cores": host_cores(), "kind": "port", "sample": sample}
+        try:
+            times = {}
+            for m in CPU_FIT_SIZES:
+                n, ta, tl = cpu_pipeline(m)
+                times[n] = (ta, tl)
+            v, det = cpu_fit(times, mesh.ndof)
+            cpu = {"value": v, "unit": "s", "cores": host_cores(), "kind": "port",
+                   "sample": cpu_sample_label(mesh.ndof), "extrapolated": True, "fit": det}
+            # the oracle as the checker: sampled row blocks of the 73,734-DOF system
+            if gpu_rows:
+                O = _oracle()
+                orc = O.Oracle(mesh)
+                worst_row, worst_fi = 0.0, 0.0
+                t0 = time.perf_counter()
+                for (b0, b1), (A, F) in gpu_rows.items():
+                    Ar, Fr = orc.ghmat8(b0, b1)
+                    rowmax = np.abs(Ar).max(axis=1, keepdims=True)
+                    worst_row = max(worst_row, float((np.abs(A - Ar) / rowmax).max()))
+                    worst_fi = max(worst_fi, float(np.abs(F - Fr).max() / max(np.abs(Fr).max(), 1e-300)))
+                parity.update({"oracle_row_blocks": [list(k) for k in gpu_rows],
+                               "rel_err_vs_oracle_rows": worst_row, "rel_err_vs_oracle_fi": worst_fi,
+                               "oracle_rows_s": time.perf_counter() - t0})
+        except Exception as ex:  # noqa: BLE001
+            cpu = {"value": None, "unit": "s", "cores": host_cores(), "kind": "port",
+                   "sample": "failed: " + str(ex)[:200]}
 
     it = [i["iterations"] for i in infos]
     line = {
@@ -383,17 +760,20 @@ def run_gpu(args, ws, rank, local):
         "data": "synthetic",
         "config": {
             "workload": WORKLOAD, "precision": args.precision,
+            "pivoting": "window (32x32 diagonal block)" if infos[-1]["pivoting"] == 1 else "partial",
             "parallelism": "replicas" if ws > 1 else "single GPU",
             "l2": "inputs larger than L2 (A is 43.5 GB FP64 + 21.7 GB FP32)",
             "fp64_plain_s": fp64_s,
             "speedup_vs_fp64": (fp64_s / t_step) if fp64_s else None,
             "rel_err_vs_fp64": rel_err,
+            "parity": parity,
             "step_ms": step_ms,
             "refine_iterations": it, "backward_error": infos[-1]["rel_residual"],
             "factor_s": infos[-1]["factor_seconds"], "refine_s": infos[-1]["refine_seconds"],
             "assembly_untimed_step": assembly,
             "lu_phase_ms_untimed_step": {k: phases[k] for k in (
                 "lu_panel_ms", "lu_swap_ms", "lu_panel_update_ms", "lu_trsm_ms", "lu_trailing_ms")},
+            "legs": legs,
         },
         "roofline": roofline,
         "cpu_baseline": cpu,
@@ -403,7 +783,6 @@ def run_gpu(args, ws, rank, local):
         "clocks": clk.summary(),
     }
     print(json.dumps(line), flush=True)
-    q.close()
     return 0
 
 
@@ -414,11 +793,20 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--precision", default="fp32-ir", choices=["fp32-ir", "bf16-ir"])
+    ap.add_argument("--pivoting", default="window", choices=["window", "partial"])
     ap.add_argument("--tol", type=float, default=1e-15)
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--legs", default="nu_sweep,somigliana,plate,batch,adjoint",
+                    help="extra legs after the headline (comma list; empty for none)")
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--case", type=int, default=0,
+                    help="profiling case: one pass on the m x m-per-face cube instead of the bench")
+    ap.add_argument("--case-points", type=int, default=0)
+    ap.add_argument("--case-precision", default="fp32-ir", choices=["fp64", "fp32-ir", "bf16-ir"])
     args = ap.parse_args()
+    if args.case:
+        return run_case(args)
     if args.warmup < 3:
         args.warmup = 3
     ws, rank, local = dist_setup(args.gpus)

@@ -276,6 +276,13 @@ typedef struct {
   long long lu_trailing_launches;
   double lu_trailing_flops;
   double lu_trailing_bytes;
+  /* internal points (every bem_internal_points* call while profiling): points, points
+   * with a near element, and the kernel evaluations (point x table point) of the far
+   * (element Gauss points) and near (40 x 40) quadratures */
+  long long ip_points;
+  long long ip_near_points;
+  double ip_far_evals;
+  double ip_near_evals;
 } bem_profile;
 int bem_profile_begin(bem_ctx* ctx, int timing);
 int bem_profile_end(bem_ctx* ctx, bem_profile* out);
