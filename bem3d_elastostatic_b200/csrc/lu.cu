@@ -233,6 +233,8 @@ __global__ void __launch_bounds__(panel_threads<T>(), 1)
 template <typename T>
 __global__ void __launch_bounds__(256) window_panel_kernel(T* S, int64_t lda, int n, int r0, int w, int* piv,
                                                            T* win, int* status) {
+  // n: the end of the columns eliminated here (the whole matrix, or the panel's
+  // diagonal block when the rest of the sub-panel is left to the panel's TRSM)
   __shared__ T D[kPanelW][kPanelW + 1];  // D[c][j] = S(r0 + j, r0 + c)
   __shared__ int s_p[kPanelW];
   const int tid = threadIdx.x, lane = tid & 31;
@@ -363,6 +365,50 @@ __global__ void swap_rows_kernel(T* S, int64_t lda, const int* piv, int k0, int 
   }
 }
 
+// A panel's interchanges (the swaps k0+t <-> piv[k0+t], t = 0..w-1 in order, w <= 512)
+// applied at once to rows [a0,a1) and [b0,b1) of S: they compose into a gather of the
+// panel's columns, x[k0 + c] := x[k0 + perm[c]], and only the columns the gather moves
+// are read and written.  A CTA takes 64 / sizeof(T) rows (32 KB of staged sources for
+// 512 moved columns); every source is read before any destination is written.
+constexpr int kPermMax = 512;
+template <typename T>
+__global__ void __launch_bounds__(256) permute_panel_kernel(T* S, int64_t lda, const int* piv, int k0, int w, int a0,
+                                                            int a1, int b0, int b1) {
+  constexpr int R = 64 / sizeof(T);  // rows per CTA
+  __shared__ int perm[kPermMax];
+  __shared__ int moved[kPermMax];
+  __shared__ int nmoved;
+  __shared__ T buf[kPermMax * R];
+  const int tid = threadIdx.x;
+  for (int c = tid; c < w; c += blockDim.x) perm[c] = c;
+  __syncthreads();
+  if (tid == 0) {
+    for (int t = 0; t < w; ++t) {
+      const int p = piv[k0 + t] - k0;
+      const int x = perm[t];
+      perm[t] = perm[p];
+      perm[p] = x;
+    }
+    int k = 0;
+    for (int c = 0; c < w; ++c)
+      if (perm[c] != c) moved[k++] = c;
+    nmoved = k;
+  }
+  __syncthreads();
+  const int nm = nmoved;
+  if (nm == 0) return;
+  const int na = a1 - a0;
+  const int rr = tid % R, slot = tid / R, nslot = blockDim.x / R;
+  const int64_t i = (int64_t)blockIdx.x * R + rr;
+  const bool ok = i < (int64_t)na + (b1 - b0);
+  const int64_t r = ok ? ((i < na) ? a0 + i : b0 + (i - na)) : 0;
+  for (int q = slot; q < nm; q += nslot)
+    if (ok) buf[q * R + rr] = S[r + (int64_t)(k0 + perm[moved[q]]) * lda];
+  __syncthreads();
+  for (int q = slot; q < nm; q += nslot)
+    if (ok) S[r + (int64_t)(k0 + moved[q]) * lda] = buf[q * R + rr];
+}
+
 // Y := X * U^{-1} in place for rows [r_lo, r_hi), X = S(rows, k0..k0+w), U the unit
 // upper triangle of S(k0..k0+w, k0..k0+w).
 template <typename T>
@@ -460,6 +506,52 @@ __global__ void __launch_bounds__(256) inv_unit_upper_kernel(const T* S11, int64
 // the off-diagonal blocks of one distance from the diagonal computed together (two
 // barriers per distance); V is written to global memory once at the end.
 constexpr int kInvThreads = 512;
+
+// V (zeroed, [128][128] column-major, shared) := U^{-1} for the unit upper triangle whose
+// strict upper part U holds (shared, zero elsewhere), jb <= 128; all threads take part.
+__device__ __forceinline__ void unit_upper_inverse_smem(const float* U, float* V, int jb, float (*tmp)[32 * 33]) {
+  constexpr int B = 32, NB = 128;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int nblk = (jb + B - 1) / B;
+  if (warp < nblk) {
+    const int o = warp * B;
+    float x[B];
+#pragma unroll
+    for (int i = 0; i < B; ++i) x[i] = (i == lane) ? 1.f : 0.f;
+#pragma unroll
+    for (int i = B - 2; i >= 0; --i) {
+      float sacc = x[i];
+#pragma unroll
+      for (int k = i + 1; k < B; ++k) sacc -= U[(o + i) + (o + k) * NB] * x[k];
+      x[i] = (i < lane) ? sacc : x[i];
+    }
+#pragma unroll
+    for (int i = 0; i < B; ++i)
+      if (o + i < jb && o + lane < jb) V[(o + i) + (o + lane) * NB] = x[i];
+  }
+  __syncthreads();
+  for (int d = 1; d < nblk; ++d) {
+    const int nb_d = nblk - d;  // blocks (bi, bi + d)
+    for (int e = tid; e < nb_d * B * B; e += kInvThreads) {
+      const int bi = e / (B * B), r = e % B, cc = (e / B) % B;
+      const int oi = bi * B, oj = (bi + d) * B;
+      float acc = 0.f;
+      for (int k = oi + B; k <= oj + B - 1 && k < jb; ++k) acc += U[(oi + r) + k * NB] * V[k + (oj + cc) * NB];
+      tmp[bi][r + cc * 33] = acc;
+    }
+    __syncthreads();
+    for (int e = tid; e < nb_d * B * B; e += kInvThreads) {
+      const int bi = e / (B * B), r = e % B, cc = (e / B) % B;
+      const int oi = bi * B, oj = (bi + d) * B;
+      float acc = 0.f;
+#pragma unroll 8
+      for (int k = 0; k < B; ++k) acc += V[(oi + r) + (oi + k) * NB] * tmp[bi][k + cc * 33];
+      if (oi + r < jb && oj + cc < jb) V[(oi + r) + (oj + cc) * NB] = -acc;
+    }
+    __syncthreads();
+  }
+}
+
 __global__ void __launch_bounds__(kInvThreads) inv_unit_upper_f32_kernel(const float* S11, int64_t lda, int jb,
                                                                          float* Vout, int ldv) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -512,6 +604,47 @@ __global__ void __launch_bounds__(kInvThreads) inv_unit_upper_f32_kernel(const f
   for (int i = tid; i < jb * jb; i += kInvThreads) {
     const int r = i % jb, cc = i / jb;
     Vout[r + (int64_t)cc * ldv] = V[r + cc * NB];
+  }
+}
+
+// The inverses a window-pivoted panel's TRSMs take, for every 128-block b of the
+// panel's diagonal block (S11 = S(j0.., j0..), jb <= 512): blockIdx.y = 0 writes
+// Vu[b] = the inverse of the unit upper triangle of block b (the multipliers, as
+// inv_unit_upper_f32_kernel), blockIdx.y = 1 writes Wl[b] = the inverse of its lower
+// triangle, diagonal included (U^T of T).  The lower inverse goes through the unit
+// upper routine: W = Lu D with Lu unit lower, so W^{-1} = D^{-1} ((Lu^T)^{-1})^T.
+// Each inverse is 128 x 128 column-major (leading dimension 128, zero outside jb x jb).
+__global__ void __launch_bounds__(kInvThreads) panel_inv_f32_kernel(const float* S11, int64_t lda, int jb,
+                                                                    float* Vu, float* Wl) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int B = 32, NB = 128, NBLK = NB / B;
+  float* U = reinterpret_cast<float*>(smem_raw);
+  float* V = U + NB * NB;
+  __shared__ float tmp[NBLK - 1][B * 33];
+  __shared__ float rdiag[NB];
+  const int b = blockIdx.x, o = b * NB, bb = min(NB, jb - o);
+  const float* D = S11 + o + (int64_t)o * lda;
+  const bool lower = blockIdx.y == 1;
+  if (!lower) {
+    stage_block<float>(U, NB, D, lda, bb, bb, NB, NB, [](int a, int c) { return a < c; });
+  } else {
+    for (int i = threadIdx.x; i < NB; i += kInvThreads) rdiag[i] = (i < bb) ? D[i + (int64_t)i * lda] : 1.f;
+    __syncthreads();
+    // U[a][c] = Lu^T[a][c] = W[c][a] / W[a][a]  (a < c)
+    for (int i = threadIdx.x; i < NB * NB; i += kInvThreads) {
+      const int a = i % NB, c = i / NB;
+      U[i] = (a < c && c < bb) ? D[c + (int64_t)a * lda] / rdiag[a] : 0.f;
+    }
+  }
+  for (int i = threadIdx.x; i < NB * NB; i += kInvThreads) V[i] = 0.f;
+  __syncthreads();
+  unit_upper_inverse_smem(U, V, bb, tmp);
+  float* out = (lower ? Wl : Vu) + (size_t)b * NB * NB;
+  for (int i = threadIdx.x; i < NB * NB; i += kInvThreads) {
+    const int r = i % NB, c = i / NB;
+    float v = 0.f;
+    if (r < bb && c < bb) v = lower ? ((r >= c) ? V[c + r * NB] / rdiag[r] : 0.f) : V[r + c * NB];
+    out[i] = v;
   }
 }
 
@@ -606,8 +739,11 @@ int gemm_bf16(bem_ctx* c, int M, int N, int K, const float* A, int64_t lda, cons
 bool gemm_tc_ok(const void* A, int64_t lda, const void* B, int64_t ldb, int elem);
 bool umma_supported(int K);
 int umma_reserve(bem_ctx* c, int M, int N, int K);
-int gemm_umma_bf16x3(bem_ctx* c, int M, int N, int K, const float* A, int64_t lda, const float* B, int64_t ldb,
-                     float* C, int64_t ldc);
+int gemm_umma_bf16(bem_ctx* c, int M, int N, int K, const float* A, int64_t lda, const float* B, int64_t ldb,
+                   float* C, int64_t ldc, int nprod);
+
+// the FP32 trailing updates of this context run on tcgen05 (umma.cu)
+static bool uses_umma(const bem_ctx* c) { return c->f32_gemm == 4 || c->f32_gemm == 2; }
 
 template <typename T>
 static int gemm_simt(bem_ctx* c, int M, int N, int K, const T* A, int64_t lda, const T* B, int64_t ldb, T* C,
@@ -622,8 +758,9 @@ static int gemm_simt(bem_ctx* c, int M, int N, int K, const T* A, int64_t lda, c
 }
 
 // FP64: DMMA tensor path; FP32: per-context choice (c->f32_gemm) of the BF16 tensor path
-// with 3 (FP32-grade) or 1 (plain BF16) terms, or SIMT FP32.  Misaligned operands take
-// the SIMT kernel.
+// with 3 (FP32-grade) or 1 (plain BF16) terms, or SIMT FP32; the trailing updates (K a
+// multiple of 64, M >= 128, N >= 256) run on tcgen05 with 3 terms (f32_gemm 4) or one
+// (f32_gemm 2, the other GEMMs keeping 3).  Misaligned operands take the SIMT kernel.
 template <typename T>
 int gemm(bem_ctx* c, int M, int N, int K, const T* A, int64_t lda, const T* B, int64_t ldb, T* C, int64_t ldc,
          int mode) {
@@ -634,9 +771,10 @@ int gemm(bem_ctx* c, int M, int N, int K, const T* A, int64_t lda, const T* B, i
     if (tc && c->f64_gemm == 1)
       return gemm_dmma(c, M, N, K, (const double*)A, lda, (const double*)B, ldb, (double*)C, ldc, mode);
   } else {
-    if (c->f32_gemm == 4 && mode == 0 && umma_supported(K) && M >= 128 && N >= 256)
-      return gemm_umma_bf16x3(c, M, N, K, (const float*)A, lda, (const float*)B, ldb, (float*)C, ldc);
-    if (tc && (c->f32_gemm == 1 || c->f32_gemm == 3 || c->f32_gemm == 4))
+    if (uses_umma(c) && mode == 0 && umma_supported(K) && M >= 128 && N >= 256)
+      return gemm_umma_bf16(c, M, N, K, (const float*)A, lda, (const float*)B, ldb, (float*)C, ldc,
+                            c->f32_gemm == 4 ? 3 : 1);
+    if (tc && (c->f32_gemm >= 1 && c->f32_gemm <= 4))
       return gemm_bf16(c, M, N, K, (const float*)A, lda, (const float*)B, ldb, (float*)C, ldc, mode,
                        c->f32_gemm == 1 ? 1 : 3);
   }
@@ -778,11 +916,15 @@ struct LUProfile {
 
 static size_t up256(size_t b) { return (b + 255) / 256 * 256; }
 
+// blocks of the TRSM-inverse region: FP32 factors keep the 2 x 4 inverses of a
+// window-pivoted 512-wide panel (panel_inv_f32_kernel), FP64 one block
+static size_t inv_blocks(int elem) { return elem == 4 ? 8 : 1; }
+
 size_t lu_workspace_bytes(int n, int nb, int gmax, int elem) {
   const size_t ldy = ((size_t)n + 31) / 32 * 32;
   return up256(2 * (size_t)gmax * sizeof(double)) + up256(2 * (size_t)gmax * sizeof(int)) +
          up256(2 * (size_t)gmax * kPanelW * elem) + up256(2 * (size_t)kPanelW * elem) + up256(16) +
-         up256((size_t)kInvBlock * kInvBlock * elem) + up256(ldy * nb * elem);
+         up256(inv_blocks(elem) * kInvBlock * kInvBlock * elem) + up256(ldy * nb * elem);
 }
 
 LUWorkspace lu_workspace_carve(void* base, int n, int nb, int gmax, int elem) {
@@ -802,7 +944,7 @@ LUWorkspace lu_workspace_carve(void* base, int n, int nb, int gmax, int elem) {
   w.status = reinterpret_cast<int*>(p + 8);
   p += up256(16);
   w.inv = p;
-  p += up256((size_t)kInvBlock * kInvBlock * elem);
+  p += up256(inv_blocks(elem) * kInvBlock * kInvBlock * elem);
   w.ybuf = p;
   return w;
 }
@@ -841,7 +983,7 @@ static int lu_factor_enqueue(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int
   // barrier counter (offset 0) and status words (offset 8) of the workspace's sync slot
   BEM_CUDA(c, cudaMemsetAsync(ws.barrier, 0, 16, c->stream));
   unsigned bar_base = 0;
-  if (sizeof(T) == 4 && c->f32_gemm == 4) BEM_CUDA(c, cudaMemsetAsync(c->umma_err.p, 0, sizeof(int), c->stream));
+  if (sizeof(T) == 4 && uses_umma(c)) BEM_CUDA(c, cudaMemsetAsync(c->umma_err.p, 0, sizeof(int), c->stream));
   T* V = reinterpret_cast<T*>(ws.inv);
   T* Y = reinterpret_cast<T*>(ws.ybuf);
   const int64_t ldy = ws.ldy;
@@ -852,15 +994,21 @@ static int lu_factor_enqueue(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int
   cudaFuncSetAttribute(inv_unit_upper_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inv_smem);
   cudaFuncSetAttribute(inv_unit_upper_f32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)(2 * kInvBlock * kInvBlock * sizeof(float)));
+  cudaFuncSetAttribute(panel_inv_f32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)(2 * kInvBlock * kInvBlock * sizeof(float)));
   int rc;
   for (int j0 = 0; j0 < n; j0 += nb) {
     const int jb = std::min(nb, n - j0);
     prof.panel = j0 / nb;
+    // window pivoting leaves the sub-panels' columns right of the panel (T rows below
+    // its diagonal block) to one blocked TRSM per panel; partial pivoting needs them
+    // eliminated sub-panel by sub-panel to search them for pivots
+    const int cend = (window && sizeof(T) == 4) ? j0 + jb : n;
     for (int r0 = j0; r0 < j0 + jb; r0 += kPanelW) {
       const int w = std::min(kPanelW, j0 + jb - r0);
       prof.begin(0, c->stream);
       if (window) {
-        if ((rc = window_panel_launch<T>(c, ws, S, lda, n, r0, w, piv))) return rc;
+        if ((rc = window_panel_launch<T>(c, ws, S, lda, cend, r0, w, piv))) return rc;
       } else if ((rc = panel_launch<T>(c, ws, S, lda, n, r0, w, piv, bar_base))) {
         return rc;
       }
@@ -869,7 +1017,10 @@ static int lu_factor_enqueue(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int
       // swaps on every other row of S: the earlier panels' multipliers (rows [0, r0),
       // so that the factors end up as T = P L U) and the trailing rows; with window
       // pivoting this launch also stores the factored window block
-      const int a0 = 0, a1 = r0, b0 = r0 + w, b1 = n;
+      // (window-pivoted FP32 panels: the panel's own rows here, the other rows once
+      // per panel by permute_panel_kernel)
+      const bool blk = cend < n;
+      const int a0 = blk ? j0 : 0, a1 = r0, b0 = r0 + w, b1 = blk ? j0 + jb : n;
       const int64_t rows = (int64_t)(a1 - a0) + (b1 - b0);
       if (rows > 0 || window) {
         swap_rows_kernel<T><<<(unsigned)std::max<int64_t>(1, (rows + 255) / 256), 256, 0, c->stream>>>(
@@ -883,15 +1034,51 @@ static int lu_factor_enqueue(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int
       if (q1 > q0) {
         trsm_small_kernel<T><<<(q1 - q0 + 127) / 128, 128, 0, c->stream>>>(S, lda, r0, w, q0, q1);
         BEM_LAUNCH_CHECK(c);
-        if ((rc = gemm<T>(c, q1 - q0, n - q0, w, S + q0 + (int64_t)r0 * lda, lda, S + r0 + (int64_t)q0 * lda, lda,
-                          S + q0 + (int64_t)q0 * lda, lda, 0)))
+        if ((rc = gemm<T>(c, q1 - q0, cend - q0, w, S + q0 + (int64_t)r0 * lda, lda, S + r0 + (int64_t)q0 * lda,
+                          lda, S + q0 + (int64_t)q0 * lda, lda, 0)))
           return rc;
       }
       prof.end(c->stream);
     }
     const int t0 = j0 + jb;
+    const bool blocked = cend < n;  // window-pivoted FP32 panel: blocked TRSMs below
+    if (blocked) {
+      prof.begin(1, c->stream);
+      const int64_t rows = (int64_t)j0 + (n - t0);
+      constexpr int R = 64 / (int)sizeof(T);
+      permute_panel_kernel<T><<<(unsigned)((rows + R - 1) / R), 256, 0, c->stream>>>(S, lda, piv, j0, jb, 0, j0, t0, n);
+      BEM_LAUNCH_CHECK(c);
+      prof.end(c->stream);
+    }
     if (t0 < n) {
       const int m = n - t0;
+      T* Vu = V;                                        // [4][128 x 128]
+      T* Wl = V + (size_t)(kInvBlock * kInvBlock) * 4;  // [4][128 x 128]
+      if (blocked) {
+        // the panel's diagonal-block inverses, then the rest of the sub-panels' columns:
+        // B = S(j0..t0, t0..n) := W^{-1} B with W the lower triangle of the diagonal
+        // block (U^T of T), by 128-row blocks: B_b -= W_{b,<b} B_{<b}; B_b = inv(W_bb) B_b
+        prof.begin(2, c->stream);
+        const int nblk = (jb + kInvBlock - 1) / kInvBlock;
+        panel_inv_f32_kernel<<<dim3(nblk, 2), kInvThreads, 2 * kInvBlock * kInvBlock * sizeof(float), c->stream>>>(
+            reinterpret_cast<const float*>(S + j0 + (int64_t)j0 * lda), lda, jb, reinterpret_cast<float*>(Vu),
+            reinterpret_cast<float*>(Wl));
+        BEM_LAUNCH_CHECK(c);
+        for (int b0 = 0; b0 < jb; b0 += kInvBlock) {
+          const int bb = std::min(kInvBlock, jb - b0);
+          T* Bb = S + (j0 + b0) + (int64_t)t0 * lda;
+          if (b0 > 0 && (rc = gemm<T>(c, bb, m, b0, S + (j0 + b0) + (int64_t)j0 * lda, lda, S + j0 + (int64_t)t0 * lda,
+                                      lda, Bb, lda, 0)))
+            return rc;
+          // Z (bb x m, leading dimension 128, in the TRSM buffer) = inv(W_bb) B_b, copied back
+          if ((rc = gemm<T>(c, bb, m, bb, Wl + (size_t)(b0 / kInvBlock) * kInvBlock * kInvBlock, kInvBlock, Bb, lda, Y,
+                            kInvBlock, 1)))
+            return rc;
+          BEM_CUDA(c, cudaMemcpy2DAsync(Bb, lda * sizeof(T), Y, kInvBlock * sizeof(T), bb * sizeof(T), m,
+                                        cudaMemcpyDeviceToDevice, c->stream));
+        }
+        prof.end(c->stream);
+      }
       prof.begin(3, c->stream);
       // TRSM of the block row, Y = X U^{-1} with U the unit upper triangle of the panel's
       // diagonal block, in 128-wide column blocks: X_b -= Y_{<b} U_{<b,b}, Y_b = X_b inv(U_bb)
@@ -901,6 +1088,12 @@ static int lu_factor_enqueue(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int
         if (b0 > 0 &&
             (rc = gemm<T>(c, m, bb, b0, Y, ldy, S + j0 + (int64_t)(j0 + b0) * lda, lda, Xb, lda, 0)))
           return rc;
+        if (blocked) {
+          if ((rc = gemm<T>(c, m, bb, bb, Xb, lda, Vu + (size_t)(b0 / kInvBlock) * kInvBlock * kInvBlock, kInvBlock,
+                            Y + (int64_t)b0 * ldy, ldy, 1)))
+            return rc;
+          continue;
+        }
         if (sizeof(T) == 4)
           inv_unit_upper_f32_kernel<<<1, kInvThreads, 2 * kInvBlock * kInvBlock * sizeof(float), c->stream>>>(
               reinterpret_cast<const float*>(S + (j0 + b0) + (int64_t)(j0 + b0) * lda), lda, bb,
@@ -932,7 +1125,7 @@ static int lu_factor_finish(bem_ctx* c, int n, int* piv, int* perm, int* info, c
   BEM_CUDA(c, cudaMemcpyAsync(st, ws.status, sizeof(st), cudaMemcpyDeviceToHost, c->stream));
   BEM_CUDA(c, cudaStreamSynchronize(c->stream));
   if (st[0] != 0) return bem_fail(c, st[0], "panel grid barrier timed out");
-  if (sizeof(T) == 4 && c->f32_gemm == 4) {
+  if (sizeof(T) == 4 && uses_umma(c)) {
     int ue = 0;
     BEM_CUDA(c, cudaMemcpy(&ue, c->umma_err.p, sizeof(int), cudaMemcpyDeviceToHost));
     if (ue != 0) return bem_fail(c, ue, "tcgen05 trailing update: an mbarrier wait timed out");
@@ -947,7 +1140,7 @@ int lu_factor_ws(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int* perm, int 
                  const LUWorkspace& ws) {
   *info = 0;
   c->dinv_src = nullptr;  // the diagonal-block inverses belong to earlier factors
-  if (sizeof(T) == 4 && c->f32_gemm == 4 && c->umma_err.count < 1) BEM_CUDA(c, c->umma_err.alloc(1));
+  if (sizeof(T) == 4 && uses_umma(c) && c->umma_err.count < 1) BEM_CUDA(c, c->umma_err.alloc(1));
   LUProfile prof = make_profile(c);
   const int rc = lu_factor_enqueue<T>(c, S, lda, n, piv, nb, ws, prof);
   if (rc) return rc;
@@ -970,7 +1163,7 @@ int lu_factor(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int* perm, int nb,
     BEM_CUDA(c, c->lu_scratch[ti].alloc(bytes));
   }
   const LUWorkspace ws = lu_workspace_carve(c->lu_scratch[ti].p, n, nb, gmax, sizeof(T));
-  if (sizeof(T) == 4 && c->f32_gemm == 4) {
+  if (sizeof(T) == 4 && uses_umma(c)) {
     int rc0;
     if (n > nb && (rc0 = umma_reserve(c, n - nb, n - nb, nb))) return rc0;
     if (c->umma_err.count < 1) BEM_CUDA(c, c->umma_err.alloc(1));

@@ -22,6 +22,59 @@ __global__ void to_fp32_kernel(const double* A, int64_t lda, int n, float* A32) 
     A32[i] = (float)A[i];
 }
 
+// Equilibration of the BF16 mode: power-of-two row scales r_i (row maxima of |A| in
+// [1, 2)), then column scales c_j of the row-scaled matrix, so that the factored copy
+// r_i A_ij c_j holds entries of magnitude < 2 whatever the units of the unknowns; the
+// scales are exact, and the preconditioner of the refinement is c (LU)^-1 r.
+__device__ __forceinline__ double pow2_scale(double mx) {
+  if (!(mx > 0.0) || !(mx < INFINITY)) return 1.0;
+  return exp2(-floor(log2(mx)));
+}
+
+// one thread per row, eight columns per step (eight loads in flight per thread)
+__global__ void row_scale_kernel(const double* __restrict__ A, int64_t lda, int n, double* __restrict__ rs) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double mx = 0.0;
+  int j = 0;
+  for (; j + 8 <= n; j += 8) {
+    double v[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) v[u] = fabs(A[i + (int64_t)(j + u) * lda]);
+#pragma unroll
+    for (int u = 0; u < 8; ++u) mx = fmax(mx, v[u]);
+  }
+  for (; j < n; ++j) mx = fmax(mx, fabs(A[i + (int64_t)j * lda]));
+  rs[i] = pow2_scale(mx);
+}
+
+// one warp per column of the row-scaled matrix
+__global__ void col_scale_kernel(const double* __restrict__ A, int64_t lda, int n, const double* __restrict__ rs,
+                                 double* __restrict__ cs) {
+  const int64_t j = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (j >= n) return;
+  double mx = 0.0;
+  for (int i = lane; i < n; i += 32) mx = fmax(mx, fabs(A[i + j * lda] * rs[i]));
+  for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+  if (lane == 0) cs[j] = pow2_scale(mx);
+}
+
+__global__ void to_fp32_scaled_kernel(const double* A, int64_t lda, int n, const double* rs, const double* cs,
+                                      float* A32) {
+  const int64_t total = (int64_t)lda * n;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t j = e / lda;
+    const int i = (int)(e - j * lda);
+    A32[e] = i < n ? (float)(A[e] * rs[i] * cs[j]) : 0.f;
+  }
+}
+
+__global__ void mul_kernel(int n, const double* s, double* x) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) x[i] *= s[i];
+}
+
 __global__ void axpy_kernel(int n, const double* d, double* x) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) x[i] += d[i];
@@ -133,13 +186,40 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
   int rc = BEM_OK;
   for (;;) {
   BEM_CUDA(c, cudaEventRecord(e0, c->stream));
-  to_fp32_kernel<<<c->sm_count * 8, 256, 0, c->stream>>>(c->A.p, lda, n, c->A32.p);
+  const bool scaled = (precision == BEM_PREC_BF16_IR);
+  if (scaled) {
+    BEM_CUDA(c, c->rowscale.alloc(n));
+    BEM_CUDA(c, c->colscale.alloc(n));
+    row_scale_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(c->A.p, lda, n, c->rowscale.p);
+    BEM_LAUNCH_CHECK(c);
+    col_scale_kernel<<<(unsigned)(((int64_t)n * 32 + 255) / 256), 256, 0, c->stream>>>(c->A.p, lda, n, c->rowscale.p,
+                                                                                      c->colscale.p);
+    BEM_LAUNCH_CHECK(c);
+    to_fp32_scaled_kernel<<<c->sm_count * 8, 256, 0, c->stream>>>(c->A.p, lda, n, c->rowscale.p, c->colscale.p,
+                                                                 c->A32.p);
+  } else {
+    to_fp32_kernel<<<c->sm_count * 8, 256, 0, c->stream>>>(c->A.p, lda, n, c->A32.p);
+  }
   BEM_LAUNCH_CHECK(c);
+  // v := M^{-1} v with M the factored copy: c (LU)^{-1} r in the scaled mode
+  auto psolve = [&](double* v) -> int {
+    if (scaled) {
+      mul_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(n, c->rowscale.p, v);
+      BEM_LAUNCH_CHECK(c);
+    }
+    int prc = lu_solve<float>(c, c->A32.p, lda, n, c->perm.p, v);
+    if (prc) return prc;
+    if (scaled) {
+      mul_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(n, c->colscale.p, v);
+      BEM_LAUNCH_CHECK(c);
+    }
+    return BEM_OK;
+  };
   const int saved = c->f32_gemm;
   if (c->f32_gemm_override >= 0)
     c->f32_gemm = c->f32_gemm_override;
   else
-    c->f32_gemm = (precision == BEM_PREC_BF16_IR) ? 1 : 4;
+    c->f32_gemm = (precision == BEM_PREC_BF16_IR) ? 2 : 4;
   int nb = kNbMixed;
   if (const char* e = getenv("BEM_LU_NB")) {  // panel width override: 128, 256, 384 or 512
     const int v = atoi(e);
@@ -182,7 +262,7 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
     for (it = 1; it <= max_iter; ++it) {
       if (ir_prof) cudaEventRecord(q0, c->stream);
       BEM_CUDA(c, cudaMemcpyAsync(d.p, r.p, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-      if ((rc = lu_solve<float>(c, c->A32.p, lda, n, c->perm.p, d.p))) return rc;
+      if ((rc = psolve(d.p))) return rc;
       axpy_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(n, d.p, c->X.p);
       BEM_LAUNCH_CHECK(c);
       if (ir_prof) cudaEventRecord(q1, c->stream);
@@ -246,7 +326,7 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
       prev = berr;
       // v0 = M^{-1} r / beta
       BEM_CUDA(c, cudaMemcpyAsync(V, r.p, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
-      if ((rc = lu_solve<float>(c, c->A32.p, lda, n, c->perm.p, V))) return rc;
+      if ((rc = psolve(V))) return rc;
       double beta = 0.0;
       if ((rc = norm2(V, &beta))) return rc;
       if (!(beta > 0.0)) break;
@@ -259,7 +339,7 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
         double* w = V + (int64_t)(j + 1) * ldv;
         // w = M^{-1} A v_j  (residual_fp64 with b = 0 gives -A v_j)
         if ((rc = residual_fp64(c, c->A.p, lda, n, V + (int64_t)j * ldv, zero.p, w, norms, false))) return rc;
-        if ((rc = lu_solve<float>(c, c->A32.p, lda, n, c->perm.p, w))) return rc;
+        if ((rc = psolve(w))) return rc;
         scale_kernel<<<vb, 256, 0, c->stream>>>(n, -1.0, w, w);
         BEM_LAUNCH_CHECK(c);
         // classical Gram-Schmidt, twice

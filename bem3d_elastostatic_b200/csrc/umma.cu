@@ -89,6 +89,7 @@ __device__ __forceinline__ void umma_commit(unsigned bar) {
 // warps 2-9 drain the other accumulator into C, so the update of C by one tile
 // overlaps the loads and MMAs of the next.  Tiles run m-fastest so a CTA wave shares
 // the B operand band.
+template <int NPROD>
 __global__ void __launch_bounds__(kThreads, 1)
     umma_update_kernel(const __grid_constant__ CUtensorMap tAh, const __grid_constant__ CUtensorMap tAl,
                        const __grid_constant__ CUtensorMap tBh, const __grid_constant__ CUtensorMap tBl,
@@ -157,12 +158,15 @@ __global__ void __launch_bounds__(kThreads, 1)
           }
           const unsigned st = base + stage * STAGE;
           const unsigned bar = smem_u32(&full[stage]);
-          asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"((unsigned)STAGE)
+          // three products need hi and lo of both operands, one product only hi
+          constexpr unsigned kBytes = NPROD == 3 ? (unsigned)STAGE : (unsigned)(A_TILE + B_TILE);
+          asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(kBytes)
                        : "memory");
           const unsigned dst[4] = {st, st + A_TILE, st + 2 * A_TILE, st + 2 * A_TILE + B_TILE};
 #pragma unroll
           for (int q = 0; q < 4; ++q)
-            asm volatile(
+            if (NPROD == 3 || q == 0 || q == 2)
+              asm volatile(
                 "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
                 "[%4];" ::"r"(dst[q]),
                 "l"(reinterpret_cast<uint64_t>(maps[q])), "r"(c * UK), "r"(row[q]), "r"(bar)
@@ -208,7 +212,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             const uint64_t b_h = sw128_desc(bh + off), b_l = sw128_desc(bl + off);
             const uint64_t pa[3] = {a_h, a_h, a_l}, pb[3] = {b_h, b_l, b_h};
 #pragma unroll
-            for (int q = 0; q < 3; ++q) {
+            for (int q = 0; q < NPROD; ++q) {
               const int acc = (c | kk | q) != 0;
               asm volatile(
                   "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
@@ -319,7 +323,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
 }
 
-// A (m x K, FP32, column-major lda) -> hi/lo BF16 [m][K] (K contiguous)
+// A (m x K, FP32, column-major lda) -> hi/lo BF16 [m][K] (K contiguous); lo nullable
 __global__ void split_a_kernel(int m, int K, const float* __restrict__ A, int64_t lda, __nv_bfloat16* hi,
                                __nv_bfloat16* lo) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -334,10 +338,10 @@ __global__ void split_a_kernel(int m, int K, const float* __restrict__ A, int64_
     l[q] = __float2bfloat16_rn(v - __bfloat162float(h[q]));
   }
   *reinterpret_cast<uint4*>(hi + (int64_t)r * K + 8 * g) = *reinterpret_cast<uint4*>(h);
-  *reinterpret_cast<uint4*>(lo + (int64_t)r * K + 8 * g) = *reinterpret_cast<uint4*>(l);
+  if (lo) *reinterpret_cast<uint4*>(lo + (int64_t)r * K + 8 * g) = *reinterpret_cast<uint4*>(l);
 }
 
-// B (K x n, FP32, column-major ldb) -> hi/lo BF16 [n][K]
+// B (K x n, FP32, column-major ldb) -> hi/lo BF16 [n][K]; lo nullable
 __global__ void split_b_kernel(int n, int K, const float* __restrict__ B, int64_t ldb, __nv_bfloat16* hi,
                                __nv_bfloat16* lo) {
   const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -352,7 +356,7 @@ __global__ void split_b_kernel(int n, int K, const float* __restrict__ B, int64_
     l[q] = __float2bfloat16_rn(v - __bfloat162float(h[q]));
   }
   *reinterpret_cast<uint4*>(hi + (int64_t)col * K + 8 * g) = *reinterpret_cast<uint4*>(h);
-  *reinterpret_cast<uint4*>(lo + (int64_t)col * K + 8 * g) = *reinterpret_cast<uint4*>(l);
+  if (lo) *reinterpret_cast<uint4*>(lo + (int64_t)col * K + 8 * g) = *reinterpret_cast<uint4*>(l);
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
@@ -383,9 +387,11 @@ int umma_reserve(bem_ctx* c, int M, int N, int K) {
   return BEM_OK;
 }
 
-// C (M x N) -= A (M x K) * B (K x N) on tcgen05 with the three-term BF16 split.
-int gemm_umma_bf16x3(bem_ctx* c, int M, int N, int K, const float* A, int64_t lda, const float* B, int64_t ldb,
-                     float* C, int64_t ldc) {
+// C (M x N) -= A (M x K) * B (K x N) on tcgen05: nprod = 3, the three-term BF16 split
+// (FP32-grade products); nprod = 1, one BF16 product (hi * hi).
+int gemm_umma_bf16(bem_ctx* c, int M, int N, int K, const float* A, int64_t lda, const float* B, int64_t ldb,
+                   float* C, int64_t ldc, int nprod) {
+  if (nprod != 1 && nprod != 3) return bem_fail(c, BEM_ERR_ARG, "umma: nprod must be 1 or 3");
   if (!umma_supported(K)) return bem_fail(c, BEM_ERR_ARG, "umma: K must be a multiple of 64 up to 512");
   if (!g_encode) {
     cudaDriverEntryPointQueryResult q;
@@ -396,7 +402,8 @@ int gemm_umma_bf16x3(bem_ctx* c, int M, int N, int K, const float* A, int64_t ld
   }
   static DeviceOnce attr;  // the kernel attribute is per device
   if (attr.pending()) {
-    cudaFuncSetAttribute(umma_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem);
+    BEM_CUDA(c, cudaFuncSetAttribute(umma_update_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem));
+    BEM_CUDA(c, cudaFuncSetAttribute(umma_update_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem));
     attr.mark();
   }
   const size_t na = (size_t)M * K, nb_ = (size_t)N * K;
@@ -411,9 +418,9 @@ int gemm_umma_bf16x3(bem_ctx* c, int M, int N, int K, const float* A, int64_t ld
   __nv_bfloat16* bh = al + na;
   __nv_bfloat16* bl = bh + nb_;
   const int64_t ta = (int64_t)M * (K / 8), tb = (int64_t)N * (K / 8);
-  split_a_kernel<<<(unsigned)((ta + 255) / 256), 256, 0, c->stream>>>(M, K, A, lda, ah, al);
+  split_a_kernel<<<(unsigned)((ta + 255) / 256), 256, 0, c->stream>>>(M, K, A, lda, ah, nprod == 3 ? al : nullptr);
   BEM_LAUNCH_CHECK(c);
-  split_b_kernel<<<(unsigned)((tb + 255) / 256), 256, 0, c->stream>>>(N, K, B, ldb, bh, bl);
+  split_b_kernel<<<(unsigned)((tb + 255) / 256), 256, 0, c->stream>>>(N, K, B, ldb, bh, nprod == 3 ? bl : nullptr);
   BEM_LAUNCH_CHECK(c);
   CUtensorMap mAh, mAl, mBh, mBl;
   if (!make_map(&mAh, ah, M, K, UM) || !make_map(&mAl, al, M, K, UM) || !make_map(&mBh, bh, N, K, UN) ||
@@ -438,8 +445,12 @@ int gemm_umma_bf16x3(bem_ctx* c, int M, int N, int K, const float* A, int64_t ld
       return bem_fail(c, BEM_ERR_CUDA, "umma: tensor map encoding of C failed");
   }
   const int grid = (int)std::min<int64_t>(tiles, c->sm_count);
-  umma_update_kernel<<<grid, kThreads, kSmem, c->stream>>>(mAh, mAl, mBh, mBl, mC, M, N, K, c->umma_err.p,
-                                                           c->wait_ns);
+  if (nprod == 3)
+    umma_update_kernel<3><<<grid, kThreads, kSmem, c->stream>>>(mAh, mAl, mBh, mBl, mC, M, N, K, c->umma_err.p,
+                                                                c->wait_ns);
+  else
+    umma_update_kernel<1><<<grid, kThreads, kSmem, c->stream>>>(mAh, mAl, mBh, mBl, mC, M, N, K, c->umma_err.p,
+                                                                c->wait_ns);
   BEM_LAUNCH_CHECK(c);
   return BEM_OK;
 }

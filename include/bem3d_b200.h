@@ -51,9 +51,11 @@ typedef struct bem_ctx bem_ctx;
 #define BEM_PREC_FP32_IR 1   /* FP32 LU whose trailing update runs on the tensor cores as a
                                 three-term BF16 split (FP32-grade products, FP32
                                 accumulation) + FP64 iterative refinement */
-#define BEM_PREC_BF16_IR 2   /* scaled FP32 LU whose trailing update runs on the tensor
-                                cores with BF16 operands and FP32 accumulation,
-                                + FP64 refinement / GMRES-IR */
+#define BEM_PREC_BF16_IR 2   /* LU of an equilibrated FP32 copy (power-of-two row and column
+                                scales) whose trailing updates run on the tcgen05 tensor
+                                cores as one BF16 product with FP32 accumulation (the
+                                panel and TRSM GEMMs keep the three-term split), + GMRES-IR
+                                in FP64 with that LU as preconditioner */
 
 /* Assembly precision modes (bem_ghmat8). */
 #define BEM_ASM_FP64 0  /* every element integral in FP64 (parity with the reference) */
