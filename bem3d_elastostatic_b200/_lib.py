@@ -27,6 +27,7 @@ NOALLOC_MAX_N = 4096
 BEM_PREC_FP64 = 0
 BEM_PREC_FP32_IR = 1
 BEM_PREC_BF16_IR = 2
+BEM_PREC_FP64_IR = 3
 BEM_PROF_COUNT = 0
 BEM_PROF_PHASES = 1
 BEM_PROF_TRAILING = 2
@@ -38,6 +39,7 @@ BEM_PIVOT_WINDOW = 1
 BEM_OPT_PIVOTING = 1
 BEM_OPT_WAIT_LIMIT_MS = 2
 BEM_OPT_WITHHOLD_BLOCK = 3
+BEM_OPT_RESIDUAL = 4
 
 # every symbol the header declares, for the export check
 EXPORTS = [

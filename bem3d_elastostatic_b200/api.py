@@ -24,7 +24,7 @@ from . import _lib
 from .mesh import Mesh
 
 PRECISIONS = {"fp64": _lib.BEM_PREC_FP64, "fp32-ir": _lib.BEM_PREC_FP32_IR,
-              "bf16-ir": _lib.BEM_PREC_BF16_IR}
+              "bf16-ir": _lib.BEM_PREC_BF16_IR, "fp64-ir": _lib.BEM_PREC_FP64_IR}
 ASSEMBLY = {"fp64": _lib.BEM_ASM_FP64, "fp32-far": _lib.BEM_ASM_FP32_FAR}
 
 

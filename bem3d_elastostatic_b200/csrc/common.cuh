@@ -177,7 +177,9 @@ struct bem_ctx {
   bem::DBuf<double> rowscale, colscale;
   // refinement vectors (residual, correction) and timing events, kept: allocation and
   // release next to a 10^10-byte system stalled the host for up to 0.7 s per solve
-  bem::DBuf<double> ir_r, ir_d;
+  bem::DBuf<double> ir_r, ir_d, ir_dmax;
+  bem::DBuf<double> A64f;     // FP64 factor copy of BEM_PREC_FP64_IR
+  bool ext_residual = true;  // BEM_OPT_RESIDUAL: refinement residuals in double-double
   cudaEvent_t solve_ev[3] = {nullptr, nullptr, nullptr};
   // FP64 inverses of the 128 x 128 diagonal blocks of the latest factorisation (for the
   // block-inverse sweeps) and the sweeps' publication slots; dinv_src/n/lda/elem name

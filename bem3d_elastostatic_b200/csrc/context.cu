@@ -159,6 +159,10 @@ int bem_set_option(bem_ctx* c, int option, int64_t value) {
       if (value < 1 || value > 60000) return bem_fail(c, BEM_ERR_ARG, "set_option: wait limit must be 1..60000 ms");
       c->wait_ns = (unsigned long long)value * 1000000ull;
       return BEM_OK;
+    case BEM_OPT_RESIDUAL:
+      if (value != 0 && value != 1) return bem_fail(c, BEM_ERR_ARG, "set_option: residual must be 0 or 1");
+      c->ext_residual = value == 1;
+      return BEM_OK;
     case BEM_OPT_WITHHOLD_BLOCK:
       if (value < -1 || value > INT32_MAX) return bem_fail(c, BEM_ERR_ARG, "set_option: bad block index");
       c->withhold_block = (int)value;
@@ -383,7 +387,7 @@ int bem_solve(bem_ctx* c, int precision, double rel_tol, int max_iter, double* F
     BEM_CUDA(c, cudaMemcpyAsync(c->X.p, c->FI.p, N * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
     rc = bem::lu_solve_fp64(c, c->A.p, c->lda, (int)N, c->X.p);
     if (rc) return rc;
-  } else if (precision == BEM_PREC_FP32_IR || precision == BEM_PREC_BF16_IR) {
+  } else if (precision == BEM_PREC_FP32_IR || precision == BEM_PREC_BF16_IR || precision == BEM_PREC_FP64_IR) {
     rc = bem::solve_mixed(c, precision, rel_tol > 0 ? rel_tol : 1e-12, max_iter > 0 ? max_iter : 50, &st,
                           info);
     if (stats) *stats = st;

@@ -264,29 +264,67 @@ __global__ void __launch_bounds__(256) window_panel_kernel(T* S, int64_t lda, in
     for (int cc = 0; cc < kPanelW; ++cc)  // lane = row: one coalesced segment per column
       D[cc][lane] = (cc < w && lane < w) ? S[r0 + lane + (int64_t)(r0 + cc) * lda] : T(0);
     __syncwarp();
-    for (int t = 0; t < w; ++t) {
-      double bv = (lane >= t && lane < w) ? fabs((double)D[lane][t]) : -1.0;
-      int bc = (lane >= t && lane < w) ? lane : INT_MAX, bg = 0;
-      for (int off = 16; off > 0; off >>= 1) {
-        const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
-        const int oc = __shfl_xor_sync(0xffffffffu, bc, off);
-        better(bv, bc, bg, ov, oc, 0);
+    if (w == kPanelW) {
+      // a full window in registers: lane c holds column c, every loop is unrolled, the
+      // pivot column reaches the other lanes by shuffles (the same operations as below)
+      T col[kPanelW];
+#pragma unroll
+      for (int j = 0; j < kPanelW; ++j) col[j] = D[lane][j];
+#pragma unroll
+      for (int t = 0; t < kPanelW; ++t) {
+        double bv = (lane >= t) ? fabs((double)col[t]) : -1.0;
+        int bc = (lane >= t) ? lane : INT_MAX, bg = 0;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+          const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
+          const int oc = __shfl_xor_sync(0xffffffffu, bc, off);
+          better(bv, bc, bg, ov, oc, 0);
+        }
+        const int p = bc;
+        if (lane == 0) s_p[t] = p;
+        if (p != t) {  // warp-uniform: lanes t and p exchange their columns
+          const int src = (lane == t) ? p : ((lane == p) ? t : lane);
+#pragma unroll
+          for (int j = 0; j < kPanelW; ++j) col[j] = __shfl_sync(0xffffffffu, col[j], src);
+        }
+        const T pv = __shfl_sync(0xffffffffu, col[t], t);
+        if (pv != T(0)) {
+          const T l = col[t] / pv;
+          if (lane > t) col[t] = l;
+#pragma unroll
+          for (int j = t + 1; j < kPanelW; ++j) {
+            const T pj = __shfl_sync(0xffffffffu, col[j], t);
+            if (lane > t) col[j] -= l * pj;
+          }
+        }
       }
-      const int p = bc;
-      if (lane == 0) s_p[t] = p;
-      if (p != t && lane < w) {
-        const T a = D[t][lane];
-        D[t][lane] = D[p][lane];
-        D[p][lane] = a;
+#pragma unroll
+      for (int j = 0; j < kPanelW; ++j) D[lane][j] = col[j];
+    } else {
+      for (int t = 0; t < w; ++t) {
+        double bv = (lane >= t && lane < w) ? fabs((double)D[lane][t]) : -1.0;
+        int bc = (lane >= t && lane < w) ? lane : INT_MAX, bg = 0;
+        for (int off = 16; off > 0; off >>= 1) {
+          const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
+          const int oc = __shfl_xor_sync(0xffffffffu, bc, off);
+          better(bv, bc, bg, ov, oc, 0);
+        }
+        const int p = bc;
+        if (lane == 0) s_p[t] = p;
+        if (p != t && lane < w) {
+          const T a = D[t][lane];
+          D[t][lane] = D[p][lane];
+          D[p][lane] = a;
+        }
+        __syncwarp();
+        const T pv = D[t][t];
+        if (pv != T(0) && lane > t && lane < w) {
+          const T l = D[lane][t] / pv;
+          D[lane][t] = l;
+          for (int j = t + 1; j < w; ++j) D[lane][j] -= l * D[t][j];
+        }
+        __syncwarp();
       }
-      __syncwarp();
-      const T pv = D[t][t];
-      if (pv != T(0) && lane > t && lane < w) {
-        const T l = D[lane][t] / pv;
-        D[lane][t] = l;
-        for (int j = t + 1; j < w; ++j) D[lane][j] -= l * D[t][j];
-      }
-      __syncwarp();
     }
     if (blockIdx.x == 0) {
       if (lane < w) {
@@ -2084,24 +2122,133 @@ __global__ void residual_finish_kernel(int n, int nchunk, const double* part, co
   }
 }
 
+// The same residual with every product and sum carried as a double-double (an FP64
+// value and its rounding error: the product's error by an FMA, the sums' by TwoSum),
+// the residual b - A x rounded to FP64 once at the end.  Its error is ~1e-32 of |A||x|
+// instead of ~n 1e-16, so that refinement can drive x to the solution of the stored
+// FP64 system itself (its forward error no longer grows with the condition number).
+// (explicitly rounded operations: no contraction into an FMA may merge them)
+__device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
+  s = __dadd_rn(a, b);
+  const double bb = __dsub_rn(s, a);
+  e = __dadd_rn(__dsub_rn(a, __dsub_rn(s, bb)), __dsub_rn(b, bb));
+}
+
+__global__ void residual_part_dd_kernel(const double* A, int64_t lda, int n, const double* x, double* part_hi,
+                                        double* part_lo, double* apart, int want_anorm) {
+  __shared__ double xs[kResCols];
+  const int cs = blockIdx.y * kResCols;
+  const int ce = min(n, cs + kResCols);
+  for (int i = threadIdx.x; i < ce - cs; i += blockDim.x) xs[i] = x[cs + i];
+  __syncthreads();
+  const int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  double hi[4] = {0, 0, 0, 0}, lo[4] = {0, 0, 0, 0}, aabs = 0.0;
+  const double* p = A + r + (int64_t)cs * lda;
+  const int cnt = ce - cs;
+  int cc = 0;
+  for (; cc + 8 <= cnt; cc += 8) {
+    double a[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) a[u] = p[(int64_t)(cc + u) * lda];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const double pr = __dmul_rn(a[u], xs[cc + u]);
+      const double pe = fma(a[u], xs[cc + u], -pr);
+      double t, e;
+      two_sum(hi[u & 3], pr, t, e);
+      hi[u & 3] = t;
+      lo[u & 3] += e + pe;
+      if (want_anorm) aabs += fabs(a[u]);
+    }
+  }
+  for (; cc < cnt; ++cc) {
+    const double a = p[(int64_t)cc * lda];
+    const double pr = __dmul_rn(a, xs[cc]);
+    const double pe = fma(a, xs[cc], -pr);
+    double t, e;
+    two_sum(hi[0], pr, t, e);
+    hi[0] = t;
+    lo[0] += e + pe;
+    if (want_anorm) aabs += fabs(a);
+  }
+  double sh = hi[0], sl = lo[0];
+#pragma unroll
+  for (int u = 1; u < 4; ++u) {
+    double t, e;
+    two_sum(sh, hi[u], t, e);
+    sh = t;
+    sl += e + lo[u];
+  }
+  part_hi[(int64_t)blockIdx.y * n + r] = sh;
+  part_lo[(int64_t)blockIdx.y * n + r] = sl;
+  if (want_anorm) apart[(int64_t)blockIdx.y * n + r] = aabs;
+}
+
+__global__ void residual_finish_dd_kernel(int n, int nchunk, const double* part_hi, const double* part_lo,
+                                          const double* apart, const double* b, const double* x, double* r,
+                                          double* norms, int want_anorm) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double rv = 0.0, xv = 0.0, bv = 0.0, av = 0.0;
+  if (i < n) {
+    double sh = 0.0, sl = 0.0, sa = 0.0;
+    for (int k = 0; k < nchunk; ++k) {
+      double t, e;
+      two_sum(sh, part_hi[(int64_t)k * n + i], t, e);
+      sh = t;
+      sl += e + part_lo[(int64_t)k * n + i];
+      if (want_anorm) sa += apart[(int64_t)k * n + i];
+    }
+    double t, e;
+    two_sum(b[i], -sh, t, e);
+    const double ri = t + (e - sl);
+    r[i] = ri;
+    rv = fabs(ri);
+    xv = fabs(x[i]);
+    bv = fabs(b[i]);
+    av = sa;
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    rv = fmax(rv, __shfl_xor_sync(0xffffffffu, rv, off));
+    xv = fmax(xv, __shfl_xor_sync(0xffffffffu, xv, off));
+    bv = fmax(bv, __shfl_xor_sync(0xffffffffu, bv, off));
+    av = fmax(av, __shfl_xor_sync(0xffffffffu, av, off));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomic_max_nonneg(norms + 0, rv);
+    atomic_max_nonneg(norms + 1, xv);
+    atomic_max_nonneg(norms + 2, bv);
+    if (want_anorm) atomic_max_nonneg(norms + 3, av);
+  }
+}
+
 int residual_fp64(bem_ctx* c, const double* A, int64_t lda, int n, const double* x, const double* b, double* r,
-                  double* norms, bool want_anorm) {
+                  double* norms, bool want_anorm, bool extended) {
   const int nchunk = (n + kResCols - 1) / kResCols;
-  const size_t need = (size_t)nchunk * n * (want_anorm ? 2 : 1) + 8;
+  const size_t need = (size_t)nchunk * n * ((want_anorm ? 2 : 1) + (extended ? 1 : 0)) + 8;
   if (c->work.count < need) {
     c->work.release();
     BEM_CUDA(c, c->work.alloc(need));
   }
   double* part = c->work.p + 8;
   double* apart = part + (size_t)nchunk * n;
+  double* part_lo = apart + (want_anorm ? (size_t)nchunk * n : 0);
   double* dn = c->work.p;
   BEM_CUDA(c, cudaMemsetAsync(dn, 0, 4 * sizeof(double), c->stream));
   dim3 grid((n + 255) / 256, nchunk);
-  residual_part_kernel<<<grid, 256, 0, c->stream>>>(A, lda, n, x, part, apart, want_anorm ? 1 : 0);
-  BEM_LAUNCH_CHECK(c);
-  residual_finish_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(n, nchunk, part, apart, b, x, r, dn,
-                                                                  want_anorm ? 1 : 0);
-  BEM_LAUNCH_CHECK(c);
+  if (extended) {
+    residual_part_dd_kernel<<<grid, 256, 0, c->stream>>>(A, lda, n, x, part, part_lo, apart, want_anorm ? 1 : 0);
+    BEM_LAUNCH_CHECK(c);
+    residual_finish_dd_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(n, nchunk, part, part_lo, apart, b, x, r, dn,
+                                                                       want_anorm ? 1 : 0);
+    BEM_LAUNCH_CHECK(c);
+  } else {
+    residual_part_kernel<<<grid, 256, 0, c->stream>>>(A, lda, n, x, part, apart, want_anorm ? 1 : 0);
+    BEM_LAUNCH_CHECK(c);
+    residual_finish_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(n, nchunk, part, apart, b, x, r, dn,
+                                                                    want_anorm ? 1 : 0);
+    BEM_LAUNCH_CHECK(c);
+  }
   BEM_CUDA(c, cudaMemcpyAsync(norms, dn, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   BEM_CUDA(c, cudaStreamSynchronize(c->stream));
   return BEM_OK;

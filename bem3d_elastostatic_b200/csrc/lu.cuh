@@ -61,10 +61,11 @@ int lu_factor(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int* perm, int nb,
 template <typename T>
 int lu_solve(bem_ctx* c, const T* S, int64_t lda, int n, const int* perm, double* b);
 
-// y = b - A x (FP64 A, column-major) and the infinity norms of y; |A| row sums on request
+// y = b - A x (FP64 A, column-major) and the infinity norms of y; |A| row sums on request;
+// extended: products and sums carried as double-doubles (y rounded once)
 int residual_fp64(bem_ctx* c, const double* A, int64_t lda, int n, const double* x, const double* b,
                   double* r, double* norms /* host: [0]=|r|inf [1]=|x|inf [2]=|b|inf [3]=|A|inf */,
-                  bool want_anorm);
+                  bool want_anorm, bool extended = false);
 
 // C (M x N, ldc) op= A (M x K, lda) * B (K x N, ldb), column-major; op: 0 -=, 1 =.
 template <typename T>

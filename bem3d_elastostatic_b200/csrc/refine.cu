@@ -15,6 +15,7 @@ namespace bem {
 // tensor work per tile as C traffic (measured at 73,734 DOF: 1.79 s per bench step at 256,
 // 1.61 s at 384, 1.58 s at 512)
 constexpr int kNbMixed = 512;
+constexpr int kNbFp64IR = 512;  // panel width of the FP64 factors of BEM_PREC_FP64_IR
 
 __global__ void to_fp32_kernel(const double* A, int64_t lda, int n, float* A32) {
   const int64_t total = (int64_t)lda * n;
@@ -78,6 +79,19 @@ __global__ void mul_kernel(int n, const double* s, double* x) {
 __global__ void axpy_kernel(int n, const double* d, double* x) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) x[i] += d[i];
+}
+
+// x += d and dmax = max |d| (non-negative doubles order like their bit patterns)
+__global__ void axpy_max_kernel(int n, const double* d, double* x, double* dmax) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double v = 0.0;
+  if (i < n) {
+    x[i] += d[i];
+    v = fabs(d[i]);
+  }
+  for (int off = 16; off > 0; off >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, off));
+  if ((threadIdx.x & 31) == 0 && v > 0.0)
+    atomicMax(reinterpret_cast<unsigned long long*>(dmax), (unsigned long long)__double_as_longlong(v));
 }
 
 // ---------------------------------------------------------------------------------
@@ -152,11 +166,21 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
       fprintf(stderr, "[solve host] %-14s %9.3f ms\n", what,
               std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - h0).count());
   };
-  if (c->A32.count != (size_t)(lda * n)) {
+  // BEM_PREC_FP64_IR factors an FP64 copy of A (partial pivoting) and refines against A
+  const bool dbl = (precision == BEM_PREC_FP64_IR);
+  if (dbl) {
+    if (c->A64f.count != (size_t)(lda * n)) {
+      c->A64f.release();
+      if (c->A64f.alloc((size_t)(lda * n)) != cudaSuccess)
+        return bem_fail(c, BEM_ERR_OOM, "allocating the FP64 factor copy");
+    }
+  } else if (c->A32.count != (size_t)(lda * n)) {
     c->A32.release();
     cudaError_t e = c->A32.alloc((size_t)(lda * n));
     if (e != cudaSuccess) return bem_fail(c, BEM_ERR_OOM, "allocating the FP32 factor copy");
   }
+  // residuals in double-double (the default) or in FP64
+  const bool ext = c->ext_residual;
   BEM_CUDA(c, c->piv.alloc(n));
   BEM_CUDA(c, c->perm.alloc(n));
   DBuf<double>& r = c->ir_r;
@@ -166,7 +190,7 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
   {
     // one workspace for the triangular solves and the residual, sized once
     const size_t nchunk = ((size_t)n + 511) / 512;
-    const size_t need = std::max(((size_t)n + 127) / 128 * 256 + 256, nchunk * n * 2 + 8);
+    const size_t need = std::max(((size_t)n + 127) / 128 * 256 + 256, nchunk * n * 3 + 8);
     if (c->work.count < need) {
       c->work.release();
       BEM_CUDA(c, c->work.alloc(need));
@@ -178,7 +202,7 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
   // Window pivoting first (pivot search within each 32-wide sub-panel's diagonal
   // block: no grid-wide exchange per pivot); if that factorisation meets a zero pivot or
   // its refinement does not converge, the solve is repeated with partial pivoting.
-  bool window = c->pivot_pref != BEM_PIVOT_PARTIAL;
+  bool window = c->pivot_pref != BEM_PIVOT_PARTIAL && !dbl;
   int fallbacks = 0;
   double berr = 1.0;
   int it = 0, restarts = 0;
@@ -197,6 +221,9 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
     BEM_LAUNCH_CHECK(c);
     to_fp32_scaled_kernel<<<c->sm_count * 8, 256, 0, c->stream>>>(c->A.p, lda, n, c->rowscale.p, c->colscale.p,
                                                                  c->A32.p);
+  } else if (dbl) {
+    BEM_CUDA(c, cudaMemcpyAsync(c->A64f.p, c->A.p, (size_t)lda * n * sizeof(double), cudaMemcpyDeviceToDevice,
+                                c->stream));
   } else {
     to_fp32_kernel<<<c->sm_count * 8, 256, 0, c->stream>>>(c->A.p, lda, n, c->A32.p);
   }
@@ -207,7 +234,8 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
       mul_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(n, c->rowscale.p, v);
       BEM_LAUNCH_CHECK(c);
     }
-    int prc = lu_solve<float>(c, c->A32.p, lda, n, c->perm.p, v);
+    int prc = dbl ? lu_solve<double>(c, c->A64f.p, lda, n, c->perm.p, v)
+                  : lu_solve<float>(c, c->A32.p, lda, n, c->perm.p, v);
     if (prc) return prc;
     if (scaled) {
       mul_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(n, c->colscale.p, v);
@@ -227,7 +255,8 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
   }
   stamp("enqueued");
   c->lu_window = window;
-  rc = lu_factor<float>(c, c->A32.p, lda, n, c->piv.p, c->perm.p, nb, info);
+  rc = dbl ? lu_factor<double>(c, c->A64f.p, lda, n, c->piv.p, c->perm.p, kNbFp64IR, info)
+           : lu_factor<float>(c, c->A32.p, lda, n, c->piv.p, c->perm.p, nb, info);
   c->lu_window = false;
   c->f32_gemm = saved;
   if (rc) return rc;
@@ -247,7 +276,8 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
   BEM_CUDA(c, cudaMemsetAsync(c->X.p, 0, n * sizeof(double), c->stream));
   BEM_CUDA(c, cudaMemcpyAsync(r.p, c->FI.p, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
   double norms[4] = {0, 0, 0, 0};
-  double anorm = -1.0, prev = 1e300;
+  double anorm = -1.0, prev = 1e300, prev_d = 1e300;
+  if (c->ir_dmax.count < 1) BEM_CUDA(c, c->ir_dmax.alloc(1));
   berr = 1.0;
   it = 0;
   restarts = 0;
@@ -263,10 +293,13 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
       if (ir_prof) cudaEventRecord(q0, c->stream);
       BEM_CUDA(c, cudaMemcpyAsync(d.p, r.p, n * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
       if ((rc = psolve(d.p))) return rc;
-      axpy_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(n, d.p, c->X.p);
+      BEM_CUDA(c, cudaMemsetAsync(c->ir_dmax.p, 0, sizeof(double), c->stream));
+      axpy_max_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(n, d.p, c->X.p, c->ir_dmax.p);
       BEM_LAUNCH_CHECK(c);
       if (ir_prof) cudaEventRecord(q1, c->stream);
-      if ((rc = residual_fp64(c, c->A.p, lda, n, c->X.p, c->FI.p, r.p, norms, anorm < 0))) return rc;
+      double dmax = 0.0;
+      BEM_CUDA(c, cudaMemcpyAsync(&dmax, c->ir_dmax.p, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+      if ((rc = residual_fp64(c, c->A.p, lda, n, c->X.p, c->FI.p, r.p, norms, anorm < 0, ext))) return rc;
       if (ir_prof) {
         cudaEventRecord(q2, c->stream);
         cudaEventSynchronize(q2);
@@ -278,8 +311,20 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
       if (anorm < 0) anorm = norms[3];
       berr = norms[0] / (anorm * norms[1] + norms[2]);
       if (!(berr == berr)) break;  // NaN: diverged
-      if (berr <= rel_tol) break;
-      if (berr > 0.5 * prev && it > 3) break;  // stagnation
+      if (!ext) {
+        if (berr <= rel_tol) break;
+        if (berr > 0.5 * prev && it > 3) break;  // stagnation
+      } else {
+        // with exact residuals the iterates approach the solution of the stored system
+        // itself: stop once the backward error meets the tolerance and the last
+        // correction is below it relative to x (at the default tolerances: below 4 units
+        // of roundoff of x), or the corrections stop shrinking (they then only carry
+        // x's rounding)
+        const double u = 1.1102230246251565e-16;
+        if (berr <= rel_tol && dmax <= std::max(4.0 * u, rel_tol) * norms[1]) break;
+        if (it > 3 && dmax > 0.5 * prev_d && berr > 0.5 * prev) break;
+        prev_d = dmax;
+      }
       prev = berr;
     }
   } else {
@@ -318,7 +363,7 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
     };
     const double inner_tol = 1e-6;
     for (restarts = 0; restarts < max_iter; ++restarts) {
-      if ((rc = residual_fp64(c, c->A.p, lda, n, c->X.p, c->FI.p, r.p, norms, anorm < 0))) return rc;
+      if ((rc = residual_fp64(c, c->A.p, lda, n, c->X.p, c->FI.p, r.p, norms, anorm < 0, ext))) return rc;
       if (anorm < 0) anorm = norms[3];
       berr = norms[0] / (anorm * norms[1] + norms[2]);
       if (!(berr == berr) || berr <= rel_tol) break;

@@ -57,6 +57,11 @@ typedef struct bem_ctx bem_ctx;
                                 panel and TRSM GEMMs keep the three-term split), + GMRES-IR
                                 in FP64 with that LU as preconditioner */
 
+#define BEM_PREC_FP64_IR 3   /* FP64 LU (partial pivoting) of a copy of A, + refinement with
+                                extended-precision residuals: the solution of the stored
+                                FP64 system to FP64 rounding, whatever its conditioning
+                                (LAPACK's extra-precise refinement, xGERFSX, in kind) */
+
 /* Assembly precision modes (bem_ghmat8). */
 #define BEM_ASM_FP64 0  /* every element integral in FP64 (parity with the reference) */
 #define BEM_ASM_FP32_FAR 1 /* far-field integrals in FP32, near-singular and singular in FP64 */
@@ -101,6 +106,13 @@ int bem_get_stream(bem_ctx* ctx, void** stream);
  *                           (grid barriers, triangular-sweep publications, tcgen05
  *                           mbarriers), 1..60000 ms, default 2000; a wait that runs out
  *                           ends its kernel and the call returns BEM_ERR_TIMEOUT
+ *   BEM_OPT_RESIDUAL        1 (default): the refinement of the *_IR modes computes its
+ *                           residuals b - A x in double-double (exact products, TwoSum
+ *                           accumulation, one rounding) and iterates until the backward
+ *                           error meets rel_tol and the last correction is below
+ *                           max(rel_tol, 4 u) relative to x (u the unit roundoff), so at
+ *                           the default tolerances the solution carries FP64 rounding
+ *                           only; 0: FP64 residuals, stopping on the backward error
  *   BEM_OPT_WITHHOLD_BLOCK  failure injection for tests: the block-inverse triangular
  *                           sweep of the next solves does not publish this 128-row block
  *                           (-1, the default, publishes all), so that the waits for it run
@@ -109,6 +121,7 @@ int bem_get_stream(bem_ctx* ctx, void** stream);
 #define BEM_OPT_PIVOTING 1
 #define BEM_OPT_WAIT_LIMIT_MS 2
 #define BEM_OPT_WITHHOLD_BLOCK 3
+#define BEM_OPT_RESIDUAL 4
 int bem_set_option(bem_ctx* ctx, int option, int64_t value);
 
 /* Input: replaces input_data (io_mod.f90:36-146) and update_material_constants
