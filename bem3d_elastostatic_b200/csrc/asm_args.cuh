@@ -21,7 +21,6 @@ struct AsmArgs {
   const double* y;
   const double* z;
   const double* tab;
-  const double* tabw;  // per element and Gauss point: sum_k p12, sum_k p12 bc(k, 0..2) (nullable)
   Material mat;
   double* A;  // mode A: (3n, 3n); mode HG: H
   int64_t lda;

@@ -242,171 +242,6 @@ __device__ __forceinline__ void regular_pair(const AsmArgs& P, int e, const doub
     for (int jj = 0; jj < 3; ++jj) fi_acc[jj] += fi[jj];
 }
 
-// The column swap (assembly_mod.f90:125-218) needs, for each displacement component ld
-// of an element, the 3 x NC block of only one kernel in full: G where u is prescribed
-// (it goes to A, times -mu), H where t is prescribed (A, or FI where a neighbour
-// prescribes u); the other kernel enters only through its sum over the element's nodes
-// weighted by the prescribed values, and the rigid-body diagonal only through H summed
-// with unit weights.  regular_pair_ld therefore integrates one component at a time
-// with 27 + 6 accumulators (against 54 + 81 for both full blocks), and takes the two
-// node sums per Gauss point from the element's tabw entry:
-//   tabw[4q] = sum_k p12[q][k],  tabw[4q + 1 + ld] = sum_k p12[q][k] bc(3k + ld).
-// U* and T* at each point are formed exactly as in regular_pair; only the order in
-// which the weighted sums are added differs.
-constexpr int kTabW = 4 * kGp;  // doubles of tabw per element
-
-__global__ void tabw_kernel(int ne, const int* __restrict__ nconec, const double* __restrict__ bc,
-                            const double* __restrict__ tab, double* __restrict__ tabw) {
-  const int64_t gid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (gid >= (int64_t)ne * kGp) return;
-  const int e = (int)(gid / kGp), q = (int)(gid % kGp);
-  const int nc = nconec[e];
-  const double* W = tab + (int64_t)e * kTabStride + kTabGeo + 9 * q;
-  double ws = 0.0, wb[3] = {0.0, 0.0, 0.0};
-  for (int k = 0; k < nc; ++k) {
-    ws += W[k];
-    for (int ld = 0; ld < 3; ++ld) wb[ld] = fma(W[k], bc[3 * k + ld + 27 * (int64_t)e], wb[ld]);
-  }
-  double* o = tabw + gid * 4;
-  o[0] = ws;
-  o[1] = wb[0];
-  o[2] = wb[1];
-  o[3] = wb[2];
-}
-
-template <int NC, bool UP, typename R>
-__device__ __forceinline__ void pair_component(const AsmArgs& P, const double* T, const double* TW, double xi0,
-                                               double xi1, double xi2, int ld, R (&full)[NC][3], R (&wsum)[3],
-                                               R (&rsum)[3]) {
-  constexpr int NG = (NC == 9) ? 36 : 16;
-  const R rc3 = (R)P.mat.c3, rc4 = (R)P.mat.c4, rc5 = (R)P.mat.c5, rc6 = (R)P.mat.c6;
-#pragma unroll
-  for (int k = 0; k < NC; ++k)
-#pragma unroll
-    for (int jj = 0; jj < 3; ++jj) full[k][jj] = R(0);
-#pragma unroll
-  for (int jj = 0; jj < 3; ++jj) wsum[jj] = rsum[jj] = R(0);
-#pragma unroll 1
-  for (int q = 0; q < NG; ++q) {
-    const R r0 = (R)(T[6 * q + 0] - xi0);
-    const R r1 = (R)(T[6 * q + 1] - xi1);
-    const R r2 = (R)(T[6 * q + 2] - xi2);
-    const R n[3] = {(R)T[6 * q + 3], (R)T[6 * q + 4], (R)T[6 * q + 5]};
-    const R ri = rsqrt(r0 * r0 + r1 * r1 + r2 * r2);
-    const R a[3] = {r0 * ri, r1 * ri, r2 * ri};
-    const R al = ld == 0 ? a[0] : (ld == 1 ? a[1] : a[2]);
-    const R nl = ld == 0 ? n[0] : (ld == 1 ? n[1] : n[2]);
-    const R c3r = rc3 * ri;
-    const R rdn = a[0] * n[0] + a[1] * n[1] + a[2] * n[2];
-    const R c5r2 = rc5 * ri * ri;
-    R u[3], t[3];
-#pragma unroll
-    for (int jj = 0; jj < 3; ++jj) {
-      // U*(jj, ld) and T*(jj, ld) as regular_pair forms them (assembly_mod.f90:618-650)
-      u[jj] = (jj == ld) ? (rc4 + a[jj] * al) * c3r : a[jj] * al * c3r;
-      const R d = (jj == ld) ? rc6 : R(0);
-      t[jj] = c5r2 * (rdn * (d + R(3) * al * a[jj]) + rc6 * (n[jj] * al - nl * a[jj]));
-    }
-    const double* W = T + kTabGeo + 9 * q;
-    const R ws = (R)TW[4 * q], wb = (R)TW[4 * q + 1 + ld];
-#pragma unroll
-    for (int k = 0; k < NC; ++k) {
-      const R w = (R)W[k];
-#pragma unroll
-      for (int jj = 0; jj < 3; ++jj) full[k][jj] = fma(UP ? u[jj] : t[jj], w, full[k][jj]);
-    }
-#pragma unroll
-    for (int jj = 0; jj < 3; ++jj) {
-      wsum[jj] = fma(UP ? t[jj] : u[jj], wb, wsum[jj]);
-      rsum[jj] = fma(t[jj], ws, rsum[jj]);
-    }
-  }
-}
-
-template <int NC, typename R>
-__device__ __forceinline__ void regular_pair_ld(const AsmArgs& P, int e, const double* T, const double* TW,
-                                                const int* kc, double xi0, double xi1, double xi2, int64_t row,
-                                                double* fi_acc, double* d1) {
-  const double mu = P.mat.mu;
-  double fi[3] = {0.0, 0.0, 0.0};
-#pragma unroll 1
-  for (int ld = 0; ld < 3; ++ld) {
-    R full[NC][3], wsum[3], rsum[3];
-    const bool up = __ldg(P.kode + 3 * e + ld) == 0;
-    if (up)
-      pair_component<NC, true, R>(P, T, TW, xi0, xi1, xi2, ld, full, wsum, rsum);
-    else
-      pair_component<NC, false, R>(P, T, TW, xi0, xi1, xi2, ld, full, wsum, rsum);
-#pragma unroll
-    for (int jj = 0; jj < 3; ++jj) d1[jj + 3 * ld] -= (double)rsum[jj];
-    if (up) {
-      // A(:, col) -= mu g (assembly_mod.f90:131-133), FI -= h u-bar
-#pragma unroll
-      for (int jj = 0; jj < 3; ++jj) fi[jj] -= (double)wsum[jj];
-      constexpr int G1 = (NC + 2) / 3;
-#pragma unroll
-      for (int k0 = 0; k0 < NC; k0 += G1) {
-        double old[G1][3];
-#pragma unroll
-        for (int kk = 0; kk < G1; ++kk)
-          if (k0 + kk < NC) {
-            const double* col = P.A + (3 * (int64_t)kc[k0 + kk] + ld) * P.lda + row;
-#pragma unroll
-            for (int jj = 0; jj < 3; ++jj) old[kk][jj] = col[jj];
-          }
-#pragma unroll
-        for (int kk = 0; kk < G1; ++kk)
-          if (k0 + kk < NC) {
-            double* col = P.A + (3 * (int64_t)kc[k0 + kk] + ld) * P.lda + row;
-#pragma unroll
-            for (int jj = 0; jj < 3; ++jj) col[jj] = old[kk][jj] - (double)full[k0 + kk][jj] * mu;
-          }
-      }
-    } else {
-      // FI += g t-bar; A(:, col) += h, or FI -= h vp where a neighbour prescribes u
-#pragma unroll
-      for (int jj = 0; jj < 3; ++jj) fi[jj] += (double)wsum[jj];
-      constexpr int H1 = (NC + 2) / 3;
-#pragma unroll
-      for (int k0 = 0; k0 < NC; k0 += H1) {
-        double old[H1][3];
-        bool uk[H1];
-#pragma unroll
-        for (int kk = 0; kk < H1; ++kk) {
-          const int k = k0 + kk;
-          if (k < NC) {
-            const int64_t dof = 3 * (int64_t)kc[k] + ld;
-            uk[kk] = __ldg(P.uknown + dof) != 0;
-            if (!uk[kk]) {
-              const double* col = P.A + dof * P.lda + row;
-#pragma unroll
-              for (int jj = 0; jj < 3; ++jj) old[kk][jj] = col[jj];
-            }
-          }
-        }
-#pragma unroll
-        for (int kk = 0; kk < H1; ++kk) {
-          const int k = k0 + kk;
-          if (k < NC) {
-            const int64_t dof = 3 * (int64_t)kc[k] + ld;
-            if (!uk[kk]) {
-              double* col = P.A + dof * P.lda + row;
-#pragma unroll
-              for (int jj = 0; jj < 3; ++jj) col[jj] = old[kk][jj] + (double)full[k][jj];
-            } else {
-              const double v = __ldg(P.vp + dof);
-#pragma unroll
-              for (int jj = 0; jj < 3; ++jj) fi[jj] = fma(-(double)full[k][jj], v, fi[jj]);
-            }
-          }
-        }
-      }
-    }
-  }
-#pragma unroll
-  for (int jj = 0; jj < 3; ++jj) fi_acc[jj] += fi[jj];
-}
-
 // PREC 0: every regular pair in FP64.  PREC 1: pairs farther than 3.5 element radii
 // from the element centroid (the near-field radius of stress_mod.f90:603-604) evaluate
 // and accumulate the Kelvin kernels in FP32; nearer pairs stay in FP64.
@@ -420,11 +255,7 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
 // warp (the batch being integrated and the next one, copied in meanwhile).
 constexpr int kTabSmem = 2 * kBatch * kTabStride * (int)sizeof(double);
 
-// V = 1 (mode A only): the per-component integration of regular_pair_ld, whose tabw
-// entries are double-buffered next to the tables ([2][kBatch][kTabW] after them).
-constexpr int kTabSmemLd = 2 * kBatch * (kTabStride + kTabW) * (int)sizeof(double);
-
-template <int MODE, int PREC, int V = 0>
+template <int MODE, int PREC>
 __device__ __forceinline__ void regular_tile(const AsmArgs& P, int tile) {
   __shared__ double s_red[kBatch][32][12];
   extern __shared__ __align__(16) double s_tab[];  // [2][kBatch][kTabStride]
@@ -439,11 +270,6 @@ __device__ __forceinline__ void regular_tile(const AsmArgs& P, int tile) {
         const char* src = reinterpret_cast<const char*>(P.tab + (int64_t)e * kTabStride);
         char* dst = reinterpret_cast<char*>(s_tab + ((b & 1) * kBatch + w) * kTabStride);
         for (int i = lane; i < kTabStride * 8 / 16; i += 32) cp_async16(dst + 16 * i, src + 16 * i);
-        if (V == 1) {
-          const char* srcw = reinterpret_cast<const char*>(P.tabw + (int64_t)e * kTabW);
-          char* dstw = reinterpret_cast<char*>(s_tab + 2 * kBatch * kTabStride + ((b & 1) * kBatch + w) * kTabW);
-          for (int i = lane; i < kTabW * 8 / 16; i += 32) cp_async16(dstw + 16 * i, srcw + 16 * i);
-        }
       }
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
@@ -465,7 +291,6 @@ __device__ __forceinline__ void regular_tile(const AsmArgs& P, int tile) {
     asm volatile("cp.async.wait_group 1;" ::: "memory");  // this batch's table is in
     __syncwarp();
     const double* T = s_tab + ((b & 1) * kBatch + w) * kTabStride;
-    const double* TW = s_tab + 2 * kBatch * kTabStride + ((b & 1) * kBatch + w) * kTabW;
     if (e >= 0) {
       const int ncone = __ldg(P.nconec + e);
       int kc[9];
@@ -494,19 +319,7 @@ __device__ __forceinline__ void regular_tile(const AsmArgs& P, int tile) {
         const double dx = xi0 - cx, dy = xi1 - cy, dz = xi2 - cz;
         far32 = dx * dx + dy * dy + dz * dz > 12.25 * r2;
       }
-      if (V == 1 && active && !sing) {
-        if (ncone == 9) {
-          if (far32)
-            regular_pair_ld<9, float>(P, e, T, TW, kc, xi0, xi1, xi2, row, fi, d1);
-          else
-            regular_pair_ld<9, double>(P, e, T, TW, kc, xi0, xi1, xi2, row, fi, d1);
-        } else {
-          if (far32)
-            regular_pair_ld<6, float>(P, e, T, TW, kc, xi0, xi1, xi2, row, fi, d1);
-          else
-            regular_pair_ld<6, double>(P, e, T, TW, kc, xi0, xi1, xi2, row, fi, d1);
-        }
-      } else if (active && !sing) {
+      if (active && !sing) {
         if (ncone == 9) {
           if (far32)
             regular_pair<9, MODE, float>(P, e, T, kc, xi0, xi1, xi2, row, fi, d1);
@@ -557,12 +370,6 @@ __device__ __forceinline__ void regular_tile(const AsmArgs& P, int tile) {
 template <int MODE, int PREC>
 __global__ void __launch_bounds__(256, 1) ghmat_regular_kernel(AsmArgs P) {
   regular_tile<MODE, PREC>(P, blockIdx.x);
-}
-
-// the per-component variant: two CTAs per SM
-template <int PREC>
-__global__ void __launch_bounds__(256, 2) ghmat_regular_ld_kernel(AsmArgs P) {
-  regular_tile<kModeA, PREC, 1>(P, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------------
@@ -851,16 +658,6 @@ static int upload_singular_constants(bem_ctx* c) {
   return BEM_OK;
 }
 
-// the assembly variant (BEM_ASM_VARIANT: 0 both full blocks per element, 1 one
-// component at a time)
-static int asm_variant() {
-  static const int v = [] {
-    const char* e = getenv("BEM_ASM_VARIANT");
-    return e ? atoi(e) : 0;
-  }();
-  return v;
-}
-
 int launch_ghmat8(bem_ctx* c, int precision) {
   if (!c->have_geometry || !c->have_bc || !c->have_material)
     return bem_fail(c, BEM_ERR_STATE, "ghmat8 needs mesh, material, bc and geometry");
@@ -891,30 +688,10 @@ int launch_ghmat8(bem_ctx* c, int precision) {
                                      kTabSmem));
     attr.mark();
   }
-  if (asm_variant() == 1) {
-    static DeviceOnce attr_ld;
-    if (attr_ld.pending()) {
-      BEM_CUDA(c, cudaFuncSetAttribute(ghmat_regular_ld_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       kTabSmemLd));
-      BEM_CUDA(c, cudaFuncSetAttribute(ghmat_regular_ld_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       kTabSmemLd));
-      attr_ld.mark();
-    }
-    BEM_CUDA(c, c->tabw.alloc((size_t)kTabW * c->ne));
-    const int64_t ng = (int64_t)c->ne * kGp;
-    tabw_kernel<<<(unsigned)((ng + 127) / 128), 128, 0, c->stream>>>(c->ne, c->nconec.p, c->bc.p, c->tab.p,
-                                                                      c->tabw.p);
-    BEM_LAUNCH_CHECK(c);
-    P.tabw = c->tabw.p;
-    if (precision == BEM_ASM_FP32_FAR)
-      ghmat_regular_ld_kernel<1><<<tiles, 256, kTabSmemLd, c->stream>>>(P);
-    else
-      ghmat_regular_ld_kernel<0><<<tiles, 256, kTabSmemLd, c->stream>>>(P);
-  } else if (precision == BEM_ASM_FP32_FAR) {
+  if (precision == BEM_ASM_FP32_FAR)
     ghmat_regular_kernel<kModeA, 1><<<tiles, 256, kTabSmem, c->stream>>>(P);
-  } else {
+  else
     ghmat_regular_kernel<kModeA, 0><<<tiles, 256, kTabSmem, c->stream>>>(P);
-  }
   BEM_LAUNCH_CHECK(c);
   ghmat_singular_kernel<kModeA><<<(c->n + 3) / 4, 128, 0, c->stream>>>(P);
   BEM_LAUNCH_CHECK(c);

@@ -392,9 +392,15 @@ __global__ void __launch_bounds__(kSolveThreads)
         for (int i = j0 + jb + tid; i < N; i += kSolveThreads) {
           double acc[kMaxRhs];
           for (int r = 0; r < nc; ++r) acc[r] = sB[i * nc + r];
-          for (int q = 0; q < jb; ++q) {
-            const double l = (double)A[i + (int64_t)(j0 + q) * S.lda];
-            for (int r = 0; r < nc; ++r) acc[r] = fma(-l, s_x[q][r], acc[r]);
+          for (int q0 = 0; q0 < jb; q0 += 8) {  // eight loads in flight, then their FMAs
+            T lv[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) lv[u] = (q0 + u < jb) ? A[i + (int64_t)(j0 + q0 + u) * S.lda] : T(0);
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+              const double l = (double)lv[u];
+              for (int r = 0; r < nc; ++r) acc[r] = fma(-l, s_x[q0 + u < jb ? q0 + u : 0][r], acc[r]);
+            }
           }
           for (int r = 0; r < nc; ++r) sB[i * nc + r] = acc[r];
         }
@@ -430,9 +436,15 @@ __global__ void __launch_bounds__(kSolveThreads)
         for (int i = tid; i < j0; i += kSolveThreads) {
           double acc[kMaxRhs];
           for (int r = 0; r < nc; ++r) acc[r] = sB[i * nc + r];
-          for (int q = 0; q < jb; ++q) {
-            const double u = (double)A[i + (int64_t)(j0 + q) * S.lda];
-            for (int r = 0; r < nc; ++r) acc[r] = fma(-u, s_x[q][r], acc[r]);
+          for (int q0 = 0; q0 < jb; q0 += 8) {  // eight loads in flight, then their FMAs
+            T uv[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) uv[k] = (q0 + k < jb) ? A[i + (int64_t)(j0 + q0 + k) * S.lda] : T(0);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+              const double u = (double)uv[k];
+              for (int r = 0; r < nc; ++r) acc[r] = fma(-u, s_x[q0 + k < jb ? q0 + k : 0][r], acc[r]);
+            }
           }
           for (int r = 0; r < nc; ++r) sB[i * nc + r] = acc[r];
         }
@@ -487,12 +499,26 @@ __global__ void __launch_bounds__(kSolveThreads)
           sX[c * nrhs + r] = X[S.v_off + c0 + c + (int64_t)r * N];
         }
         __syncthreads();
-        if (i < N)
-          for (int c = 0; c < cn; ++c) {
+        if (i < N) {
+          // eight columns per step: eight independent loads in flight per thread (one
+          // CTA per system streams its whole A, so memory-level parallelism sets the time)
+          int c = 0;
+          for (; c + 8 <= cn; c += 8) {
+            double a[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) a[u] = As[i + (int64_t)(c0 + c + u) * S.lda];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+              asum += fabs(a[u]);
+              for (int r = 0; r < nrhs; ++r) acc[r] = fma(-a[u], sX[(c + u) * nrhs + r], acc[r]);
+            }
+          }
+          for (; c < cn; ++c) {
             const double a = As[i + (int64_t)(c0 + c) * S.lda];
             asum += fabs(a);
             for (int r = 0; r < nrhs; ++r) acc[r] = fma(-a, sX[c * nrhs + r], acc[r]);
           }
+        }
       }
       if (i < N) {
         amax = fmax(amax, asum);

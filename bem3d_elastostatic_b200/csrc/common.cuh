@@ -156,7 +156,6 @@ struct bem_ctx {
 
   // geometry (reference layout) and the packed assembly table
   bem::DBuf<double> eta1, eta2, eta3, xja, xg1, xg2, xg3, ff, tab;
-  bem::DBuf<double> tabw;  // per element and Gauss point: node sums of p12 (assembly.cu)
   bool have_geometry = false;
 
   // system

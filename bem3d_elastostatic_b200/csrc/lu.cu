@@ -220,6 +220,66 @@ __global__ void __launch_bounds__(panel_threads<T>(), 1)
   }
 }
 
+// LU with partial pivoting of a full 32 x 32 window by one warp, in place in D
+// (D[c][j] = row j of column c; lane c owns column c in registers): per step the pivot
+// column is broadcast by shuffles and the other lanes eliminate.  The search of a step
+// is one vote (is any candidate larger than the diagonal?) and only then the warp
+// argmax with the smallest-index tie rule; the operations are those of the general
+// loops.  The step loop is not unrolled (the warp's whole code stays in the
+// instruction cache); s_p[t] receives the local pivot of step t.
+template <typename T>
+__device__ __forceinline__ void window_lu_warp(T (*D)[kPanelW + 1], int* s_p, int lane) {
+  constexpr int W = kPanelW;
+  T col[W];
+#pragma unroll
+  for (int j = 0; j < W; ++j) col[j] = D[lane][j];
+#pragma unroll 1
+  for (int t = 0; t < W; ++t) {
+    T ct = T(0);
+#pragma unroll
+    for (int j = 0; j < W; ++j)
+      if (j == t) ct = col[j];
+    T pv = __shfl_sync(0xffffffffu, ct, t);
+    int p = t;
+    if (__any_sync(0xffffffffu, lane > t && fabs((double)ct) > fabs((double)pv))) {
+      double bv = (lane >= t) ? fabs((double)ct) : -1.0;
+      int bc = (lane >= t) ? lane : INT_MAX, bg = 0;
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
+        const int oc = __shfl_xor_sync(0xffffffffu, bc, off);
+        better(bv, bc, bg, ov, oc, 0);
+      }
+      p = bc;
+      if (p != t) {  // lanes t and p exchange their columns
+        const int src = (lane == t) ? p : ((lane == p) ? t : lane);
+#pragma unroll
+        for (int j = 0; j < W; ++j) col[j] = __shfl_sync(0xffffffffu, col[j], src);
+#pragma unroll
+        for (int j = 0; j < W; ++j)
+          if (j == t) ct = col[j];
+        pv = __shfl_sync(0xffffffffu, ct, t);
+      }
+    }
+    if (lane == 0) s_p[t] = p;
+    if (pv != T(0)) {
+      const T l = ct / pv;
+#pragma unroll
+      for (int j = 0; j < W; ++j) {
+        const T pj = __shfl_sync(0xffffffffu, col[j], t);
+        if (lane > t) {
+          if (j == t)
+            col[j] = l;
+          else if (j > t)
+            col[j] -= l * pj;
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < W; ++j) D[lane][j] = col[j];
+}
+
 // Window pivoting: the sub-panel's pivot search is restricted to its w x w diagonal
 // block (T rows r0..r0+w), so the sub-panel needs no grid-wide exchange.  Every CTA
 // factors that block redundantly in shared memory (warp 0: lane c owns column c of the
@@ -265,41 +325,7 @@ __global__ void __launch_bounds__(256) window_panel_kernel(T* S, int64_t lda, in
       D[cc][lane] = (cc < w && lane < w) ? S[r0 + lane + (int64_t)(r0 + cc) * lda] : T(0);
     __syncwarp();
     if (w == kPanelW) {
-      // a full window in registers: lane c holds column c, every loop is unrolled, the
-      // pivot column reaches the other lanes by shuffles (the same operations as below)
-      T col[kPanelW];
-#pragma unroll
-      for (int j = 0; j < kPanelW; ++j) col[j] = D[lane][j];
-#pragma unroll
-      for (int t = 0; t < kPanelW; ++t) {
-        double bv = (lane >= t) ? fabs((double)col[t]) : -1.0;
-        int bc = (lane >= t) ? lane : INT_MAX, bg = 0;
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-          const double ov = __shfl_xor_sync(0xffffffffu, bv, off);
-          const int oc = __shfl_xor_sync(0xffffffffu, bc, off);
-          better(bv, bc, bg, ov, oc, 0);
-        }
-        const int p = bc;
-        if (lane == 0) s_p[t] = p;
-        if (p != t) {  // warp-uniform: lanes t and p exchange their columns
-          const int src = (lane == t) ? p : ((lane == p) ? t : lane);
-#pragma unroll
-          for (int j = 0; j < kPanelW; ++j) col[j] = __shfl_sync(0xffffffffu, col[j], src);
-        }
-        const T pv = __shfl_sync(0xffffffffu, col[t], t);
-        if (pv != T(0)) {
-          const T l = col[t] / pv;
-          if (lane > t) col[t] = l;
-#pragma unroll
-          for (int j = t + 1; j < kPanelW; ++j) {
-            const T pj = __shfl_sync(0xffffffffu, col[j], t);
-            if (lane > t) col[j] -= l * pj;
-          }
-        }
-      }
-#pragma unroll
-      for (int j = 0; j < kPanelW; ++j) D[lane][j] = col[j];
+      window_lu_warp<T>(D, s_p, lane);
     } else {
       for (int t = 0; t < w; ++t) {
         double bv = (lane >= t && lane < w) ? fabs((double)D[lane][t]) : -1.0;
@@ -370,6 +396,100 @@ __global__ void __launch_bounds__(256) window_panel_kernel(T* S, int64_t lda, in
 #pragma unroll
     for (int j = 0; j < kPanelW; ++j)
       if (j < w) dst[j] = x[j];
+  }
+}
+
+// The whole step of one 32-wide sub-panel of a window-pivoted FP32 panel in one CTA
+// (the panel's diagonal block only; rows and columns outside it follow per panel):
+// warp 0 factors the 32 x 32 window in registers while the other threads load their
+// columns; every thread then eliminates its column of the sub-panel (columns
+// [r0 + 32, t0)), the factored window goes back into S, and one thread per row of the
+// block applies the window's interchanges as a gather and, below the window, the
+// unit-lower TRSM of trsm_small_kernel.  Pivots and the first exact zero pivot as
+// window_panel_kernel.  w = 32; t0 - r0 <= kBlockThreads.
+constexpr int kBlockThreads = 512;
+__global__ void __launch_bounds__(kBlockThreads) window_block_kernel(float* S, int64_t lda, int j0, int t0, int r0,
+                                                                     int* piv, int* status) {
+  constexpr int W = kPanelW;
+  __shared__ float D[W][W + 1];  // D[c][j] = S(r0 + j, r0 + c)
+  __shared__ int s_p[W], s_g[W];
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int c = r0 + W + tid;  // this thread's column
+  float x[W];
+  const bool has_col = c < t0;
+  if (has_col) {
+    const float* src = S + r0 + (int64_t)c * lda;
+#pragma unroll
+    for (int q = 0; q < W / 4; ++q) {
+      const float4 v = *reinterpret_cast<const float4*>(src + 4 * q);
+      x[4 * q] = v.x;
+      x[4 * q + 1] = v.y;
+      x[4 * q + 2] = v.z;
+      x[4 * q + 3] = v.w;
+    }
+  }
+  if (tid < W) {
+#pragma unroll
+    for (int cc = 0; cc < W; ++cc) D[cc][lane] = S[r0 + lane + (int64_t)(r0 + cc) * lda];
+    __syncwarp();
+    window_lu_warp<float>(D, s_p, lane);
+    __syncwarp();
+    if (lane == 0) {
+      // the window's interchanges composed into a gather: y[b] = x[g[b]]
+      for (int b = 0; b < W; ++b) s_g[b] = b;
+      for (int t = 0; t < W; ++t) {
+        const int p = s_p[t], a = s_g[t];
+        s_g[t] = s_g[p];
+        s_g[p] = a;
+      }
+      for (int t = 0; t < W; ++t)
+        if (D[t][t] == 0.f) {
+          if (status[1] == 0) status[1] = r0 + t + 1;
+          break;
+        }
+    }
+    piv[r0 + lane] = r0 + s_p[lane];
+  }
+  __syncthreads();
+  if (has_col) {
+#pragma unroll
+    for (int t = 0; t < W; ++t) {
+      const float pv = D[t][t];
+      if (pv != 0.f) {
+        const float l = x[t] / pv;
+        x[t] = l;
+#pragma unroll
+        for (int j = t + 1; j < W; ++j) x[j] -= l * D[t][j];
+      }
+    }
+    float* dst = S + r0 + (int64_t)c * lda;
+#pragma unroll
+    for (int q = 0; q < W / 4; ++q)
+      *reinterpret_cast<float4*>(dst + 4 * q) = make_float4(x[4 * q], x[4 * q + 1], x[4 * q + 2], x[4 * q + 3]);
+  }
+  // the factored window
+  for (int i = tid; i < W * W; i += blockDim.x) {
+    const int j = i % W, cc = i / W;
+    S[r0 + j + (int64_t)(r0 + cc) * lda] = D[cc][j];
+  }
+  // rows of the block outside the window: the interchanges, and below it the TRSM
+  const int nabove = r0 - j0, nrows = (t0 - j0) - W;
+  if (tid < nrows) {
+    const int r = tid < nabove ? j0 + tid : r0 + W + (tid - nabove);
+    float y[W];
+#pragma unroll
+    for (int b = 0; b < W; ++b) y[b] = S[r + (int64_t)(r0 + s_g[b]) * lda];
+    if (r >= r0 + W) {
+#pragma unroll
+      for (int b = 0; b < W; ++b) {
+        float v = y[b];
+#pragma unroll
+        for (int a = 0; a < b; ++a) v -= y[a] * D[b][a];  // U(a, b) = S(r0 + a, r0 + b)
+        y[b] = v;
+      }
+    }
+#pragma unroll
+    for (int b = 0; b < W; ++b) S[r + (int64_t)(r0 + b) * lda] = y[b];
   }
 }
 
@@ -1045,6 +1165,21 @@ static int lu_factor_enqueue(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int
     for (int r0 = j0; r0 < j0 + jb; r0 += kPanelW) {
       const int w = std::min(kPanelW, j0 + jb - r0);
       prof.begin(0, c->stream);
+      if (cend < n && w == kPanelW && sizeof(T) == 4 && lda % 4 == 0 &&
+          (reinterpret_cast<uintptr_t>(S) & 15) == 0) {
+        // window-pivoted FP32 panel: the sub-panel's step in one CTA, then its GEMM
+        window_block_kernel<<<1, kBlockThreads, 0, c->stream>>>(reinterpret_cast<float*>(S), lda, j0, j0 + jb, r0, piv,
+                                                                 ws.status);
+        BEM_LAUNCH_CHECK(c);
+        prof.end(c->stream);
+        const int q0 = r0 + w, q1 = j0 + jb;
+        prof.begin(2, c->stream);
+        if (q1 > q0 && (rc = gemm<T>(c, q1 - q0, cend - q0, w, S + q0 + (int64_t)r0 * lda, lda,
+                                     S + r0 + (int64_t)q0 * lda, lda, S + q0 + (int64_t)q0 * lda, lda, 0)))
+          return rc;
+        prof.end(c->stream);
+        continue;
+      }
       if (window) {
         if ((rc = window_panel_launch<T>(c, ws, S, lda, cend, r0, w, piv))) return rc;
       } else if ((rc = panel_launch<T>(c, ws, S, lda, n, r0, w, piv, bar_base))) {
