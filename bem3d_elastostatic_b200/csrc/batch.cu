@@ -352,7 +352,7 @@ __global__ void __launch_bounds__(kSolveThreads)
     for (int r0 = 0; r0 < S.nrhs; r0 += nc_max) {
       const int nc = min(nc_max, S.nrhs - r0);
       for (int i = tid; i < N; i += kSolveThreads)
-        for (int r = 0; r < nc; ++r) sB[i * nc + r] = R[S.v_off + i + (int64_t)(r0 + r) * N];
+        _Pragma("unroll") for (int r = 0; r < kMaxRhs; ++r) if (r < nc) sB[i * nc + r] = R[S.v_off + i + (int64_t)(r0 + r) * N];
       __syncthreads();
       if (tid < nc)
         for (int j = 0; j < N; ++j) {
@@ -374,15 +374,15 @@ __global__ void __launch_bounds__(kSolveThreads)
         __syncthreads();
         if (tid < 32) {
           double b[kMaxRhs];
-          for (int r = 0; r < nc; ++r) b[r] = (lane < jb) ? sB[(j0 + lane) * nc + r] : 0.0;
+          _Pragma("unroll") for (int r = 0; r < kMaxRhs; ++r) if (r < nc) b[r] = (lane < jb) ? sB[(j0 + lane) * nc + r] : 0.0;
           for (int t = 0; t < jb; ++t) {
             const double l = (lane > t && lane < jb) ? s_d[lane][t] : 0.0;
-            for (int r = 0; r < nc; ++r) {
+            _Pragma("unroll") for (int r = 0; r < kMaxRhs; ++r) if (r < nc) {
               const double xt = __shfl_sync(0xffffffffu, b[r], t);
               b[r] = fma(-l, xt, b[r]);
             }
           }
-          for (int r = 0; r < nc; ++r)
+          _Pragma("unroll") for (int r = 0; r < kMaxRhs; ++r) if (r < nc)
             if (lane < jb) {
               sB[(j0 + lane) * nc + r] = b[r];
               s_x[lane][r] = b[r];
@@ -391,7 +391,7 @@ __global__ void __launch_bounds__(kSolveThreads)
         __syncthreads();
         for (int i = j0 + jb + tid; i < N; i += kSolveThreads) {
           double acc[kMaxRhs];
-          for (int r = 0; r < nc; ++r) acc[r] = sB[i * nc + r];
+          _Pragma("unroll") for (int r = 0; r < kMaxRhs; ++r) if (r < nc) acc[r] = sB[i * nc + r];
           for (int q0 = 0; q0 < jb; q0 += 8) {  // eight loads in flight, then their FMAs
             T lv[8];
 #pragma unroll
@@ -399,10 +399,10 @@ __global__ void __launch_bounds__(kSolveThreads)
 #pragma unroll
             for (int u = 0; u < 8; ++u) {
               const double l = (double)lv[u];
-              for (int r = 0; r < nc; ++r) acc[r] = fma(-l, s_x[q0 + u < jb ? q0 + u : 0][r], acc[r]);
+              _Pragma("unroll") for (int r = 0; r < kMaxRhs; ++r) if (r < nc) acc[r] = fma(-l, s_x[q0 + u < jb ? q0 + u : 0][r], acc[r]);
             }
           }
-          for (int r = 0; r < nc; ++r) sB[i * nc + r] = acc[r];
+          _Pragma("unroll") for (int r = 0; r < kMaxRhs; ++r) if (r < nc) sB[i * nc + r] = acc[r];
         }
         __syncthreads();
       }
@@ -416,17 +416,17 @@ __global__ void __launch_bounds__(kSolveThreads)
         __syncthreads();
         if (tid < 32) {
           double b[kMaxRhs];
-          for (int r = 0; r < nc; ++r) b[r] = (lane < jb) ? sB[(j0 + lane) * nc + r] : 0.0;
+          _Pragma("unroll") for (int r = 0; r < kMaxRhs; ++r) if (r < nc) b[r] = (lane < jb) ? sB[(j0 + lane) * nc + r] : 0.0;
           for (int t = jb - 1; t >= 0; --t) {
             const double d = s_d[t][t];
             const double u = (lane < t) ? s_d[lane][t] : 0.0;
-            for (int r = 0; r < nc; ++r) {
+            _Pragma("unroll") for (int r = 0; r < kMaxRhs; ++r) if (r < nc) {
               const double xt = __shfl_sync(0xffffffffu, b[r], t) / d;
               if (lane == t) b[r] = xt;
               else b[r] = fma(-u, xt, b[r]);
             }
           }
-          for (int r = 0; r < nc; ++r)
+          _Pragma("unroll") for (int r = 0; r < kMaxRhs; ++r) if (r < nc)
             if (lane < jb) {
               sB[(j0 + lane) * nc + r] = b[r];
               s_x[lane][r] = b[r];
@@ -435,7 +435,7 @@ __global__ void __launch_bounds__(kSolveThreads)
         __syncthreads();
         for (int i = tid; i < j0; i += kSolveThreads) {
           double acc[kMaxRhs];
-          for (int r = 0; r < nc; ++r) acc[r] = sB[i * nc + r];
+          _Pragma("unroll") for (int r = 0; r < kMaxRhs; ++r) if (r < nc) acc[r] = sB[i * nc + r];
           for (int q0 = 0; q0 < jb; q0 += 8) {  // eight loads in flight, then their FMAs
             T uv[8];
 #pragma unroll
@@ -443,15 +443,15 @@ __global__ void __launch_bounds__(kSolveThreads)
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
               const double u = (double)uv[k];
-              for (int r = 0; r < nc; ++r) acc[r] = fma(-u, s_x[q0 + k < jb ? q0 + k : 0][r], acc[r]);
+              _Pragma("unroll") for (int r = 0; r < kMaxRhs; ++r) if (r < nc) acc[r] = fma(-u, s_x[q0 + k < jb ? q0 + k : 0][r], acc[r]);
             }
           }
-          for (int r = 0; r < nc; ++r) sB[i * nc + r] = acc[r];
+          _Pragma("unroll") for (int r = 0; r < kMaxRhs; ++r) if (r < nc) sB[i * nc + r] = acc[r];
         }
         __syncthreads();
       }
       for (int i = tid; i < N; i += kSolveThreads)
-        for (int r = 0; r < nc; ++r) {
+        _Pragma("unroll") for (int r = 0; r < kMaxRhs; ++r) if (r < nc) {
           double* xo = X + S.v_off + i + (int64_t)(r0 + r) * N;
           *xo = accumulate ? *xo + sB[i * nc + r] : sB[i * nc + r];
         }
@@ -489,7 +489,7 @@ __global__ void __launch_bounds__(kSolveThreads)
     for (int rb = 0; rb < rows_per; ++rb) {
       const int i = tid + rb * kSolveThreads;
       double acc[kMaxRhs], asum = 0.0;
-      for (int r = 0; r < nrhs; ++r) acc[r] = (i < N) ? B[S.v_off + i + (int64_t)r * N] : 0.0;
+      _Pragma("unroll") for (int r = 0; r < kMaxRhs; ++r) if (r < nrhs) acc[r] = (i < N) ? B[S.v_off + i + (int64_t)r * N] : 0.0;
       const int ncol = max(1, (int)(kSolveSmem / (sizeof(double) * (size_t)nrhs)));
       for (int c0 = 0; c0 < N; c0 += ncol) {
         const int cn = min(ncol, N - c0);
@@ -510,19 +510,19 @@ __global__ void __launch_bounds__(kSolveThreads)
 #pragma unroll
             for (int u = 0; u < 8; ++u) {
               asum += fabs(a[u]);
-              for (int r = 0; r < nrhs; ++r) acc[r] = fma(-a[u], sX[(c + u) * nrhs + r], acc[r]);
+              _Pragma("unroll") for (int r = 0; r < kMaxRhs; ++r) if (r < nrhs) acc[r] = fma(-a[u], sX[(c + u) * nrhs + r], acc[r]);
             }
           }
           for (; c < cn; ++c) {
             const double a = As[i + (int64_t)(c0 + c) * S.lda];
             asum += fabs(a);
-            for (int r = 0; r < nrhs; ++r) acc[r] = fma(-a, sX[c * nrhs + r], acc[r]);
+            _Pragma("unroll") for (int r = 0; r < kMaxRhs; ++r) if (r < nrhs) acc[r] = fma(-a, sX[c * nrhs + r], acc[r]);
           }
         }
       }
       if (i < N) {
         amax = fmax(amax, asum);
-        for (int r = 0; r < nrhs; ++r) {
+        _Pragma("unroll") for (int r = 0; r < kMaxRhs; ++r) if (r < nrhs) {
           R[S.v_off + i + (int64_t)r * N] = acc[r];
           rmax[r] = fmax(rmax[r], fabs(acc[r]));
           xmax[r] = fmax(xmax[r], fabs(X[S.v_off + i + (int64_t)r * N]));
@@ -532,14 +532,14 @@ __global__ void __launch_bounds__(kSolveThreads)
     }
     for (int off = 16; off > 0; off >>= 1) {
       amax = fmax(amax, __shfl_xor_sync(0xffffffffu, amax, off));
-      for (int r = 0; r < nrhs; ++r) {
+      _Pragma("unroll") for (int r = 0; r < kMaxRhs; ++r) if (r < nrhs) {
         rmax[r] = fmax(rmax[r], __shfl_xor_sync(0xffffffffu, rmax[r], off));
         xmax[r] = fmax(xmax[r], __shfl_xor_sync(0xffffffffu, xmax[r], off));
         bmax[r] = fmax(bmax[r], __shfl_xor_sync(0xffffffffu, bmax[r], off));
       }
     }
     if (lane == 0) {
-      for (int r = 0; r < nrhs; ++r) {
+      _Pragma("unroll") for (int r = 0; r < kMaxRhs; ++r) if (r < nrhs) {
         s_red[wp][r] = rmax[r];
         s_red[wp][kMaxRhs + r] = xmax[r];
         s_red[wp][2 * kMaxRhs + r] = bmax[r];
@@ -550,7 +550,7 @@ __global__ void __launch_bounds__(kSolveThreads)
     if (tid == 0) {
       double an = 0.0, be = 0.0;
       for (int w = 0; w < kSolveThreads / 32; ++w) an = fmax(an, s_red[w][3 * kMaxRhs]);
-      for (int r = 0; r < nrhs; ++r) {
+      _Pragma("unroll") for (int r = 0; r < kMaxRhs; ++r) if (r < nrhs) {
         double rn = 0.0, xn = 0.0, bn = 0.0;
         for (int w = 0; w < kSolveThreads / 32; ++w) {
           rn = fmax(rn, s_red[w][r]);

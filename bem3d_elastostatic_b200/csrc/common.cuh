@@ -177,6 +177,7 @@ struct bem_ctx {
   // refinement vectors (residual, correction) and timing events, kept: allocation and
   // release next to a 10^10-byte system stalled the host for up to 0.7 s per solve
   bem::DBuf<double> ir_r, ir_d, ir_dmax;
+  bem::DBuf<double> gm_V, gm_h, gm_part, gm_zero;  // GMRES-IR basis and reduction buffers
   bem::DBuf<double> A64f;     // FP64 factor copy of BEM_PREC_FP64_IR
   bool ext_residual = true;  // BEM_OPT_RESIDUAL: refinement residuals in double-double
   cudaEvent_t solve_ev[3] = {nullptr, nullptr, nullptr};

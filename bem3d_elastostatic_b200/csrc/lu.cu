@@ -221,25 +221,20 @@ __global__ void __launch_bounds__(panel_threads<T>(), 1)
 }
 
 // LU with partial pivoting of a full 32 x 32 window by one warp, in place in D
-// (D[c][j] = row j of column c; lane c owns column c in registers): per step the pivot
-// column is broadcast by shuffles and the other lanes eliminate.  The search of a step
-// is one vote (is any candidate larger than the diagonal?) and only then the warp
-// argmax with the smallest-index tie rule; the operations are those of the general
-// loops.  The step loop is not unrolled (the warp's whole code stays in the
-// instruction cache); s_p[t] receives the local pivot of step t.
+// (D[c][j] = row j of column c; lane c owns column c).  Per step the search is one vote
+// (is any candidate larger than the diagonal?) and only then the warp argmax with the
+// smallest-index tie rule; the update loads the pivot column and the lane's own column
+// into registers, updates them there and stores the lane's column back, so the step's
+// shared-memory accesses are independent of one another.  The operations are those of
+// the general loops; the step loop is not unrolled (the warp's code stays in the
+// instruction cache).  s_p[t] receives the local pivot of step t.
 template <typename T>
 __device__ __forceinline__ void window_lu_warp(T (*D)[kPanelW + 1], int* s_p, int lane) {
   constexpr int W = kPanelW;
-  T col[W];
-#pragma unroll
-  for (int j = 0; j < W; ++j) col[j] = D[lane][j];
 #pragma unroll 1
   for (int t = 0; t < W; ++t) {
-    T ct = T(0);
-#pragma unroll
-    for (int j = 0; j < W; ++j)
-      if (j == t) ct = col[j];
-    T pv = __shfl_sync(0xffffffffu, ct, t);
+    T ct = D[lane][t];
+    T pv = D[t][t];
     int p = t;
     if (__any_sync(0xffffffffu, lane > t && fabs((double)ct) > fabs((double)pv))) {
       double bv = (lane >= t) ? fabs((double)ct) : -1.0;
@@ -251,33 +246,33 @@ __device__ __forceinline__ void window_lu_warp(T (*D)[kPanelW + 1], int* s_p, in
         better(bv, bc, bg, ov, oc, 0);
       }
       p = bc;
-      if (p != t) {  // lanes t and p exchange their columns
-        const int src = (lane == t) ? p : ((lane == p) ? t : lane);
-#pragma unroll
-        for (int j = 0; j < W; ++j) col[j] = __shfl_sync(0xffffffffu, col[j], src);
-#pragma unroll
-        for (int j = 0; j < W; ++j)
-          if (j == t) ct = col[j];
-        pv = __shfl_sync(0xffffffffu, ct, t);
+      if (p != t) {  // columns t and p exchanged: lane j swaps their element j
+        const T a = D[t][lane];
+        D[t][lane] = D[p][lane];
+        D[p][lane] = a;
+        __syncwarp();
+        ct = D[lane][t];
+        pv = D[t][t];
       }
     }
     if (lane == 0) s_p[t] = p;
-    if (pv != T(0)) {
+    if (pv != T(0) && lane > t) {
       const T l = ct / pv;
+      T pr[W], my[W];
 #pragma unroll
       for (int j = 0; j < W; ++j) {
-        const T pj = __shfl_sync(0xffffffffu, col[j], t);
-        if (lane > t) {
-          if (j == t)
-            col[j] = l;
-          else if (j > t)
-            col[j] -= l * pj;
-        }
+        pr[j] = D[t][j];
+        my[j] = D[lane][j];
       }
-    }
-  }
 #pragma unroll
-  for (int j = 0; j < W; ++j) D[lane][j] = col[j];
+      for (int j = 0; j < W; ++j)
+        if (j > t) my[j] -= l * pr[j];
+#pragma unroll
+      for (int j = 0; j < W; ++j)
+        if (j >= t) D[lane][j] = (j == t) ? l : my[j];
+    }
+    __syncwarp();
+  }
 }
 
 // Window pivoting: the sub-panel's pivot search is restricted to its w x w diagonal

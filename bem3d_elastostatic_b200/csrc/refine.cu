@@ -331,11 +331,16 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
     // GMRES-IR: Krylov basis V (kGmresM + 1 vectors), FP64; Hessenberg least squares
     // by Givens rotations on the host
     const int64_t ldv = ((int64_t)n + 31) / 32 * 32;
-    DBuf<double> Vb, hd, part, zero;
-    BEM_CUDA(c, Vb.alloc((size_t)ldv * (kGmresM + 1)));
-    BEM_CUDA(c, hd.alloc(2 * (kGmresM + 1)));
-    BEM_CUDA(c, part.alloc((size_t)kDotBlocks * (kGmresM + 1)));
-    BEM_CUDA(c, zero.alloc(n));
+    // the Krylov basis and the reduction buffers are kept in the context (allocation
+    // and release next to a 10^10-byte system stall the host)
+    DBuf<double>& Vb = c->gm_V;
+    DBuf<double>& hd = c->gm_h;
+    DBuf<double>& part = c->gm_part;
+    DBuf<double>& zero = c->gm_zero;
+    if (Vb.count != (size_t)ldv * (kGmresM + 1)) BEM_CUDA(c, Vb.alloc((size_t)ldv * (kGmresM + 1)));
+    if (hd.count != 2 * (size_t)(kGmresM + 1)) BEM_CUDA(c, hd.alloc(2 * (kGmresM + 1)));
+    if (part.count != (size_t)kDotBlocks * (kGmresM + 1)) BEM_CUDA(c, part.alloc((size_t)kDotBlocks * (kGmresM + 1)));
+    if (zero.count != (size_t)n) BEM_CUDA(c, zero.alloc(n));
     BEM_CUDA(c, cudaMemsetAsync(zero.p, 0, n * sizeof(double), c->stream));
     double* V = Vb.p;
     const int vb = (n + 255) / 256;
