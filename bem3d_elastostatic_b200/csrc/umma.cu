@@ -35,12 +35,19 @@ constexpr int UM = 128;                 // tile rows (UMMA M)
 constexpr int UN = 256;                 // tile columns (UMMA N)
 constexpr int UK = 64;                  // K chunk per TMA box (128 bytes of BF16)
 constexpr int kMaxK = 512;              // largest panel width
-constexpr int kStages = 2;              // shared-memory ring of K chunks
 constexpr int A_TILE = UM * UK * 2;     // 16 KB
 constexpr int B_TILE = UN * UK * 2;     // 32 KB
-constexpr int STAGE = 2 * A_TILE + 2 * B_TILE;  // hi + lo of A and B: 96 KB
+// shared-memory ring of K chunks: three products stage hi + lo of A and B (96 KB) in
+// two stages, one product only the hi parts (48 KB) in four, 192 KB either way
+template <int NPROD>
+struct Ring {
+  static constexpr int stages = NPROD == 3 ? 2 : 4;
+  static constexpr int stage = NPROD == 3 ? 2 * A_TILE + 2 * B_TILE : A_TILE + B_TILE;
+};
+constexpr int kRing = 2 * (2 * A_TILE + 2 * B_TILE);
+static_assert(Ring<1>::stages * Ring<1>::stage == kRing && Ring<3>::stages * Ring<3>::stage == kRing, "ring size");
 constexpr int kStg = 2 * 32 * UM * 4;  // two 128 x 32 FP32 staging boxes (one per epilogue half)
-constexpr int kSmem = kStages * STAGE + 1024 + 256 + kStg;
+constexpr int kSmem = kRing + 1024 + 256 + kStg;
 constexpr unsigned kTmemCols = 512;     // two 128 x 256 FP32 accumulators
 constexpr int kEpiThreads = 256;        // 8 epilogue warps
 constexpr int kThreads = 64 + kEpiThreads;
@@ -95,18 +102,20 @@ __global__ void __launch_bounds__(kThreads, 1)
                        const __grid_constant__ CUtensorMap tBh, const __grid_constant__ CUtensorMap tBl,
                        const __grid_constant__ CUtensorMap tC, int M, int N, int K, int* err,
                        unsigned long long wait_ns) {
+  constexpr int kStages = Ring<NPROD>::stages, STAGE = Ring<NPROD>::stage;
   extern __shared__ __align__(16) unsigned char umma_smem[];
   const unsigned raw = smem_u32(umma_smem);
   const unsigned base = (raw + 1023u) & ~1023u;  // 1024-byte aligned operand tiles
   unsigned char* gbase = umma_smem + (base - raw);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(gbase + kStages * STAGE);
-  uint64_t* full = bars;        // [kStages] TMA -> MMA
-  uint64_t* empty = bars + 2;   // [kStages] MMA -> TMA
-  uint64_t* tfull = bars + 4;   // [2] MMA -> epilogue
-  uint64_t* tempty = bars + 6;  // [2] epilogue -> MMA
-  uint64_t* drain = bars + 8;   // MMA completion before teardown
-  unsigned* tmem_slot = reinterpret_cast<unsigned*>(gbase + kStages * STAGE + 128);
-  volatile int* abort_flag = reinterpret_cast<volatile int*>(gbase + kStages * STAGE + 136);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(gbase + kRing);
+  uint64_t* full = bars;                      // [kStages] TMA -> MMA
+  uint64_t* empty = bars + kStages;           // [kStages] MMA -> TMA
+  uint64_t* tfull = bars + 2 * kStages;       // [2] MMA -> epilogue
+  uint64_t* tempty = bars + 2 * kStages + 2;  // [2] epilogue -> MMA
+  uint64_t* drain = bars + 2 * kStages + 4;   // MMA completion before teardown
+  static_assert((2 * kStages + 5) * 8 <= 128, "barrier block");
+  unsigned* tmem_slot = reinterpret_cast<unsigned*>(gbase + kRing + 128);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(gbase + kRing + 136);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int tiles_m = (M + UM - 1) / UM, tiles_n = (N + UN - 1) / UN, total = tiles_m * tiles_n;
@@ -146,7 +155,9 @@ __global__ void __launch_bounds__(kThreads, 1)
     if (lane == 0) {
       int stage = 0;
       unsigned phase = 0;
-      int last[kStages] = {-1, -1};
+      int last[kStages];
+#pragma unroll
+      for (int s = 0; s < kStages; ++s) last[s] = -1;
       const CUtensorMap* maps[4] = {&tAh, &tAl, &tBh, &tBl};
       for (int t = blockIdx.x; t < total && !*abort_flag; t += gridDim.x) {
         const int m0 = (t % tiles_m) * UM, n0 = (t / tiles_m) * UN;
@@ -162,7 +173,9 @@ __global__ void __launch_bounds__(kThreads, 1)
           constexpr unsigned kBytes = NPROD == 3 ? (unsigned)STAGE : (unsigned)(A_TILE + B_TILE);
           asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(kBytes)
                        : "memory");
-          const unsigned dst[4] = {st, st + A_TILE, st + 2 * A_TILE, st + 2 * A_TILE + B_TILE};
+          // stage layout: three products [A hi | A lo | B hi | B lo], one [A hi | B hi]
+          const unsigned dst[4] = {st, st + A_TILE, NPROD == 3 ? st + 2 * A_TILE : st + A_TILE,
+                                   st + 2 * A_TILE + B_TILE};
 #pragma unroll
           for (int q = 0; q < 4; ++q)
             if (NPROD == 3 || q == 0 || q == 2)
@@ -204,7 +217,8 @@ __global__ void __launch_bounds__(kThreads, 1)
           }
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
           const unsigned st = base + stage * STAGE;
-          const unsigned ah = st, al = st + A_TILE, bh = st + 2 * A_TILE, bl = st + 2 * A_TILE + B_TILE;
+          const unsigned ah = st, al = st + A_TILE, bh = NPROD == 3 ? st + 2 * A_TILE : st + A_TILE,
+                         bl = st + 2 * A_TILE + B_TILE;
 #pragma unroll
           for (int kk = 0; kk < UK / 16; ++kk) {
             const unsigned off = kk * 32;  // 16 BF16 = 32 bytes along K inside the swizzle atom
@@ -247,7 +261,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     // that half's staging box and its leader thread issues the box's reduction
     const int lq = warp & 3;
     const int half = (warp - 2) >> 2;  // 0 or 1
-    float* stg = reinterpret_cast<float*>(gbase + kStages * STAGE + 256) + half * (32 * UM);
+    float* stg = reinterpret_cast<float*>(gbase + kRing + 256) + half * (32 * UM);
     const unsigned stg_s = smem_u32(stg);
     const bool leader = (lq == 0 && lane == 0);
     int ab = 0;

@@ -2,8 +2,9 @@
 
 * 73,734-DOF unit cube (32 x 32 quad9 per face; A is 43.5 GB) at nu = 0.0, 0.3 and
   0.49: sampled row blocks of A and FI against the oracle's ghmat8 rows (the
-  entrywise bar of test_gpu_parity: 1e-12 of the row scale); the mixed-precision
-  solution (FP32 window-pivoted LU, refinement with double-double residuals) against
+  entrywise bar of test_gpu_parity: 1e-12 of the row scale); the solutions of both
+  mixed modes (FP32 window-pivoted LU with refinement, the equilibrated LU with one
+  BF16 tensor-core product and GMRES-IR; double-double residuals) against
   the FP64 solution of the same stored system at 1e-10, the FP64 reference being the
   FP64 LU with the same extra-precise refinement (the plain FP64 LU solution differs
   from it by up to ~kappa 1e-16, ~1e-10 at these conditions, and is checked at 1e-8);
@@ -60,12 +61,16 @@ def test_cube32_rows_solution_and_analytic(nu):
         x = q.solve_linear_system("fp32-ir", tol=1e-15, max_iter=60)
         info = dict(q.solve_info)
         u, _ = q.reorganize_solution()
+        xb = q.solve_linear_system("bf16-ir", tol=1e-12, max_iter=60)
+        info_b = dict(q.solve_info)
         xref = q.solve_linear_system("fp64-ir", tol=1e-15, max_iter=20)
         q.ghmat8()
         x64 = q.solve_linear_system("fp64")
         err = np.abs(x - xref).max() / np.abs(xref).max()
         assert err <= 1e-10, (nu, err, info)
         assert info["rel_residual"] <= 1e-14
+        errb = np.abs(xb - xref).max() / np.abs(xref).max()
+        assert errb <= 1e-10, (nu, errb, info_b)
         err64 = np.abs(x64 - xref).max() / np.abs(xref).max()
         assert err64 <= 1e-8, (nu, err64)
         P = mesh.node_coords()
