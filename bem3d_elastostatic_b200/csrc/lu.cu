@@ -227,9 +227,11 @@ __global__ void __launch_bounds__(panel_threads<T>(), 1)
 // into registers, updates them there and stores the lane's column back, so the step's
 // shared-memory accesses are independent of one another.  The operations are those of
 // the general loops; the step loop is not unrolled (the warp's code stays in the
-// instruction cache).  s_p[t] receives the local pivot of step t.
+// instruction cache).  s_p[t] receives the local pivot of step t; s_g (nullable, the
+// identity on entry) receives the interchanges composed into a gather: column b of the
+// factored window came from column s_g[b].
 template <typename T>
-__device__ __forceinline__ void window_lu_warp(T (*D)[kPanelW + 1], int* s_p, int lane) {
+__device__ __forceinline__ void window_lu_warp(T (*D)[kPanelW + 1], int* s_p, int lane, int* s_g = nullptr) {
   constexpr int W = kPanelW;
 #pragma unroll 1
   for (int t = 0; t < W; ++t) {
@@ -250,6 +252,11 @@ __device__ __forceinline__ void window_lu_warp(T (*D)[kPanelW + 1], int* s_p, in
         const T a = D[t][lane];
         D[t][lane] = D[p][lane];
         D[p][lane] = a;
+        if (s_g && lane == 0) {
+          const int gt = s_g[t];
+          s_g[t] = s_g[p];
+          s_g[p] = gt;
+        }
         __syncwarp();
         ct = D[lane][t];
         pv = D[t][t];
@@ -488,6 +495,191 @@ __global__ void __launch_bounds__(kBlockThreads) window_block_kernel(float* S, i
   }
 }
 
+// Grid barrier of a cooperative launch (bounded): every thread's earlier writes are
+// ordered before the arrival (CTA barrier, then thread 0's fence and release); the
+// wait gives up after wait_ns or once another CTA recorded an error, and records
+// BEM_ERR_TIMEOUT.  Returns false when the launch must stop.
+__device__ __forceinline__ bool coop_barrier(unsigned* barrier, unsigned target, int* status,
+                                             unsigned long long wait_ns, int* s_abort) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    red_release_add_u32(barrier, 1u);
+    const unsigned long long t0 = globaltimer_ns();
+    unsigned spins = 0;
+    int abort = 0;
+    while (ld_acquire_u32(barrier) < target) {
+      if ((++spins & 63u) == 0 && (globaltimer_ns() - t0 > wait_ns || *((volatile int*)status) != 0)) {
+        abort = 1;
+        break;
+      }
+      __nanosleep(32);
+    }
+    if (abort) atomicCAS(status, 0, BEM_ERR_TIMEOUT);
+    __threadfence();
+    *s_abort = abort;
+  }
+  __syncthreads();
+  return *s_abort == 0;
+}
+
+// The diagonal block [j0, t0)^2 of a window-pivoted FP32 panel in one cooperative
+// launch: the 32-wide sub-panels in turn, each in three phases separated by grid
+// barriers (two per sub-panel) instead of kernel boundaries:
+//   A  every CTA's warp 0 stages and factors the 32 x 32 window (redundantly; the
+//      interchanges composed into a gather on the way); CTA 0 records the pivots and
+//      the first exact zero pivot;
+//   B  the sub-panel's vectors, one thread each, spread over the CTAs in contiguous
+//      runs: every column c in [r0 + 32, t0) eliminated with the window's steps
+//      (window_panel_kernel's column operations), every row of the block outside the
+//      window gathered through the interchanges and, below the window, solved with
+//      the window's unit-lower triangle (trsm_small_kernel's operations);
+//   C  the rank-32 update of the block's trailing part, S(q, q) -= S(q, w) S(w, q)
+//      with q = [r0 + 32, t0) and w the window, in 64 x 64 tiles (FP32 FMA), and
+//      CTA 0 stores the factored window (every CTA has read it by now).
+// Every read of S goes through L2 (__ldcg): the other CTAs' writes of the previous
+// phase are ordered by the barrier, never by this SM's L1.  The rows and columns
+// outside the block follow per panel (permute_panel_kernel, the blocked TRSMs).
+constexpr int kCoopThreads = 256;
+constexpr int kCoopTile = 64;
+constexpr int kCoopMaxCtas = 64;
+__global__ void __launch_bounds__(kCoopThreads, 1)
+    panel_coop_kernel(float* S, int64_t lda, int j0, int t0, int* piv, unsigned* barrier, unsigned bar_base,
+                      int* status, unsigned long long wait_ns) {
+  constexpr int W = kPanelW;
+  constexpr int TP = kCoopTile + 4;  // strip pitch: 16-byte rows, 4-way store conflicts at most
+  __shared__ float D[W][W + 1];     // D[c][j] = S(r0 + j, r0 + c)
+  __shared__ int s_p[W], s_g[W];
+  __shared__ __align__(16) float Ls[W][TP];  // Ls[k][r] = S(q0 + tr + r, r0 + k)
+  __shared__ __align__(16) float Us[W][TP];  // Us[k][c] = S(r0 + k, q0 + tc + c)
+  __shared__ int s_abort;
+  const int G = gridDim.x, g = blockIdx.x, tid = threadIdx.x, lane = tid & 31;
+  unsigned target = bar_base;
+  for (int r0 = j0; r0 < t0; r0 += W) {
+    const int q0 = r0 + W, m = t0 - q0;
+    // A: the window
+    if (tid < W) {
+#pragma unroll 4
+      for (int cc = 0; cc < W; ++cc) D[cc][lane] = __ldcg(S + r0 + lane + (int64_t)(r0 + cc) * lda);
+      s_g[lane] = lane;
+      __syncwarp();
+      window_lu_warp<float>(D, s_p, lane, s_g);
+      if (g == 0) {
+        piv[r0 + lane] = r0 + s_p[lane];
+        if (lane == 0) {
+          for (int t = 0; t < W; ++t)
+            if (D[t][t] == 0.f) {
+              if (status[1] == 0) status[1] = r0 + t + 1;
+              break;
+            }
+        }
+      }
+    }
+    __syncthreads();
+    // B: columns [q0, t0), then rows [j0, r0) and [q0, t0)
+    {
+      const int nabove = r0 - j0;
+      const int nvec = m + nabove + m;
+      const int per = (nvec + G - 1) / G;
+      const int v0 = g * per, v1 = min(nvec, v0 + per);
+      for (int v = v0 + tid; v < v1; v += blockDim.x) {
+        if (v < m) {
+          float x[W];
+          float* col = S + r0 + (int64_t)(q0 + v) * lda;
+#pragma unroll
+          for (int q = 0; q < W / 4; ++q) {
+            const float4 f = __ldcg(reinterpret_cast<const float4*>(col) + q);
+            x[4 * q] = f.x;
+            x[4 * q + 1] = f.y;
+            x[4 * q + 2] = f.z;
+            x[4 * q + 3] = f.w;
+          }
+#pragma unroll
+          for (int t = 0; t < W; ++t) {
+            const float pv = D[t][t];
+            if (pv != 0.f) {
+              const float l = x[t] / pv;
+              x[t] = l;
+#pragma unroll
+              for (int j = t + 1; j < W; ++j) x[j] -= l * D[t][j];
+            }
+          }
+#pragma unroll
+          for (int q = 0; q < W / 4; ++q)
+            reinterpret_cast<float4*>(col)[q] = make_float4(x[4 * q], x[4 * q + 1], x[4 * q + 2], x[4 * q + 3]);
+        } else {
+          const int i = v - m;
+          const int r = i < nabove ? j0 + i : q0 + (i - nabove);
+          float y[W];
+#pragma unroll
+          for (int b = 0; b < W; ++b) y[b] = __ldcg(S + r + (int64_t)(r0 + s_g[b]) * lda);
+          if (r >= q0) {
+#pragma unroll
+            for (int b = 0; b < W; ++b) {
+              float a = y[b];
+#pragma unroll
+              for (int k = 0; k < b; ++k) a -= y[k] * D[b][k];  // U(k, b) = S(r0 + k, r0 + b)
+              y[b] = a;
+            }
+          }
+#pragma unroll
+          for (int b = 0; b < W; ++b) S[r + (int64_t)(r0 + b) * lda] = y[b];
+        }
+      }
+    }
+    target += (unsigned)G;
+    if (!coop_barrier(barrier, target, status, wait_ns, &s_abort)) return;
+    // C: the trailing tiles; CTA 0 stores the window
+    if (g == 0)
+      for (int i = tid; i < W * W; i += blockDim.x) {
+        const int j = i % W, cc = i / W;
+        S[r0 + j + (int64_t)(r0 + cc) * lda] = D[cc][j];
+      }
+    const int nt = (m + kCoopTile - 1) / kCoopTile;
+    for (int tau = g; tau < nt * nt; tau += G) {
+      const int tr = (tau % nt) * kCoopTile, tc = (tau / nt) * kCoopTile;
+      for (int i = tid; i < W * kCoopTile; i += blockDim.x) {
+        const int rr = i % kCoopTile, k = i / kCoopTile;
+        Ls[k][rr] = (tr + rr < m) ? __ldcg(S + q0 + tr + rr + (int64_t)(r0 + k) * lda) : 0.f;
+      }
+      for (int i = tid; i < W * kCoopTile; i += blockDim.x) {
+        const int k = i % W, cc = i / W;
+        Us[k][cc] = (tc + cc < m) ? __ldcg(S + r0 + k + (int64_t)(q0 + tc + cc) * lda) : 0.f;
+      }
+      __syncthreads();
+      const int ri = (tid % 16) * 4, ci = (tid / 16) * 4;
+      float acc[4][4] = {};
+#pragma unroll 8
+      for (int k = 0; k < W; ++k) {
+        const float4 a = *reinterpret_cast<const float4*>(&Ls[k][ri]);
+        const float4 b = *reinterpret_cast<const float4*>(&Us[k][ci]);
+        const float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int v = 0; v < 4; ++v) acc[u][v] = fmaf(av[u], bv[v], acc[u][v]);
+      }
+      // m is a multiple of 32: a 4-row group lies wholly inside or outside the block
+      if (tr + ri < m) {
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          if (tc + ci + v >= m) break;
+          float4* cp = reinterpret_cast<float4*>(S + q0 + tr + ri + (int64_t)(q0 + tc + ci + v) * lda);
+          float4 cv = __ldcg(cp);
+          cv.x -= acc[0][v];
+          cv.y -= acc[1][v];
+          cv.z -= acc[2][v];
+          cv.w -= acc[3][v];
+          *cp = cv;
+        }
+      }
+      __syncthreads();
+    }
+    target += (unsigned)G;
+    if (!coop_barrier(barrier, target, status, wait_ns, &s_abort)) return;
+  }
+}
+
 // Applies swaps k0+t <-> piv[k0+t] (t = 0..w-1 in order) to rows [a0,a1) and [b0,b1).
 // With window pivoting `win` (nullable) holds the factored w x w diagonal block of the
 // sub-panel (leading dimension kPanelW), which CTA 0 copies into S(k0.., k0..) first;
@@ -518,11 +710,13 @@ __global__ void swap_rows_kernel(T* S, int64_t lda, const int* piv, int k0, int 
   }
 }
 
-// A panel's interchanges (the swaps k0+t <-> piv[k0+t], t = 0..w-1 in order, w <= 512)
-// applied at once to rows [a0,a1) and [b0,b1) of S: they compose into a gather of the
-// panel's columns, x[k0 + c] := x[k0 + perm[c]], and only the columns the gather moves
-// are read and written.  A CTA takes 64 / sizeof(T) rows (32 KB of staged sources for
-// 512 moved columns); every source is read before any destination is written.
+// A window-pivoted panel's interchanges (the swaps k0+t <-> piv[k0+t], t = 0..w-1 in
+// order, w <= 512, every swap inside its 32-wide sub-panel) applied at once to rows
+// [a0,a1) and [b0,b1) of S: they compose into a gather of the panel's columns,
+// x[k0 + c] := x[k0 + perm[c]], and only the columns the gather moves are read and
+// written.  The sub-panels compose independently (one warp lane each, in parallel).
+// A CTA takes 64 / sizeof(T) rows (32 KB of staged sources for 512 moved columns);
+// every source is read before any destination is written.
 constexpr int kPermMax = 512;
 template <typename T>
 __global__ void __launch_bounds__(256) permute_panel_kernel(T* S, int64_t lda, const int* piv, int k0, int w, int a0,
@@ -530,23 +724,31 @@ __global__ void __launch_bounds__(256) permute_panel_kernel(T* S, int64_t lda, c
   constexpr int R = 64 / sizeof(T);  // rows per CTA
   __shared__ int perm[kPermMax];
   __shared__ int moved[kPermMax];
+  __shared__ int sp[kPermMax];
   __shared__ int nmoved;
   __shared__ T buf[kPermMax * R];
-  const int tid = threadIdx.x;
-  for (int c = tid; c < w; c += blockDim.x) perm[c] = c;
-  __syncthreads();
-  if (tid == 0) {
-    for (int t = 0; t < w; ++t) {
-      const int p = piv[k0 + t] - k0;
-      const int x = perm[t];
-      perm[t] = perm[p];
-      perm[p] = x;
-    }
-    int k = 0;
-    for (int c = 0; c < w; ++c)
-      if (perm[c] != c) moved[k++] = c;
-    nmoved = k;
+  const int tid = threadIdx.x, lane = tid & 31;
+  for (int c = tid; c < w; c += blockDim.x) {
+    perm[c] = c;
+    sp[c] = piv[k0 + c] - k0;
   }
+  if (tid == 0) nmoved = 0;
+  __syncthreads();
+  if (lane == 0) {
+    for (int g0 = (tid >> 5) * kPanelW; g0 < w; g0 += (int)(blockDim.x >> 5) * kPanelW) {
+      const int ge = min(w, g0 + kPanelW);
+      for (int t = g0; t < ge; ++t) {
+        const int p = sp[t];
+        const int x = perm[t];
+        perm[t] = perm[p];
+        perm[p] = x;
+      }
+    }
+  }
+  __syncthreads();
+  // the moved columns, in any order (a slot's source and destination stay paired)
+  for (int c = tid; c < w; c += blockDim.x)
+    if (perm[c] != c) moved[atomicAdd(&nmoved, 1)] = c;
   __syncthreads();
   const int nm = nmoved;
   if (nm == 0) return;
@@ -1150,6 +1352,13 @@ static int lu_factor_enqueue(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int
   cudaFuncSetAttribute(panel_inv_f32_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)(2 * kInvBlock * kInvBlock * sizeof(float)));
   int rc;
+  // window-pivoted FP32 panels: the diagonal block in one cooperative launch
+  // (panel_coop_kernel; BEM_PANEL_COOP=0 selects a launch pair per sub-panel)
+  static const bool coop_env = [] {
+    const char* e = getenv("BEM_PANEL_COOP");
+    return !(e && e[0] == '0');
+  }();
+  const int coop_g = std::min(kCoopMaxCtas, c->sm_count);
   for (int j0 = 0; j0 < n; j0 += nb) {
     const int jb = std::min(nb, n - j0);
     prof.panel = j0 / nb;
@@ -1157,7 +1366,24 @@ static int lu_factor_enqueue(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int
     // its diagonal block) to one blocked TRSM per panel; partial pivoting needs them
     // eliminated sub-panel by sub-panel to search them for pivots
     const int cend = (window && sizeof(T) == 4) ? j0 + jb : n;
-    for (int r0 = j0; r0 < j0 + jb; r0 += kPanelW) {
+    const bool coop = coop_env && cend < n && sizeof(T) == 4 && jb % kPanelW == 0 && lda % 4 == 0 &&
+                      (reinterpret_cast<uintptr_t>(S) & 15) == 0 && coop_g >= 1;
+    if (coop) {
+      prof.begin(0, c->stream);
+      float* Sf = reinterpret_cast<float*>(S);
+      int a_j0 = j0, a_t0 = j0 + jb;
+      unsigned bb = bar_base;
+      unsigned long long wns = c->wait_ns;
+      int* st = ws.status;
+      unsigned* bar = ws.barrier;
+      void* args[] = {&Sf, const_cast<int64_t*>(&lda), &a_j0, &a_t0, &piv, &bar, &bb, &st, &wns};
+      BEM_CUDA(c, cudaLaunchCooperativeKernel((void*)panel_coop_kernel, dim3(coop_g), dim3(kCoopThreads), args, 0,
+                                              c->stream));
+      ++c->launches;
+      bar_base += 2u * (unsigned)(jb / kPanelW) * (unsigned)coop_g;
+      prof.end(c->stream);
+    }
+    for (int r0 = j0; r0 < j0 + jb && !coop; r0 += kPanelW) {
       const int w = std::min(kPanelW, j0 + jb - r0);
       prof.begin(0, c->stream);
       if (cend < n && w == kPanelW && sizeof(T) == 4 && lda % 4 == 0 &&

@@ -37,17 +37,18 @@ constexpr int UK = 64;                  // K chunk per TMA box (128 bytes of BF1
 constexpr int kMaxK = 512;              // largest panel width
 constexpr int A_TILE = UM * UK * 2;     // 16 KB
 constexpr int B_TILE = UN * UK * 2;     // 32 KB
-// shared-memory ring of K chunks: three products stage hi + lo of A and B (96 KB) in
-// two stages, one product only the hi parts (48 KB) in four, 192 KB either way
-template <int NPROD>
-struct Ring {
-  static constexpr int stages = NPROD == 3 ? 2 : 4;
+// Shared memory: a ring of K chunks, then the barriers, then the epilogue's staging
+// boxes (128 x 32 FP32 each, NSTG per epilogue half).  Three products stage hi + lo of
+// A and B (96 KB a chunk); one product only the hi parts (48 KB).
+template <int NPROD, int STAGES, int NSTG>
+struct Cfg {
   static constexpr int stage = NPROD == 3 ? 2 * A_TILE + 2 * B_TILE : A_TILE + B_TILE;
+  static constexpr int ring = STAGES * stage;
+  static constexpr int box = 32 * UM * 4;
+  static constexpr int smem = ring + 1024 + 256 + 2 * NSTG * box;
+  static_assert(smem <= 227 * 1024, "shared memory");
+  static_assert((2 * STAGES + 5) * 8 <= 128, "barrier block");
 };
-constexpr int kRing = 2 * (2 * A_TILE + 2 * B_TILE);
-static_assert(Ring<1>::stages * Ring<1>::stage == kRing && Ring<3>::stages * Ring<3>::stage == kRing, "ring size");
-constexpr int kStg = 2 * 32 * UM * 4;  // two 128 x 32 FP32 staging boxes (one per epilogue half)
-constexpr int kSmem = kRing + 1024 + 256 + kStg;
 constexpr unsigned kTmemCols = 512;     // two 128 x 256 FP32 accumulators
 constexpr int kEpiThreads = 256;        // 8 epilogue warps
 constexpr int kThreads = 64 + kEpiThreads;
@@ -96,13 +97,14 @@ __device__ __forceinline__ void umma_commit(unsigned bar) {
 // warps 2-9 drain the other accumulator into C, so the update of C by one tile
 // overlaps the loads and MMAs of the next.  Tiles run m-fastest so a CTA wave shares
 // the B operand band.
-template <int NPROD>
+template <int NPROD, int STAGES, int NSTG>
 __global__ void __launch_bounds__(kThreads, 1)
     umma_update_kernel(const __grid_constant__ CUtensorMap tAh, const __grid_constant__ CUtensorMap tAl,
                        const __grid_constant__ CUtensorMap tBh, const __grid_constant__ CUtensorMap tBl,
                        const __grid_constant__ CUtensorMap tC, int M, int N, int K, int* err,
                        unsigned long long wait_ns) {
-  constexpr int kStages = Ring<NPROD>::stages, STAGE = Ring<NPROD>::stage;
+  using C_ = Cfg<NPROD, STAGES, NSTG>;
+  constexpr int kStages = STAGES, STAGE = C_::stage, kRing = C_::ring;
   extern __shared__ __align__(16) unsigned char umma_smem[];
   const unsigned raw = smem_u32(umma_smem);
   const unsigned base = (raw + 1023u) & ~1023u;  // 1024-byte aligned operand tiles
@@ -113,7 +115,6 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint64_t* tfull = bars + 2 * kStages;       // [2] MMA -> epilogue
   uint64_t* tempty = bars + 2 * kStages + 2;  // [2] epilogue -> MMA
   uint64_t* drain = bars + 2 * kStages + 4;   // MMA completion before teardown
-  static_assert((2 * kStages + 5) * 8 <= 128, "barrier block");
   unsigned* tmem_slot = reinterpret_cast<unsigned*>(gbase + kRing + 128);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(gbase + kRing + 136);
 
@@ -261,8 +262,8 @@ __global__ void __launch_bounds__(kThreads, 1)
     // that half's staging box and its leader thread issues the box's reduction
     const int lq = warp & 3;
     const int half = (warp - 2) >> 2;  // 0 or 1
-    float* stg = reinterpret_cast<float*>(gbase + kRing + 256) + half * (32 * UM);
-    const unsigned stg_s = smem_u32(stg);
+    float* stg0 = reinterpret_cast<float*>(gbase + kRing + 256) + half * NSTG * (32 * UM);
+    int bx = 0;  // boxes this half has staged: box bx uses buffer bx % NSTG
     const bool leader = (lq == 0 && lane == 0);
     int ab = 0;
     unsigned aphase = 0;
@@ -298,8 +299,12 @@ __global__ void __launch_bounds__(kThreads, 1)
               "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
             : "r"(taddr)
             : "memory");
-        // the half's previous box must have been read out of shared memory
-        if (leader && pending) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+        // the box that last used this buffer must have been read out of shared memory
+        // (bulk groups complete in order: at most NSTG - 1 newer ones may still read)
+        float* stg = stg0 + (bx % NSTG) * (32 * UM);
+        const unsigned stg_s = smem_u32(stg);
+        ++bx;
+        if (leader && pending) asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(NSTG - 1) : "memory");
         asm volatile("bar.sync %0, 128;" ::"r"(1 + half) : "memory");
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
         const int rr = lq * 32 + lane;
@@ -414,10 +419,23 @@ int gemm_umma_bf16(bem_ctx* c, int M, int N, int K, const float* A, int64_t lda,
       return bem_fail(c, BEM_ERR_CUDA, "cuTensorMapEncodeTiled not available");
     g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
   }
+  // one product: three ring stages and two staging boxes per epilogue half
+  // (BEM_UMMA_RING=4: four stages, one box); three products: two stages, one box
+  static const bool ring4 = [] {
+    const char* e = getenv("BEM_UMMA_RING");
+    return e && e[0] == '4';
+  }();
+  using K1a = Cfg<1, 3, 2>;
+  using K1b = Cfg<1, 4, 1>;
+  using K3 = Cfg<3, 2, 1>;
   static DeviceOnce attr;  // the kernel attribute is per device
   if (attr.pending()) {
-    BEM_CUDA(c, cudaFuncSetAttribute(umma_update_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem));
-    BEM_CUDA(c, cudaFuncSetAttribute(umma_update_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem));
+    BEM_CUDA(c, cudaFuncSetAttribute(umma_update_kernel<1, 3, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     K1a::smem));
+    BEM_CUDA(c, cudaFuncSetAttribute(umma_update_kernel<1, 4, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     K1b::smem));
+    BEM_CUDA(c, cudaFuncSetAttribute(umma_update_kernel<3, 2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     K3::smem));
     attr.mark();
   }
   const size_t na = (size_t)M * K, nb_ = (size_t)N * K;
@@ -460,11 +478,14 @@ int gemm_umma_bf16(bem_ctx* c, int M, int N, int K, const float* A, int64_t lda,
   }
   const int grid = (int)std::min<int64_t>(tiles, c->sm_count);
   if (nprod == 3)
-    umma_update_kernel<3><<<grid, kThreads, kSmem, c->stream>>>(mAh, mAl, mBh, mBl, mC, M, N, K, c->umma_err.p,
-                                                                c->wait_ns);
+    umma_update_kernel<3, 2, 1><<<grid, kThreads, K3::smem, c->stream>>>(mAh, mAl, mBh, mBl, mC, M, N, K,
+                                                                         c->umma_err.p, c->wait_ns);
+  else if (ring4)
+    umma_update_kernel<1, 4, 1><<<grid, kThreads, K1b::smem, c->stream>>>(mAh, mAl, mBh, mBl, mC, M, N, K,
+                                                                          c->umma_err.p, c->wait_ns);
   else
-    umma_update_kernel<1><<<grid, kThreads, kSmem, c->stream>>>(mAh, mAl, mBh, mBl, mC, M, N, K, c->umma_err.p,
-                                                                c->wait_ns);
+    umma_update_kernel<1, 3, 2><<<grid, kThreads, K1a::smem, c->stream>>>(mAh, mAl, mBh, mBl, mC, M, N, K,
+                                                                          c->umma_err.p, c->wait_ns);
   BEM_LAUNCH_CHECK(c);
   return BEM_OK;
 }
