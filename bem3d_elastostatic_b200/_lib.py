@@ -40,6 +40,7 @@ BEM_OPT_PIVOTING = 1
 BEM_OPT_WAIT_LIMIT_MS = 2
 BEM_OPT_WITHHOLD_BLOCK = 3
 BEM_OPT_RESIDUAL = 4
+BEM_OPT_PANEL_WIDTH = 5
 
 # every symbol the header declares, for the export check
 EXPORTS = [
@@ -204,7 +205,8 @@ class Context:
         self.check(self.L.bem_sync(self.h), "sync")
 
     def set_option(self, option: int, value: int):
-        """bem_set_option: BEM_OPT_PIVOTING, BEM_OPT_WAIT_LIMIT_MS, BEM_OPT_WITHHOLD_BLOCK."""
+        """bem_set_option: BEM_OPT_PIVOTING, BEM_OPT_WAIT_LIMIT_MS, BEM_OPT_WITHHOLD_BLOCK,
+        BEM_OPT_RESIDUAL, BEM_OPT_PANEL_WIDTH."""
         self.check(self.L.bem_set_option(self.h, int(option), int(value)), "set_option")
 
     def profile_begin(self, timing=True):

@@ -209,6 +209,7 @@ struct bem_ctx {
   // sweep block (BEM_OPT_WITHHOLD_BLOCK, -1 = none)
   unsigned long long wait_ns = 2000000000ull;
   int withhold_block = -1;
+  int panel_width = 0;  // FP32 factorisation panel width of the *_IR modes (0: the mode's own)
   int f32_gemm_override = -1;  // BEM_F32_GEMM environment override (0, 1, 3)
   // tcgen05 trailing update: BF16 hi/lo operand copies and its error word
   bem::DBuf<unsigned long long> ip_counters;  // internal points: far and near evaluations

@@ -163,6 +163,11 @@ int bem_set_option(bem_ctx* c, int option, int64_t value) {
       if (value != 0 && value != 1) return bem_fail(c, BEM_ERR_ARG, "set_option: residual must be 0 or 1");
       c->ext_residual = value == 1;
       return BEM_OK;
+    case BEM_OPT_PANEL_WIDTH:
+      if (value != 0 && (value < 128 || value > 1024 || value % 128 != 0))
+        return bem_fail(c, BEM_ERR_ARG, "set_option: panel width must be 0 or a multiple of 128 up to 1024");
+      c->panel_width = (int)value;
+      return BEM_OK;
     case BEM_OPT_WITHHOLD_BLOCK:
       if (value < -1 || value > INT32_MAX) return bem_fail(c, BEM_ERR_ARG, "set_option: bad block index");
       c->withhold_block = (int)value;

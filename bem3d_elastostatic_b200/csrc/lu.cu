@@ -711,12 +711,13 @@ __global__ void swap_rows_kernel(T* S, int64_t lda, const int* piv, int k0, int 
 }
 
 // A window-pivoted panel's interchanges (the swaps k0+t <-> piv[k0+t], t = 0..w-1 in
-// order, w <= 512, every swap inside its 32-wide sub-panel) applied at once to rows
-// [a0,a1) and [b0,b1) of S: they compose into a gather of the panel's columns,
+// order, every swap inside its 32-wide sub-panel) applied at once to rows [a0,a1) and
+// [b0,b1) of S: they compose into a gather of the panel's columns,
 // x[k0 + c] := x[k0 + perm[c]], and only the columns the gather moves are read and
-// written.  The sub-panels compose independently (one warp lane each, in parallel).
-// A CTA takes 64 / sizeof(T) rows (32 KB of staged sources for 512 moved columns);
-// every source is read before any destination is written.
+// written.  The panel goes in chunks of up to 512 columns (no swap crosses a chunk);
+// within a chunk the sub-panels compose independently (one warp lane each, in
+// parallel).  A CTA takes 64 / sizeof(T) rows (32 KB of staged sources for 512 moved
+// columns); every source of a chunk is read before any destination is written.
 constexpr int kPermMax = 512;
 template <typename T>
 __global__ void __launch_bounds__(256) permute_panel_kernel(T* S, int64_t lda, const int* piv, int k0, int w, int a0,
@@ -728,40 +729,45 @@ __global__ void __launch_bounds__(256) permute_panel_kernel(T* S, int64_t lda, c
   __shared__ int nmoved;
   __shared__ T buf[kPermMax * R];
   const int tid = threadIdx.x, lane = tid & 31;
-  for (int c = tid; c < w; c += blockDim.x) {
-    perm[c] = c;
-    sp[c] = piv[k0 + c] - k0;
-  }
-  if (tid == 0) nmoved = 0;
-  __syncthreads();
-  if (lane == 0) {
-    for (int g0 = (tid >> 5) * kPanelW; g0 < w; g0 += (int)(blockDim.x >> 5) * kPanelW) {
-      const int ge = min(w, g0 + kPanelW);
-      for (int t = g0; t < ge; ++t) {
-        const int p = sp[t];
-        const int x = perm[t];
-        perm[t] = perm[p];
-        perm[p] = x;
-      }
-    }
-  }
-  __syncthreads();
-  // the moved columns, in any order (a slot's source and destination stay paired)
-  for (int c = tid; c < w; c += blockDim.x)
-    if (perm[c] != c) moved[atomicAdd(&nmoved, 1)] = c;
-  __syncthreads();
-  const int nm = nmoved;
-  if (nm == 0) return;
   const int na = a1 - a0;
   const int rr = tid % R, slot = tid / R, nslot = blockDim.x / R;
   const int64_t i = (int64_t)blockIdx.x * R + rr;
   const bool ok = i < (int64_t)na + (b1 - b0);
   const int64_t r = ok ? ((i < na) ? a0 + i : b0 + (i - na)) : 0;
-  for (int q = slot; q < nm; q += nslot)
-    if (ok) buf[q * R + rr] = S[r + (int64_t)(k0 + perm[moved[q]]) * lda];
-  __syncthreads();
-  for (int q = slot; q < nm; q += nslot)
-    if (ok) S[r + (int64_t)(k0 + moved[q]) * lda] = buf[q * R + rr];
+  for (int h0 = 0; h0 < w; h0 += kPermMax) {
+    const int hw = min(kPermMax, w - h0), kh = k0 + h0;
+    for (int c = tid; c < hw; c += blockDim.x) {
+      perm[c] = c;
+      sp[c] = piv[kh + c] - kh;
+    }
+    if (tid == 0) nmoved = 0;
+    __syncthreads();
+    if (lane == 0) {
+      for (int g0 = (tid >> 5) * kPanelW; g0 < hw; g0 += (int)(blockDim.x >> 5) * kPanelW) {
+        const int ge = min(hw, g0 + kPanelW);
+        for (int t = g0; t < ge; ++t) {
+          const int p = sp[t];
+          const int x = perm[t];
+          perm[t] = perm[p];
+          perm[p] = x;
+        }
+      }
+    }
+    __syncthreads();
+    // the moved columns, in any order (a slot's source and destination stay paired)
+    for (int c = tid; c < hw; c += blockDim.x)
+      if (perm[c] != c) moved[atomicAdd(&nmoved, 1)] = c;
+    __syncthreads();
+    const int nm = nmoved;  // uniform in the CTA
+    if (nm > 0) {
+      for (int q = slot; q < nm; q += nslot)
+        if (ok) buf[q * R + rr] = S[r + (int64_t)(kh + perm[moved[q]]) * lda];
+      __syncthreads();
+      for (int q = slot; q < nm; q += nslot)
+        if (ok) S[r + (int64_t)(kh + moved[q]) * lda] = buf[q * R + rr];
+    }
+    __syncthreads();  // perm, moved and buf are reused by the next chunk
+  }
 }
 
 // Y := X * U^{-1} in place for rows [r_lo, r_hi), X = S(rows, k0..k0+w), U the unit
@@ -1273,13 +1279,13 @@ static size_t up256(size_t b) { return (b + 255) / 256 * 256; }
 
 // blocks of the TRSM-inverse region: FP32 factors keep the 2 x 4 inverses of a
 // window-pivoted 512-wide panel (panel_inv_f32_kernel), FP64 one block
-static size_t inv_blocks(int elem) { return elem == 4 ? 8 : 1; }
+static size_t inv_blocks(int elem, int nb) { return elem == 4 ? 2 * (size_t)((nb + kInvBlock - 1) / kInvBlock) : 1; }
 
 size_t lu_workspace_bytes(int n, int nb, int gmax, int elem) {
   const size_t ldy = ((size_t)n + 31) / 32 * 32;
   return up256(2 * (size_t)gmax * sizeof(double)) + up256(2 * (size_t)gmax * sizeof(int)) +
          up256(2 * (size_t)gmax * kPanelW * elem) + up256(2 * (size_t)kPanelW * elem) + up256(16) +
-         up256(inv_blocks(elem) * kInvBlock * kInvBlock * elem) + up256(ldy * nb * elem);
+         up256(inv_blocks(elem, nb) * kInvBlock * kInvBlock * elem) + up256(ldy * nb * elem);
 }
 
 LUWorkspace lu_workspace_carve(void* base, int n, int nb, int gmax, int elem) {
@@ -1299,7 +1305,7 @@ LUWorkspace lu_workspace_carve(void* base, int n, int nb, int gmax, int elem) {
   w.status = reinterpret_cast<int*>(p + 8);
   p += up256(16);
   w.inv = p;
-  p += up256(inv_blocks(elem) * kInvBlock * kInvBlock * elem);
+  p += up256(inv_blocks(elem, nb) * kInvBlock * kInvBlock * elem);
   w.ybuf = p;
   return w;
 }
@@ -1386,7 +1392,7 @@ static int lu_factor_enqueue(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int
     for (int r0 = j0; r0 < j0 + jb && !coop; r0 += kPanelW) {
       const int w = std::min(kPanelW, j0 + jb - r0);
       prof.begin(0, c->stream);
-      if (cend < n && w == kPanelW && sizeof(T) == 4 && lda % 4 == 0 &&
+      if (cend < n && w == kPanelW && jb <= kBlockThreads && sizeof(T) == 4 && lda % 4 == 0 &&
           (reinterpret_cast<uintptr_t>(S) & 15) == 0) {
         // window-pivoted FP32 panel: the sub-panel's step in one CTA, then its GEMM
         window_block_kernel<<<1, kBlockThreads, 0, c->stream>>>(reinterpret_cast<float*>(S), lda, j0, j0 + jb, r0, piv,
@@ -1446,8 +1452,9 @@ static int lu_factor_enqueue(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int
     }
     if (t0 < n) {
       const int m = n - t0;
-      T* Vu = V;                                        // [4][128 x 128]
-      T* Wl = V + (size_t)(kInvBlock * kInvBlock) * 4;  // [4][128 x 128]
+      const int nib = (nb + kInvBlock - 1) / kInvBlock;
+      T* Vu = V;                                          // [nib][128 x 128]
+      T* Wl = V + (size_t)(kInvBlock * kInvBlock) * nib;  // [nib][128 x 128]
       if (blocked) {
         // the panel's diagonal-block inverses, then the rest of the sub-panels' columns:
         // B = S(j0..t0, t0..n) := W^{-1} B with W the lower triangle of the diagonal

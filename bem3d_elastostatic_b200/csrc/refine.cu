@@ -14,7 +14,8 @@ namespace bem {
 // panel width of the FP32 factorisation: at 512 the tcgen05 trailing update has as much
 // tensor work per tile as C traffic (measured at 73,734 DOF: 1.79 s per bench step at 256,
 // 1.61 s at 384, 1.58 s at 512)
-constexpr int kNbMixed = 512;
+constexpr int kNbMixed = 512;   // panel width of the FP32 factors of BEM_PREC_FP32_IR
+constexpr int kNbBf16 = 1024;   // and of BEM_PREC_BF16_IR
 constexpr int kNbFp64IR = 512;  // panel width of the FP64 factors of BEM_PREC_FP64_IR
 
 __global__ void to_fp32_kernel(const double* A, int64_t lda, int n, float* A32) {
@@ -248,11 +249,10 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
     c->f32_gemm = c->f32_gemm_override;
   else
     c->f32_gemm = (precision == BEM_PREC_BF16_IR) ? 2 : 4;
-  int nb = kNbMixed;
-  if (const char* e = getenv("BEM_LU_NB")) {  // panel width override: 128, 256, 384 or 512
-    const int v = atoi(e);
-    if (v >= 128 && v <= 512 && v % 128 == 0) nb = v;
-  }
+  // the one-product update is HBM-bound (the FP32 trailing matrix is read and written
+  // once per panel): the wider panel halves that traffic; the three-product update is
+  // tensor-bound
+  const int nb = c->panel_width > 0 ? c->panel_width : (precision == BEM_PREC_BF16_IR ? kNbBf16 : kNbMixed);
   stamp("enqueued");
   c->lu_window = window;
   rc = dbl ? lu_factor<double>(c, c->A64f.p, lda, n, c->piv.p, c->perm.p, kNbFp64IR, info)

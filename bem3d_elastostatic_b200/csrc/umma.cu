@@ -34,7 +34,7 @@ namespace {
 constexpr int UM = 128;                 // tile rows (UMMA M)
 constexpr int UN = 256;                 // tile columns (UMMA N)
 constexpr int UK = 64;                  // K chunk per TMA box (128 bytes of BF16)
-constexpr int kMaxK = 512;              // largest panel width
+constexpr int kMaxK = 1024;             // largest panel width
 constexpr int A_TILE = UM * UK * 2;     // 16 KB
 constexpr int B_TILE = UN * UK * 2;     // 32 KB
 // Shared memory: a ring of K chunks, then the barriers, then the epilogue's staging
@@ -411,7 +411,7 @@ int umma_reserve(bem_ctx* c, int M, int N, int K) {
 int gemm_umma_bf16(bem_ctx* c, int M, int N, int K, const float* A, int64_t lda, const float* B, int64_t ldb,
                    float* C, int64_t ldc, int nprod) {
   if (nprod != 1 && nprod != 3) return bem_fail(c, BEM_ERR_ARG, "umma: nprod must be 1 or 3");
-  if (!umma_supported(K)) return bem_fail(c, BEM_ERR_ARG, "umma: K must be a multiple of 64 up to 512");
+  if (!umma_supported(K)) return bem_fail(c, BEM_ERR_ARG, "umma: K must be a multiple of 64 up to 1024");
   if (!g_encode) {
     cudaDriverEntryPointQueryResult q;
     void* fn = nullptr;

@@ -546,6 +546,8 @@ def run_case(args):
     q = Quadesth(mesh)
     if args.pivoting == "partial":
         q.set_option(_lib.BEM_OPT_PIVOTING, _lib.BEM_PIVOT_PARTIAL)
+    if args.panel_width:
+        q.set_option(_lib.BEM_OPT_PANEL_WIDTH, args.panel_width)
     q.precompute_element_geometry()
     q.ghmat8()
     x = q.solve_linear_system(args.case_precision, tol=1e-15, max_iter=60)
@@ -574,6 +576,8 @@ def run_gpu(args, ws, rank, local):
     q = Quadesth(mesh, device=local)
     if args.pivoting == "partial":
         q.set_option(_lib.BEM_OPT_PIVOTING, _lib.BEM_PIVOT_PARTIAL)
+    if args.panel_width:
+        q.set_option(_lib.BEM_OPT_PANEL_WIDTH, args.panel_width)
     stream = torch.cuda.ExternalStream(q.ctx.stream(), device=local)
 
     def step(precision):
@@ -844,6 +848,8 @@ def main():
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--precision", default="bf16-ir", choices=["fp32-ir", "bf16-ir"])
     ap.add_argument("--pivoting", default="window", choices=["window", "partial"])
+    ap.add_argument("--panel-width", type=int, default=0,
+                    help="FP32 factorisation panel width (multiple of 128 up to 1024; 0: the mode's own)")
     # refinement to a backward error of 1e-12 with the last correction below 1e-12 of x
     # (double-double residuals): the forward error against the solution of the stored
     # FP64 system is then ~1e-13, reported as rel_err_vs_fp64_ir

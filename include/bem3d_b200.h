@@ -117,11 +117,15 @@ int bem_get_stream(bem_ctx* ctx, void** stream);
  *                           sweep of the next solves does not publish this 128-row block
  *                           (-1, the default, publishes all), so that the waits for it run
  *                           out and the solve returns BEM_ERR_TIMEOUT with the context
- *                           still usable */
+ *                           still usable
+ *   BEM_OPT_PANEL_WIDTH     panel width of the FP32 factorisations of the *_IR modes: a
+ *                           multiple of 128 up to 1024, or 0 (default) for the mode's
+ *                           own (1024 for BEM_PREC_BF16_IR, 512 for BEM_PREC_FP32_IR) */
 #define BEM_OPT_PIVOTING 1
 #define BEM_OPT_WAIT_LIMIT_MS 2
 #define BEM_OPT_WITHHOLD_BLOCK 3
 #define BEM_OPT_RESIDUAL 4
+#define BEM_OPT_PANEL_WIDTH 5
 int bem_set_option(bem_ctx* ctx, int option, int64_t value);
 
 /* Input: replaces input_data (io_mod.f90:36-146) and update_material_constants

@@ -26,13 +26,17 @@ def cube8_ref(cube8_mesh):
     return O.Oracle(cube8_mesh).run()
 
 
+@pytest.mark.parametrize("panel_width", [0, 512, 1024])
 @pytest.mark.parametrize("pivoting", [_lib.BEM_PIVOT_WINDOW, _lib.BEM_PIVOT_PARTIAL])
 @pytest.mark.parametrize("precision", ["fp32-ir", "bf16-ir"])
-def test_pivoting_modes_vs_oracle(pivoting, precision, cube8_mesh, cube8_ref):
+def test_pivoting_modes_vs_oracle(pivoting, precision, panel_width, cube8_mesh, cube8_ref):
+    """Both pivotings, both mixed modes, the modes' own panel widths and both explicit
+    ones (4,614 DOF: 9 or 4 full panels and a partial last one)."""
     from bem3d_elastostatic_b200.api import Quadesth
 
     q = Quadesth(cube8_mesh)
     q.set_option(_lib.BEM_OPT_PIVOTING, pivoting)
+    q.set_option(_lib.BEM_OPT_PANEL_WIDTH, panel_width)
     q.precompute_element_geometry()
     q.ghmat8()
     x = q.solve_linear_system(precision, tol=1e-15, max_iter=60)
@@ -93,6 +97,9 @@ def test_set_option_rejects_bad_values():
     assert L.bem_set_option(h, _lib.BEM_OPT_WAIT_LIMIT_MS, 0) == _lib.BEM_ERR_ARG
     assert L.bem_set_option(h, _lib.BEM_OPT_WAIT_LIMIT_MS, 60001) == _lib.BEM_ERR_ARG
     assert L.bem_set_option(h, 99, 0) == _lib.BEM_ERR_ARG
+    for bad in (64, 100, 1152, -128):
+        assert L.bem_set_option(h, _lib.BEM_OPT_PANEL_WIDTH, bad) == _lib.BEM_ERR_ARG
+    assert L.bem_set_option(h, _lib.BEM_OPT_PANEL_WIDTH, 768) == 0
     assert L.bem_set_option(h, _lib.BEM_OPT_WAIT_LIMIT_MS, 500) == 0
     ctx.close()
 
