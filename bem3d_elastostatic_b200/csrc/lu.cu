@@ -282,6 +282,83 @@ __device__ __forceinline__ void window_lu_warp(T (*D)[kPanelW + 1], int* s_p, in
   }
 }
 
+// v[t] for a warp-uniform runtime t, by a five-level multiplexer (31 selects, depth 5):
+// the array stays in registers.
+__device__ __forceinline__ float pick32(const float (&v)[kPanelW], int t) {
+  float a[16], b[8], c[4], d[2];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) a[k] = (t & 1) ? v[2 * k + 1] : v[2 * k];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) b[k] = (t & 2) ? a[2 * k + 1] : a[2 * k];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) c[k] = (t & 4) ? b[2 * k + 1] : b[2 * k];
+#pragma unroll
+  for (int k = 0; k < 2; ++k) d[k] = (t & 8) ? c[2 * k + 1] : c[2 * k];
+  return (t & 16) ? d[1] : d[0];
+}
+
+// window_lu_warp for a full FP32 window with lane c's column in registers (v[j] =
+// D[c][j] on entry and on exit): per step the candidate entry comes from the registers
+// through pick32, the pivot column is broadcast by shuffles, and an interchange moves
+// the two lanes' whole columns (and their original indices) by shuffles.  The pivot
+// rule (largest magnitude among lanes >= t, ties to the smallest index, after a vote
+// on whether any lane beats the diagonal) and the arithmetic (one IEEE division and
+// one fused multiply-add per entry) are window_lu_warp's.  s_p[t] receives step t's
+// local pivot; s_g[b] the original window column of factored column b.
+__device__ __forceinline__ void window_lu_warp_f32(float (*D)[kPanelW + 1], int* s_p, int* s_g, int lane) {
+  constexpr int W = kPanelW;
+  constexpr unsigned FULL = 0xffffffffu;
+  float v[W];
+#pragma unroll
+  for (int j = 0; j < W; ++j) v[j] = D[lane][j];
+  int g = lane;
+#pragma unroll 1
+  for (int t = 0; t < W; ++t) {
+    float ct = pick32(v, t);
+    float pv = __shfl_sync(FULL, ct, t);
+    int p = t;
+    if (__any_sync(FULL, lane > t && fabsf(ct) > fabsf(pv))) {
+      float bv = (lane >= t) ? fabsf(ct) : -1.f;
+      int bc = (lane >= t) ? lane : INT_MAX;
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const float ov = __shfl_xor_sync(FULL, bv, off);
+        const int oc = __shfl_xor_sync(FULL, bc, off);
+        if (ov > bv || (ov == bv && oc < bc)) {
+          bv = ov;
+          bc = oc;
+        }
+      }
+      p = bc;
+      if (p != t) {  // lanes t and p exchange their columns
+        const int src = (lane == t) ? p : ((lane == p) ? t : lane);
+#pragma unroll
+        for (int j = 0; j < W; ++j) v[j] = __shfl_sync(FULL, v[j], src);
+        g = __shfl_sync(FULL, g, src);
+        ct = __shfl_sync(FULL, ct, src);
+        pv = __shfl_sync(FULL, ct, t);
+      }
+    }
+    if (lane == 0) s_p[t] = p;
+    float pr[W];
+#pragma unroll
+    for (int j = 0; j < W; ++j)
+      if (j > t) pr[j] = __shfl_sync(FULL, v[j], t);  // t is warp-uniform
+    if (pv != 0.f && lane > t) {
+      const float l = ct / pv;
+#pragma unroll
+      for (int j = 0; j < W; ++j) {
+        if (j > t) v[j] -= l * pr[j];
+        if (j == t) v[j] = l;
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < W; ++j) D[lane][j] = v[j];
+  s_g[lane] = g;
+  __syncwarp();
+}
+
 // Window pivoting: the sub-panel's pivot search is restricted to its w x w diagonal
 // block (T rows r0..r0+w), so the sub-panel needs no grid-wide exchange.  Every CTA
 // factors that block redundantly in shared memory (warp 0: lane c owns column c of the
@@ -559,11 +636,13 @@ __global__ void __launch_bounds__(kCoopThreads, 1)
     const int q0 = r0 + W, m = t0 - q0;
     // A: the window
     if (tid < W) {
-#pragma unroll 4
-      for (int cc = 0; cc < W; ++cc) D[cc][lane] = __ldcg(S + r0 + lane + (int64_t)(r0 + cc) * lda);
-      s_g[lane] = lane;
+      float wv[W];  // every load in flight before the first store
+#pragma unroll
+      for (int cc = 0; cc < W; ++cc) wv[cc] = __ldcg(S + r0 + lane + (int64_t)(r0 + cc) * lda);
+#pragma unroll
+      for (int cc = 0; cc < W; ++cc) D[cc][lane] = wv[cc];
       __syncwarp();
-      window_lu_warp<float>(D, s_p, lane, s_g);
+      window_lu_warp_f32(D, s_p, s_g, lane);
       if (g == 0) {
         piv[r0 + lane] = r0 + s_p[lane];
         if (lane == 0) {
@@ -638,16 +717,35 @@ __global__ void __launch_bounds__(kCoopThreads, 1)
     const int nt = (m + kCoopTile - 1) / kCoopTile;
     for (int tau = g; tau < nt * nt; tau += G) {
       const int tr = (tau % nt) * kCoopTile, tc = (tau / nt) * kCoopTile;
-      for (int i = tid; i < W * kCoopTile; i += blockDim.x) {
+      const int ri = (tid % 16) * 4, ci = (tid / 16) * 4;
+      // every load of the tile in flight before the first use: the strips, then C
+      constexpr int NS = W * kCoopTile / kCoopThreads;
+      float lv[NS], uv[NS];
+#pragma unroll
+      for (int u = 0; u < NS; ++u) {
+        const int i = tid + u * kCoopThreads;
         const int rr = i % kCoopTile, k = i / kCoopTile;
-        Ls[k][rr] = (tr + rr < m) ? __ldcg(S + q0 + tr + rr + (int64_t)(r0 + k) * lda) : 0.f;
+        lv[u] = (tr + rr < m) ? __ldcg(S + q0 + tr + rr + (int64_t)(r0 + k) * lda) : 0.f;
       }
-      for (int i = tid; i < W * kCoopTile; i += blockDim.x) {
+#pragma unroll
+      for (int u = 0; u < NS; ++u) {
+        const int i = tid + u * kCoopThreads;
         const int k = i % W, cc = i / W;
-        Us[k][cc] = (tc + cc < m) ? __ldcg(S + r0 + k + (int64_t)(q0 + tc + cc) * lda) : 0.f;
+        uv[u] = (tc + cc < m) ? __ldcg(S + r0 + k + (int64_t)(q0 + tc + cc) * lda) : 0.f;
+      }
+      float4 cv[4];
+#pragma unroll
+      for (int v = 0; v < 4; ++v)
+        cv[v] = (tr + ri < m && tc + ci + v < m)
+                    ? __ldcg(reinterpret_cast<const float4*>(S + q0 + tr + ri + (int64_t)(q0 + tc + ci + v) * lda))
+                    : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+      for (int u = 0; u < NS; ++u) {
+        const int i = tid + u * kCoopThreads;
+        Ls[i / kCoopTile][i % kCoopTile] = lv[u];
+        Us[i % W][i / W] = uv[u];
       }
       __syncthreads();
-      const int ri = (tid % 16) * 4, ci = (tid / 16) * 4;
       float acc[4][4] = {};
 #pragma unroll 8
       for (int k = 0; k < W; ++k) {
@@ -663,14 +761,14 @@ __global__ void __launch_bounds__(kCoopThreads, 1)
       if (tr + ri < m) {
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
-          if (tc + ci + v >= m) break;
-          float4* cp = reinterpret_cast<float4*>(S + q0 + tr + ri + (int64_t)(q0 + tc + ci + v) * lda);
-          float4 cv = __ldcg(cp);
-          cv.x -= acc[0][v];
-          cv.y -= acc[1][v];
-          cv.z -= acc[2][v];
-          cv.w -= acc[3][v];
-          *cp = cv;
+          if (tc + ci + v < m) {
+            float4 o = cv[v];
+            o.x -= acc[0][v];
+            o.y -= acc[1][v];
+            o.z -= acc[2][v];
+            o.w -= acc[3][v];
+            *reinterpret_cast<float4*>(S + q0 + tr + ri + (int64_t)(q0 + tc + ci + v) * lda) = o;
+          }
         }
       }
       __syncthreads();
@@ -1101,10 +1199,14 @@ bool gemm_tc_ok(const void* A, int64_t lda, const void* B, int64_t ldb, int elem
 bool umma_supported(int K);
 int umma_reserve(bem_ctx* c, int M, int N, int K);
 int gemm_umma_bf16(bem_ctx* c, int M, int N, int K, const float* A, int64_t lda, const float* B, int64_t ldb,
-                   float* C, int64_t ldc, int nprod);
+                   float* C, int64_t ldc, int nprod, bool store);
 
 // the FP32 trailing updates of this context run on tcgen05 (umma.cu)
 static bool uses_umma(const bem_ctx* c) { return c->f32_gemm == 4 || c->f32_gemm == 2; }
+// C as the tcgen05 epilogue's bulk tensor copies need it: 16-byte aligned base and column stride
+static bool umma_c_ok(const void* C, int64_t ldc) {
+  return (reinterpret_cast<uintptr_t>(C) & 15) == 0 && (ldc * 4) % 16 == 0;
+}
 
 template <typename T>
 static int gemm_simt(bem_ctx* c, int M, int N, int K, const T* A, int64_t lda, const T* B, int64_t ldb, T* C,
@@ -1119,9 +1221,10 @@ static int gemm_simt(bem_ctx* c, int M, int N, int K, const T* A, int64_t lda, c
 }
 
 // FP64: DMMA tensor path; FP32: per-context choice (c->f32_gemm) of the BF16 tensor path
-// with 3 (FP32-grade) or 1 (plain BF16) terms, or SIMT FP32; the trailing updates (K a
-// multiple of 64, M >= 128, N >= 256) run on tcgen05 with 3 terms (f32_gemm 4) or one
-// (f32_gemm 2, the other GEMMs keeping 3).  Misaligned operands take the SIMT kernel.
+// with 3 (FP32-grade) or 1 (plain BF16) terms, or SIMT FP32.  With tcgen05 (f32_gemm 4
+// or 2), GEMMs with K a multiple of 64, M >= 128 and N >= 256 run there with 3 terms
+// (mode 0, C -= A B, and mode 1, C = A B); the trailing updates take trailing_gemm,
+// which gives f32_gemm 2 its one-term update.  Misaligned operands take the SIMT kernel.
 template <typename T>
 int gemm(bem_ctx* c, int M, int N, int K, const T* A, int64_t lda, const T* B, int64_t ldb, T* C, int64_t ldc,
          int mode) {
@@ -1132,14 +1235,22 @@ int gemm(bem_ctx* c, int M, int N, int K, const T* A, int64_t lda, const T* B, i
     if (tc && c->f64_gemm == 1)
       return gemm_dmma(c, M, N, K, (const double*)A, lda, (const double*)B, ldb, (double*)C, ldc, mode);
   } else {
-    if (uses_umma(c) && mode == 0 && umma_supported(K) && M >= 128 && N >= 256)
-      return gemm_umma_bf16(c, M, N, K, (const float*)A, lda, (const float*)B, ldb, (float*)C, ldc,
-                            c->f32_gemm == 4 ? 3 : 1);
+    if (uses_umma(c) && umma_supported(K) && M >= 128 && N >= 256 && umma_c_ok(C, ldc))
+      return gemm_umma_bf16(c, M, N, K, (const float*)A, lda, (const float*)B, ldb, (float*)C, ldc, 3, mode == 1);
     if (tc && (c->f32_gemm >= 1 && c->f32_gemm <= 4))
       return gemm_bf16(c, M, N, K, (const float*)A, lda, (const float*)B, ldb, (float*)C, ldc, mode,
                        c->f32_gemm == 1 ? 1 : 3);
   }
   return gemm_simt<T>(c, M, N, K, A, lda, B, ldb, C, ldc, mode);
+}
+
+// The trailing update C -= A B of an FP32 factorisation: one BF16 product on tcgen05 in
+// the BF16 mode (f32_gemm 2), three otherwise.
+static int trailing_gemm(bem_ctx* c, int M, int N, int K, const float* A, int64_t lda, const float* B, int64_t ldb,
+                         float* C, int64_t ldc) {
+  if (c->f32_gemm == 2 && umma_supported(K) && M >= 128 && N >= 256 && umma_c_ok(C, ldc))
+    return gemm_umma_bf16(c, M, N, K, A, lda, B, ldb, C, ldc, 1, false);
+  return gemm<float>(c, M, N, K, A, lda, B, ldb, C, ldc, 0);
 }
 
 template int gemm<double>(bem_ctx*, int, int, int, const double*, int64_t, const double*, int64_t, double*,
@@ -1281,11 +1392,14 @@ static size_t up256(size_t b) { return (b + 255) / 256 * 256; }
 // window-pivoted 512-wide panel (panel_inv_f32_kernel), FP64 one block
 static size_t inv_blocks(int elem, int nb) { return elem == 4 ? 2 * (size_t)((nb + kInvBlock - 1) / kInvBlock) : 1; }
 
+static size_t finv_count(int elem, int nb) { return elem == 4 ? 2 * (size_t)nb * nb + (size_t)nb * kInvBlock : 0; }
+
 size_t lu_workspace_bytes(int n, int nb, int gmax, int elem) {
   const size_t ldy = ((size_t)n + 31) / 32 * 32;
   return up256(2 * (size_t)gmax * sizeof(double)) + up256(2 * (size_t)gmax * sizeof(int)) +
          up256(2 * (size_t)gmax * kPanelW * elem) + up256(2 * (size_t)kPanelW * elem) + up256(16) +
-         up256(inv_blocks(elem, nb) * kInvBlock * kInvBlock * elem) + up256(ldy * nb * elem);
+         up256(inv_blocks(elem, nb) * kInvBlock * kInvBlock * elem) + up256(finv_count(elem, nb) * elem) +
+         up256(ldy * nb * elem);
 }
 
 LUWorkspace lu_workspace_carve(void* base, int n, int nb, int gmax, int elem) {
@@ -1306,6 +1420,8 @@ LUWorkspace lu_workspace_carve(void* base, int n, int nb, int gmax, int elem) {
   p += up256(16);
   w.inv = p;
   p += up256(inv_blocks(elem, nb) * kInvBlock * kInvBlock * elem);
+  w.finv = finv_count(elem, nb) ? p : nullptr;
+  p += up256(finv_count(elem, nb) * elem);
   w.ybuf = p;
   return w;
 }
@@ -1455,32 +1571,50 @@ static int lu_factor_enqueue(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int
       const int nib = (nb + kInvBlock - 1) / kInvBlock;
       T* Vu = V;                                          // [nib][128 x 128]
       T* Wl = V + (size_t)(kInvBlock * kInvBlock) * nib;  // [nib][128 x 128]
+      // blocked panels (FP32): jb x jb inverses of the unit upper and the lower triangle,
+      // and a jb x 128 scratch
+      T* XU = blocked ? reinterpret_cast<T*>(ws.finv) : nullptr;
+      T* XL = blocked ? XU + (size_t)jb * jb : nullptr;
+      T* Tt = blocked ? XL + (size_t)jb * jb : nullptr;
       if (blocked) {
-        // the panel's diagonal-block inverses, then the rest of the sub-panels' columns:
-        // B = S(j0..t0, t0..n) := W^{-1} B with W the lower triangle of the diagonal
-        // block (U^T of T), by 128-row blocks: B_b -= W_{b,<b} B_{<b}; B_b = inv(W_bb) B_b
+        // the panel's diagonal-block inverses: the 128 x 128 ones, then the two full
+        // triangles' block column by block column (U unit upper, W lower, both of the
+        // panel's diagonal block of S):
+        //   XU_{<b,b} = -(XU_{<b,<b} U_{<b,b}) inv(U_bb),  XL_{b,<b} = -inv(W_bb) (W_{b,<b} XL_{<b,<b});
+        // then the rest of the sub-panels' columns in one product, B = S(j0..t0, t0..n)
+        // := W^{-1} B, through the TRSM buffer
         prof.begin(2, c->stream);
         const int nblk = (jb + kInvBlock - 1) / kInvBlock;
         panel_inv_f32_kernel<<<dim3(nblk, 2), kInvThreads, 2 * kInvBlock * kInvBlock * sizeof(float), c->stream>>>(
             reinterpret_cast<const float*>(S + j0 + (int64_t)j0 * lda), lda, jb, reinterpret_cast<float*>(Vu),
             reinterpret_cast<float*>(Wl));
         BEM_LAUNCH_CHECK(c);
+        BEM_CUDA(c, cudaMemsetAsync(XU, 0, 2 * (size_t)jb * jb * sizeof(T), c->stream));
         for (int b0 = 0; b0 < jb; b0 += kInvBlock) {
           const int bb = std::min(kInvBlock, jb - b0);
-          T* Bb = S + (j0 + b0) + (int64_t)t0 * lda;
-          if (b0 > 0 && (rc = gemm<T>(c, bb, m, b0, S + (j0 + b0) + (int64_t)j0 * lda, lda, S + j0 + (int64_t)t0 * lda,
-                                      lda, Bb, lda, 0)))
+          const T* Vb = Vu + (size_t)(b0 / kInvBlock) * kInvBlock * kInvBlock;
+          const T* Wb = Wl + (size_t)(b0 / kInvBlock) * kInvBlock * kInvBlock;
+          BEM_CUDA(c, cudaMemcpy2DAsync(XU + b0 + (size_t)b0 * jb, jb * sizeof(T), Vb, kInvBlock * sizeof(T),
+                                        bb * sizeof(T), bb, cudaMemcpyDeviceToDevice, c->stream));
+          BEM_CUDA(c, cudaMemcpy2DAsync(XL + b0 + (size_t)b0 * jb, jb * sizeof(T), Wb, kInvBlock * sizeof(T),
+                                        bb * sizeof(T), bb, cudaMemcpyDeviceToDevice, c->stream));
+          if (b0 == 0) continue;
+          if ((rc = gemm<T>(c, b0, bb, b0, XU, jb, S + j0 + (int64_t)(j0 + b0) * lda, lda, Tt, jb, 1)) ||
+              (rc = gemm<T>(c, b0, bb, bb, Tt, jb, Vb, kInvBlock, XU + (size_t)b0 * jb, jb, 0)) ||
+              (rc = gemm<T>(c, bb, b0, b0, S + (j0 + b0) + (int64_t)j0 * lda, lda, XL, jb, Tt, kInvBlock, 1)) ||
+              (rc = gemm<T>(c, bb, b0, bb, Wb, kInvBlock, Tt, kInvBlock, XL + b0, jb, 0)))
             return rc;
-          // Z (bb x m, leading dimension 128, in the TRSM buffer) = inv(W_bb) B_b, copied back
-          if ((rc = gemm<T>(c, bb, m, bb, Wl + (size_t)(b0 / kInvBlock) * kInvBlock * kInvBlock, kInvBlock, Bb, lda, Y,
-                            kInvBlock, 1)))
-            return rc;
-          BEM_CUDA(c, cudaMemcpy2DAsync(Bb, lda * sizeof(T), Y, kInvBlock * sizeof(T), bb * sizeof(T), m,
-                                        cudaMemcpyDeviceToDevice, c->stream));
         }
+        if ((rc = gemm<T>(c, jb, m, jb, XL, jb, S + j0 + (int64_t)t0 * lda, lda, Y, jb, 1))) return rc;
+        BEM_CUDA(c, cudaMemcpy2DAsync(S + j0 + (int64_t)t0 * lda, lda * sizeof(T), Y, jb * sizeof(T), jb * sizeof(T), m,
+                                      cudaMemcpyDeviceToDevice, c->stream));
         prof.end(c->stream);
       }
       prof.begin(3, c->stream);
+      if (blocked) {
+        // TRSM of the block row in one product, Y = X U^{-1}
+        if ((rc = gemm<T>(c, m, jb, jb, S + t0 + (int64_t)j0 * lda, lda, XU, jb, Y, ldy, 1))) return rc;
+      } else {
       // TRSM of the block row, Y = X U^{-1} with U the unit upper triangle of the panel's
       // diagonal block, in 128-wide column blocks: X_b -= Y_{<b} U_{<b,b}, Y_b = X_b inv(U_bb)
       for (int b0 = 0; b0 < jb; b0 += kInvBlock) {
@@ -1489,12 +1623,6 @@ static int lu_factor_enqueue(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int
         if (b0 > 0 &&
             (rc = gemm<T>(c, m, bb, b0, Y, ldy, S + j0 + (int64_t)(j0 + b0) * lda, lda, Xb, lda, 0)))
           return rc;
-        if (blocked) {
-          if ((rc = gemm<T>(c, m, bb, bb, Xb, lda, Vu + (size_t)(b0 / kInvBlock) * kInvBlock * kInvBlock, kInvBlock,
-                            Y + (int64_t)b0 * ldy, ldy, 1)))
-            return rc;
-          continue;
-        }
         if (sizeof(T) == 4)
           inv_unit_upper_f32_kernel<<<1, kInvThreads, 2 * kInvBlock * kInvBlock * sizeof(float), c->stream>>>(
               reinterpret_cast<const float*>(S + (j0 + b0) + (int64_t)(j0 + b0) * lda), lda, bb,
@@ -1505,12 +1633,19 @@ static int lu_factor_enqueue(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int
         BEM_LAUNCH_CHECK(c);
         if ((rc = gemm<T>(c, m, bb, bb, Xb, lda, V, kInvBlock, Y + (int64_t)b0 * ldy, ldy, 1))) return rc;
       }
+      }
       BEM_CUDA(c, cudaMemcpy2DAsync(S + t0 + (int64_t)j0 * lda, lda * sizeof(T), Y, ldy * sizeof(T), m * sizeof(T),
                                     jb, cudaMemcpyDeviceToDevice, c->stream));
       prof.end(c->stream);
       prof.begin(4, c->stream);
-      if ((rc = gemm<T>(c, m, m, jb, Y, ldy, S + j0 + (int64_t)t0 * lda, lda, S + t0 + (int64_t)t0 * lda, lda, 0)))
+      if constexpr (sizeof(T) == 4) {
+        if ((rc = trailing_gemm(c, m, m, jb, Y, ldy, S + j0 + (int64_t)t0 * lda, lda, S + t0 + (int64_t)t0 * lda,
+                                lda)))
+          return rc;
+      } else if ((rc = gemm<T>(c, m, m, jb, Y, ldy, S + j0 + (int64_t)t0 * lda, lda, S + t0 + (int64_t)t0 * lda, lda,
+                               0))) {
         return rc;
+      }
       prof.end(c->stream, 2.0 * m * (double)m * jb, (2.0 * m * (double)m + 2.0 * m * (double)jb) * sizeof(T));
     }
   }
@@ -1566,7 +1701,9 @@ int lu_factor(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int* perm, int nb,
   const LUWorkspace ws = lu_workspace_carve(c->lu_scratch[ti].p, n, nb, gmax, sizeof(T));
   if (sizeof(T) == 4 && uses_umma(c)) {
     int rc0;
-    if (n > nb && (rc0 = umma_reserve(c, n - nb, n - nb, nb))) return rc0;
+    // the largest operand pair: the trailing update's (M + N = 2 (n - nb)) or a blocked
+    // TRSM's (M + N <= n)
+    if (n > nb && (rc0 = umma_reserve(c, std::max(n, 2 * (n - nb)), 0, nb))) return rc0;
     if (c->umma_err.count < 1) BEM_CUDA(c, c->umma_err.alloc(1));
   }
   if (const char* e = getenv("BEM_LU_GRAPH"))

@@ -32,7 +32,9 @@ struct LUWorkspace {
   void* diag_col;     // [2][kPanelW] of T
   unsigned* barrier;  // grid-barrier counter (zeroed before every panel launch)
   int* status;        // [0] error code, [1] info (zeroed at the start of a factorisation)
-  void* inv;          // nb x nb of T
+  void* inv;          // the 128 x 128 diagonal-block inverses of a panel (T)
+  void* finv;         // FP32 panels: the panel's two full triangle inverses (2 nb x nb)
+                      // and their assembly's scratch (nb x 128), else null
   void* ybuf;         // ldy x nb of T
   int64_t ldy;
   int gmax;           // most CTAs a panel launch may use

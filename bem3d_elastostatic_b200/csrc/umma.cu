@@ -97,7 +97,7 @@ __device__ __forceinline__ void umma_commit(unsigned bar) {
 // warps 2-9 drain the other accumulator into C, so the update of C by one tile
 // overlaps the loads and MMAs of the next.  Tiles run m-fastest so a CTA wave shares
 // the B operand band.
-template <int NPROD, int STAGES, int NSTG>
+template <int NPROD, int STAGES, int NSTG, bool STORE>
 __global__ void __launch_bounds__(kThreads, 1)
     umma_update_kernel(const __grid_constant__ CUtensorMap tAh, const __grid_constant__ CUtensorMap tAl,
                        const __grid_constant__ CUtensorMap tBh, const __grid_constant__ CUtensorMap tBl,
@@ -309,17 +309,23 @@ __global__ void __launch_bounds__(kThreads, 1)
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
         const int rr = lq * 32 + lane;
 #pragma unroll
-        for (int j = 0; j < 32; ++j) stg[j * UM + rr] = -__uint_as_float(r[j]);
+        for (int j = 0; j < 32; ++j) stg[j * UM + rr] = STORE ? __uint_as_float(r[j]) : -__uint_as_float(r[j]);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("bar.sync %0, 128;" ::"r"(1 + half) : "memory");
         if (leader) {
           // rows m0.. (128-aligned, never negative), columns n0 + j0..; the tensor map
           // clips the box at M and N
-          asm volatile(
-              "cp.reduce.async.bulk.tensor.2d.global.shared::cta.add.tile.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
-                  reinterpret_cast<uint64_t>(&tC)),
-              "r"(m0), "r"(n0 + j0), "r"(stg_s)
-              : "memory");
+          if (STORE)
+            asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
+                             reinterpret_cast<uint64_t>(&tC)),
+                         "r"(m0), "r"(n0 + j0), "r"(stg_s)
+                         : "memory");
+          else
+            asm volatile(
+                "cp.reduce.async.bulk.tensor.2d.global.shared::cta.add.tile.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
+                    reinterpret_cast<uint64_t>(&tC)),
+                "r"(m0), "r"(n0 + j0), "r"(stg_s)
+                : "memory");
           asm volatile("cp.async.bulk.commit_group;" ::: "memory");
           pending = true;
         }
@@ -407,10 +413,12 @@ int umma_reserve(bem_ctx* c, int M, int N, int K) {
 }
 
 // C (M x N) -= A (M x K) * B (K x N) on tcgen05: nprod = 3, the three-term BF16 split
-// (FP32-grade products); nprod = 1, one BF16 product (hi * hi).
+// (FP32-grade products); nprod = 1, one BF16 product (hi * hi).  store: C = A B
+// instead (three products only; the epilogue's boxes are stored, not added).
 int gemm_umma_bf16(bem_ctx* c, int M, int N, int K, const float* A, int64_t lda, const float* B, int64_t ldb,
-                   float* C, int64_t ldc, int nprod) {
+                   float* C, int64_t ldc, int nprod, bool store) {
   if (nprod != 1 && nprod != 3) return bem_fail(c, BEM_ERR_ARG, "umma: nprod must be 1 or 3");
+  if (store && nprod != 3) return bem_fail(c, BEM_ERR_ARG, "umma: the storing form takes three products");
   if (!umma_supported(K)) return bem_fail(c, BEM_ERR_ARG, "umma: K must be a multiple of 64 up to 1024");
   if (!g_encode) {
     cudaDriverEntryPointQueryResult q;
@@ -419,22 +427,17 @@ int gemm_umma_bf16(bem_ctx* c, int M, int N, int K, const float* A, int64_t lda,
       return bem_fail(c, BEM_ERR_CUDA, "cuTensorMapEncodeTiled not available");
     g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
   }
-  // one product: three ring stages and two staging boxes per epilogue half
-  // (BEM_UMMA_RING=4: four stages, one box); three products: two stages, one box
-  static const bool ring4 = [] {
-    const char* e = getenv("BEM_UMMA_RING");
-    return e && e[0] == '4';
-  }();
-  using K1a = Cfg<1, 3, 2>;
-  using K1b = Cfg<1, 4, 1>;
+  // one product: four ring stages (48 KB each); three products: two (96 KB each); one
+  // staging box per epilogue half (two measured no faster)
+  using K1 = Cfg<1, 4, 1>;
   using K3 = Cfg<3, 2, 1>;
   static DeviceOnce attr;  // the kernel attribute is per device
   if (attr.pending()) {
-    BEM_CUDA(c, cudaFuncSetAttribute(umma_update_kernel<1, 3, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     K1a::smem));
-    BEM_CUDA(c, cudaFuncSetAttribute(umma_update_kernel<1, 4, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     K1b::smem));
-    BEM_CUDA(c, cudaFuncSetAttribute(umma_update_kernel<3, 2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    BEM_CUDA(c, cudaFuncSetAttribute(umma_update_kernel<1, 4, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     K1::smem));
+    BEM_CUDA(c, cudaFuncSetAttribute(umma_update_kernel<3, 2, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     K3::smem));
+    BEM_CUDA(c, cudaFuncSetAttribute(umma_update_kernel<3, 2, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      K3::smem));
     attr.mark();
   }
@@ -477,15 +480,15 @@ int gemm_umma_bf16(bem_ctx* c, int M, int N, int K, const float* A, int64_t lda,
       return bem_fail(c, BEM_ERR_CUDA, "umma: tensor map encoding of C failed");
   }
   const int grid = (int)std::min<int64_t>(tiles, c->sm_count);
-  if (nprod == 3)
-    umma_update_kernel<3, 2, 1><<<grid, kThreads, K3::smem, c->stream>>>(mAh, mAl, mBh, mBl, mC, M, N, K,
-                                                                         c->umma_err.p, c->wait_ns);
-  else if (ring4)
-    umma_update_kernel<1, 4, 1><<<grid, kThreads, K1b::smem, c->stream>>>(mAh, mAl, mBh, mBl, mC, M, N, K,
-                                                                          c->umma_err.p, c->wait_ns);
+  if (store)
+    umma_update_kernel<3, 2, 1, true><<<grid, kThreads, K3::smem, c->stream>>>(mAh, mAl, mBh, mBl, mC, M, N, K,
+                                                                               c->umma_err.p, c->wait_ns);
+  else if (nprod == 3)
+    umma_update_kernel<3, 2, 1, false><<<grid, kThreads, K3::smem, c->stream>>>(mAh, mAl, mBh, mBl, mC, M, N, K,
+                                                                                c->umma_err.p, c->wait_ns);
   else
-    umma_update_kernel<1, 3, 2><<<grid, kThreads, K1a::smem, c->stream>>>(mAh, mAl, mBh, mBl, mC, M, N, K,
-                                                                          c->umma_err.p, c->wait_ns);
+    umma_update_kernel<1, 4, 1, false><<<grid, kThreads, K1::smem, c->stream>>>(mAh, mAl, mBh, mBl, mC, M, N, K,
+                                                                                c->umma_err.p, c->wait_ns);
   BEM_LAUNCH_CHECK(c);
   return BEM_OK;
 }

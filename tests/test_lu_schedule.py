@@ -4,10 +4,13 @@ factored with row pivoting (column pivoting of S), U in S's lower triangle and t
 unit multipliers in its strict upper triangle.  The test replays the launch order --
 window factorisation of each 32-wide sub-panel within its 32 x 32 diagonal block,
 interchanges on the panel's rows, TRSM and GEMM restricted to the panel's diagonal
-block, the panel's interchanges on every other row at once, the blocked TRSM
-B := W^{-1} B with inv(W_bb) formed through the unit-upper inverse of (Lu^T), and the
-block-row TRSM with the unit-upper inverses -- and checks P T = L U in FP64."""
+block, the panel's interchanges on every other row at once, the 128 x 128 inverses of
+the diagonal block's triangles (the lower one through the unit-upper inverse of
+(Lu^T)), the full triangle inverses assembled from them block column by block column,
+and the two TRSMs as single products B := W^{-1} B and Y = X U^{-1} -- and checks
+P T = L U in FP64."""
 import numpy as np
+import pytest
 
 
 def _unit_upper_inv(U):
@@ -59,31 +62,38 @@ def window_lu(A, nb=512, W=32, B=128):
                 perm[[t, p]] = perm[[p, t]]
             S[np.ix_(rows, j0 + np.arange(jb))] = S[np.ix_(rows, j0 + perm)]
             Dg = S[j0:t0, j0:t0]
-            for b0 in range(0, jb, B):  # B := W^{-1} B
+            # 128-block inverses (panel_inv_f32_kernel): unit upper, and the lower
+            # triangle's through the unit-upper inverse of (Lu^T)
+            Vu, Wl = [], []
+            for b0 in range(0, jb, B):
                 bb = min(B, jb - b0)
-                if b0:
-                    S[j0 + b0:j0 + b0 + bb, t0:] -= S[j0 + b0:j0 + b0 + bb, j0:j0 + b0] @ S[j0:j0 + b0, t0:]
+                Vu.append(_unit_upper_inv(Dg[b0:b0 + bb, b0:b0 + bb]))
                 Wbb = np.tril(Dg[b0:b0 + bb, b0:b0 + bb])
                 rd = np.diag(Wbb)
-                V = _unit_upper_inv(Wbb.T / rd[:, None])  # (Lu^T)^{-1}
-                S[j0 + b0:j0 + b0 + bb, t0:] = (V.T / rd[:, None]) @ S[j0 + b0:j0 + b0 + bb, t0:]
-            Y = np.zeros((n - t0, jb))
-            for b0 in range(0, jb, B):  # Y = X U^{-1}
+                Wl.append(_unit_upper_inv(Wbb.T / rd[:, None]).T / rd[:, None])
+            # the full inverses, block column by block column
+            XU = np.zeros((jb, jb))
+            XL = np.zeros((jb, jb))
+            for k, b0 in enumerate(range(0, jb, B)):
                 bb = min(B, jb - b0)
-                Xb = S[t0:, j0 + b0:j0 + b0 + bb].copy()
+                XU[b0:b0 + bb, b0:b0 + bb] = Vu[k]
+                XL[b0:b0 + bb, b0:b0 + bb] = Wl[k]
                 if b0:
-                    Xb -= Y[:, :b0] @ S[j0:j0 + b0, j0 + b0:j0 + b0 + bb]
-                Y[:, b0:b0 + bb] = Xb @ _unit_upper_inv(Dg[b0:b0 + bb, b0:b0 + bb])
+                    XU[:b0, b0:b0 + bb] = -(XU[:b0, :b0] @ Dg[:b0, b0:b0 + bb]) @ Vu[k]
+                    XL[b0:b0 + bb, :b0] = -Wl[k] @ (Dg[b0:b0 + bb, :b0] @ XL[:b0, :b0])
+            S[j0:t0, t0:] = XL @ S[j0:t0, t0:]  # B := W^{-1} B
+            Y = S[t0:, j0:t0] @ XU  # Y = X U^{-1}
             S[t0:, j0:t0] = Y
             S[t0:, t0:] -= Y @ S[j0:t0, t0:]
     return S, piv
 
 
-def test_window_pivoted_schedule_factors_the_matrix():
+@pytest.mark.parametrize("n,nb", [(700, 512), (1300, 1024), (700, 256)])
+def test_window_pivoted_schedule_factors_the_matrix(n, nb):
+    """Panels of 512, 1024 and 256 with a ragged last panel and last 128-block."""
     rng = np.random.default_rng(1)
-    n = 700  # two panels, a ragged last panel and a ragged last 128-block
     A = rng.standard_normal((n, n)) + 4.0 * np.eye(n)
-    S, piv = window_lu(A)
+    S, piv = window_lu(A, nb=nb)
     assert np.all((piv >= np.arange(n) // 32 * 32) & (piv < np.minimum(np.arange(n) // 32 * 32 + 32, n)))
     T = A.T.copy()
     for i in range(n):  # P T with P = tau_0 tau_1 ... applied in order
