@@ -1199,7 +1199,7 @@ bool gemm_tc_ok(const void* A, int64_t lda, const void* B, int64_t ldb, int elem
 bool umma_supported(int K);
 int umma_reserve(bem_ctx* c, int M, int N, int K);
 int gemm_umma_bf16(bem_ctx* c, int M, int N, int K, const float* A, int64_t lda, const float* B, int64_t ldb,
-                   float* C, int64_t ldc, int nprod, bool store);
+                   float* C, int64_t ldc, int nprod, bool store, int kmode);
 
 // the FP32 trailing updates of this context run on tcgen05 (umma.cu)
 static bool uses_umma(const bem_ctx* c) { return c->f32_gemm == 4 || c->f32_gemm == 2; }
@@ -1236,7 +1236,8 @@ int gemm(bem_ctx* c, int M, int N, int K, const T* A, int64_t lda, const T* B, i
       return gemm_dmma(c, M, N, K, (const double*)A, lda, (const double*)B, ldb, (double*)C, ldc, mode);
   } else {
     if (uses_umma(c) && umma_supported(K) && M >= 128 && N >= 256 && umma_c_ok(C, ldc))
-      return gemm_umma_bf16(c, M, N, K, (const float*)A, lda, (const float*)B, ldb, (float*)C, ldc, 3, mode == 1);
+      return gemm_umma_bf16(c, M, N, K, (const float*)A, lda, (const float*)B, ldb, (float*)C, ldc, 3, mode == 1,
+                            0);
     if (tc && (c->f32_gemm >= 1 && c->f32_gemm <= 4))
       return gemm_bf16(c, M, N, K, (const float*)A, lda, (const float*)B, ldb, (float*)C, ldc, mode,
                        c->f32_gemm == 1 ? 1 : 3);
@@ -1249,8 +1250,17 @@ int gemm(bem_ctx* c, int M, int N, int K, const T* A, int64_t lda, const T* B, i
 static int trailing_gemm(bem_ctx* c, int M, int N, int K, const float* A, int64_t lda, const float* B, int64_t ldb,
                          float* C, int64_t ldc) {
   if (c->f32_gemm == 2 && umma_supported(K) && M >= 128 && N >= 256 && umma_c_ok(C, ldc))
-    return gemm_umma_bf16(c, M, N, K, A, lda, B, ldb, C, ldc, 1, false);
+    return gemm_umma_bf16(c, M, N, K, A, lda, B, ldb, C, ldc, 1, false, 0);
   return gemm<float>(c, M, N, K, A, lda, B, ldb, C, ldc, 0);
+}
+
+// C = A B with a triangular factor (kmode 1: A lower, kmode 2: B upper): on tcgen05 each
+// tile skips the K chunks of the factor's zero part.
+static int gemm_tri(bem_ctx* c, int M, int N, int K, const float* A, int64_t lda, const float* B, int64_t ldb,
+                    float* C, int64_t ldc, int kmode) {
+  if (uses_umma(c) && umma_supported(K) && M >= 128 && N >= 256 && umma_c_ok(C, ldc))
+    return gemm_umma_bf16(c, M, N, K, A, lda, B, ldb, C, ldc, 3, true, kmode);
+  return gemm<float>(c, M, N, K, A, lda, B, ldb, C, ldc, 1);
 }
 
 template int gemm<double>(bem_ctx*, int, int, int, const double*, int64_t, const double*, int64_t, double*,
@@ -1605,7 +1615,10 @@ static int lu_factor_enqueue(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int
               (rc = gemm<T>(c, bb, b0, bb, Wb, kInvBlock, Tt, kInvBlock, XL + b0, jb, 0)))
             return rc;
         }
-        if ((rc = gemm<T>(c, jb, m, jb, XL, jb, S + j0 + (int64_t)t0 * lda, lda, Y, jb, 1))) return rc;
+        if ((rc = gemm_tri(c, jb, m, jb, reinterpret_cast<const float*>(XL), jb,
+                           reinterpret_cast<const float*>(S + j0 + (int64_t)t0 * lda), lda, reinterpret_cast<float*>(Y),
+                           jb, 1)))
+          return rc;
         BEM_CUDA(c, cudaMemcpy2DAsync(S + j0 + (int64_t)t0 * lda, lda * sizeof(T), Y, jb * sizeof(T), jb * sizeof(T), m,
                                       cudaMemcpyDeviceToDevice, c->stream));
         prof.end(c->stream);
@@ -1613,7 +1626,9 @@ static int lu_factor_enqueue(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int
       prof.begin(3, c->stream);
       if (blocked) {
         // TRSM of the block row in one product, Y = X U^{-1}
-        if ((rc = gemm<T>(c, m, jb, jb, S + t0 + (int64_t)j0 * lda, lda, XU, jb, Y, ldy, 1))) return rc;
+        if ((rc = gemm_tri(c, m, jb, jb, reinterpret_cast<const float*>(S + t0 + (int64_t)j0 * lda), lda,
+                           reinterpret_cast<const float*>(XU), jb, reinterpret_cast<float*>(Y), ldy, 2)))
+          return rc;
       } else {
       // TRSM of the block row, Y = X U^{-1} with U the unit upper triangle of the panel's
       // diagonal block, in 128-wide column blocks: X_b -= Y_{<b} U_{<b,b}, Y_b = X_b inv(U_bb)

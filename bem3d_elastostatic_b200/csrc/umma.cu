@@ -101,7 +101,7 @@ template <int NPROD, int STAGES, int NSTG, bool STORE>
 __global__ void __launch_bounds__(kThreads, 1)
     umma_update_kernel(const __grid_constant__ CUtensorMap tAh, const __grid_constant__ CUtensorMap tAl,
                        const __grid_constant__ CUtensorMap tBh, const __grid_constant__ CUtensorMap tBl,
-                       const __grid_constant__ CUtensorMap tC, int M, int N, int K, int* err,
+                       const __grid_constant__ CUtensorMap tC, int M, int N, int K, int kmode, int* err,
                        unsigned long long wait_ns) {
   using C_ = Cfg<NPROD, STAGES, NSTG>;
   constexpr int kStages = STAGES, STAGE = C_::stage, kRing = C_::ring;
@@ -120,7 +120,12 @@ __global__ void __launch_bounds__(kThreads, 1)
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int tiles_m = (M + UM - 1) / UM, tiles_n = (N + UN - 1) / UN, total = tiles_m * tiles_n;
-  const int nchunk = K / UK;
+  // K chunks of the tile at (m0, n0): all, or with a triangular operand only those that
+  // meet its nonzero part (kmode 1: A lower triangular, kmode 2: B upper triangular)
+  auto chunks = [&](int m0, int n0) {
+    const int ke = kmode == 1 ? min(K, m0 + UM) : (kmode == 2 ? min(K, n0 + UN) : K);
+    return (ke + UK - 1) / UK;
+  };
 
   if (threadIdx.x == 0) {
     *abort_flag = 0;
@@ -163,6 +168,7 @@ __global__ void __launch_bounds__(kThreads, 1)
       for (int t = blockIdx.x; t < total && !*abort_flag; t += gridDim.x) {
         const int m0 = (t % tiles_m) * UM, n0 = (t / tiles_m) * UN;
         const int row[4] = {m0, m0, n0, n0};
+        const int nchunk = chunks(m0, n0);
         for (int c = 0; c < nchunk; ++c) {
           if (!mbar_wait(smem_u32(&empty[stage]), phase ^ 1u, abort_flag, wait_ns)) {
             fail();
@@ -210,6 +216,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const unsigned d = tmem + (unsigned)(ab * UN);
+        const int nchunk = chunks((t % tiles_m) * UM, (t / tiles_m) * UN);
         bool ok = true;
         for (int c = 0; c < nchunk; ++c) {
           if (!mbar_wait(smem_u32(&full[stage]), phase, abort_flag, wait_ns)) {
@@ -414,9 +421,12 @@ int umma_reserve(bem_ctx* c, int M, int N, int K) {
 
 // C (M x N) -= A (M x K) * B (K x N) on tcgen05: nprod = 3, the three-term BF16 split
 // (FP32-grade products); nprod = 1, one BF16 product (hi * hi).  store: C = A B
-// instead (three products only; the epilogue's boxes are stored, not added).
+// instead (three products only; the epilogue's boxes are stored, not added).  kmode 1
+// (A lower triangular) or 2 (B upper triangular): each tile runs only the K chunks that
+// meet the operand's nonzero part.
 int gemm_umma_bf16(bem_ctx* c, int M, int N, int K, const float* A, int64_t lda, const float* B, int64_t ldb,
-                   float* C, int64_t ldc, int nprod, bool store) {
+                   float* C, int64_t ldc, int nprod, bool store, int kmode) {
+  if (kmode < 0 || kmode > 2) return bem_fail(c, BEM_ERR_ARG, "umma: kmode must be 0, 1 or 2");
   if (nprod != 1 && nprod != 3) return bem_fail(c, BEM_ERR_ARG, "umma: nprod must be 1 or 3");
   if (store && nprod != 3) return bem_fail(c, BEM_ERR_ARG, "umma: the storing form takes three products");
   if (!umma_supported(K)) return bem_fail(c, BEM_ERR_ARG, "umma: K must be a multiple of 64 up to 1024");
@@ -482,13 +492,13 @@ int gemm_umma_bf16(bem_ctx* c, int M, int N, int K, const float* A, int64_t lda,
   const int grid = (int)std::min<int64_t>(tiles, c->sm_count);
   if (store)
     umma_update_kernel<3, 2, 1, true><<<grid, kThreads, K3::smem, c->stream>>>(mAh, mAl, mBh, mBl, mC, M, N, K,
-                                                                               c->umma_err.p, c->wait_ns);
+                                                                               kmode, c->umma_err.p, c->wait_ns);
   else if (nprod == 3)
     umma_update_kernel<3, 2, 1, false><<<grid, kThreads, K3::smem, c->stream>>>(mAh, mAl, mBh, mBl, mC, M, N, K,
-                                                                                c->umma_err.p, c->wait_ns);
+                                                                                kmode, c->umma_err.p, c->wait_ns);
   else
     umma_update_kernel<1, 4, 1, false><<<grid, kThreads, K1::smem, c->stream>>>(mAh, mAl, mBh, mBl, mC, M, N, K,
-                                                                                c->umma_err.p, c->wait_ns);
+                                                                                kmode, c->umma_err.p, c->wait_ns);
   BEM_LAUNCH_CHECK(c);
   return BEM_OK;
 }
