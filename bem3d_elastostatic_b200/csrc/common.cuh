@@ -128,6 +128,10 @@ struct LUGraph {
 struct bem_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
+  // a second stream for independent work inside a factorisation (forked from and joined
+  // back to `stream` by the two events; null: everything on `stream`)
+  cudaStream_t aux_stream = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   std::string last_error;
   int sm_count = 148;
 

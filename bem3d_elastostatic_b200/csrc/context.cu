@@ -113,7 +113,13 @@ int bem_ctx_create(bem_ctx** out, int device) {
   c->device = device;
   cudaError_t e = cudaSetDevice(device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->aux_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
   if (e != cudaSuccess) {
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->aux_stream) cudaStreamDestroy(c->aux_stream);
+    if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return BEM_ERR_CUDA;
   }
@@ -128,6 +134,10 @@ int bem_ctx_destroy(bem_ctx* c) {
   if (!c) return BEM_OK;
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
+  cudaStreamSynchronize(c->aux_stream);
+  cudaEventDestroy(c->ev_fork);
+  cudaEventDestroy(c->ev_join);
+  cudaStreamDestroy(c->aux_stream);
   cudaStreamDestroy(c->stream);
   delete c;  // DBuf destructors free device memory
   return BEM_OK;

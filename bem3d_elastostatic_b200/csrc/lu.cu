@@ -1393,7 +1393,9 @@ static size_t up256(size_t b) { return (b + 255) / 256 * 256; }
 // window-pivoted 512-wide panel (panel_inv_f32_kernel), FP64 one block
 static size_t inv_blocks(int elem, int nb) { return elem == 4 ? 2 * (size_t)((nb + kInvBlock - 1) / kInvBlock) : 1; }
 
-static size_t finv_count(int elem, int nb) { return elem == 4 ? 2 * (size_t)nb * nb + (size_t)nb * kInvBlock : 0; }
+static size_t finv_count(int elem, int nb) {
+  return elem == 4 ? 2 * (size_t)nb * nb + 2 * (size_t)nb * kInvBlock : 0;
+}
 
 size_t lu_workspace_bytes(int n, int nb, int gmax, int elem) {
   const size_t ldy = ((size_t)n + 31) / 32 * 32;
@@ -1573,10 +1575,11 @@ static int lu_factor_enqueue(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int
       T* Vu = V;                                          // [nib][128 x 128]
       T* Wl = V + (size_t)(kInvBlock * kInvBlock) * nib;  // [nib][128 x 128]
       // blocked panels (FP32): jb x jb inverses of the unit upper and the lower triangle,
-      // and a jb x 128 scratch
+      // and a jb x 128 scratch for each
       T* XU = blocked ? reinterpret_cast<T*>(ws.finv) : nullptr;
       T* XL = blocked ? XU + (size_t)jb * jb : nullptr;
-      T* Tt = blocked ? XL + (size_t)jb * jb : nullptr;
+      T* Tu = blocked ? XL + (size_t)jb * jb : nullptr;
+      T* Tl = blocked ? Tu + (size_t)jb * kInvBlock : nullptr;
       if (blocked) {
         // the panel's diagonal-block inverses: the 128 x 128 ones, then the two full
         // triangles' block column by block column (U unit upper, W lower, both of the
@@ -1591,19 +1594,42 @@ static int lu_factor_enqueue(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int
             reinterpret_cast<float*>(Wl));
         BEM_LAUNCH_CHECK(c);
         BEM_CUDA(c, cudaMemsetAsync(XU, 0, 2 * (size_t)jb * jb * sizeof(T), c->stream));
-        for (int b0 = 0; b0 < jb; b0 += kInvBlock) {
+        // the two inverses are independent: XU's chain (no tcgen05 GEMM, whose operand
+        // buffer is the context's) runs on the auxiliary stream, joined before the
+        // block-row TRSM that needs it; XL's chain and the L21 product run here
+        cudaStream_t main_stream = c->stream;
+        const bool fork = c->aux_stream != nullptr;
+        if (fork) {
+          BEM_CUDA(c, cudaEventRecord(c->ev_fork, main_stream));
+          BEM_CUDA(c, cudaStreamWaitEvent(c->aux_stream, c->ev_fork, 0));
+          c->stream = c->aux_stream;
+        }
+        rc = 0;
+        for (int b0 = 0; b0 < jb && rc == 0; b0 += kInvBlock) {
           const int bb = std::min(kInvBlock, jb - b0);
           const T* Vb = Vu + (size_t)(b0 / kInvBlock) * kInvBlock * kInvBlock;
+          if (cudaMemcpy2DAsync(XU + b0 + (size_t)b0 * jb, jb * sizeof(T), Vb, kInvBlock * sizeof(T), bb * sizeof(T),
+                                bb, cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess) {
+            rc = bem_fail(c, BEM_ERR_CUDA, "inverse assembly copy failed");
+          } else if (b0 > 0) {
+            rc = gemm<T>(c, b0, bb, b0, XU, jb, S + j0 + (int64_t)(j0 + b0) * lda, lda, Tu, jb, 1);
+            if (rc == 0) rc = gemm<T>(c, b0, bb, bb, Tu, jb, Vb, kInvBlock, XU + (size_t)b0 * jb, jb, 0);
+          }
+        }
+        if (fork) {
+          if (rc == 0 && cudaEventRecord(c->ev_join, c->aux_stream) != cudaSuccess)
+            rc = bem_fail(c, BEM_ERR_CUDA, "event record failed");
+          c->stream = main_stream;
+        }
+        if (rc) return rc;
+        for (int b0 = 0; b0 < jb; b0 += kInvBlock) {
+          const int bb = std::min(kInvBlock, jb - b0);
           const T* Wb = Wl + (size_t)(b0 / kInvBlock) * kInvBlock * kInvBlock;
-          BEM_CUDA(c, cudaMemcpy2DAsync(XU + b0 + (size_t)b0 * jb, jb * sizeof(T), Vb, kInvBlock * sizeof(T),
-                                        bb * sizeof(T), bb, cudaMemcpyDeviceToDevice, c->stream));
           BEM_CUDA(c, cudaMemcpy2DAsync(XL + b0 + (size_t)b0 * jb, jb * sizeof(T), Wb, kInvBlock * sizeof(T),
                                         bb * sizeof(T), bb, cudaMemcpyDeviceToDevice, c->stream));
           if (b0 == 0) continue;
-          if ((rc = gemm<T>(c, b0, bb, b0, XU, jb, S + j0 + (int64_t)(j0 + b0) * lda, lda, Tt, jb, 1)) ||
-              (rc = gemm<T>(c, b0, bb, bb, Tt, jb, Vb, kInvBlock, XU + (size_t)b0 * jb, jb, 0)) ||
-              (rc = gemm<T>(c, bb, b0, b0, S + (j0 + b0) + (int64_t)j0 * lda, lda, XL, jb, Tt, kInvBlock, 1)) ||
-              (rc = gemm<T>(c, bb, b0, bb, Wb, kInvBlock, Tt, kInvBlock, XL + b0, jb, 0)))
+          if ((rc = gemm<T>(c, bb, b0, b0, S + (j0 + b0) + (int64_t)j0 * lda, lda, XL, jb, Tl, kInvBlock, 1)) ||
+              (rc = gemm<T>(c, bb, b0, bb, Wb, kInvBlock, Tl, kInvBlock, XL + b0, jb, 0)))
             return rc;
         }
         if ((rc = gemm_tri(c, jb, m, jb, reinterpret_cast<const float*>(XL), jb,
@@ -1616,6 +1642,7 @@ static int lu_factor_enqueue(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int
       }
       prof.begin(3, c->stream);
       if (blocked) {
+        if (c->aux_stream) BEM_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join, 0));
         // TRSM of the block row in one product, Y = X U^{-1}
         if ((rc = gemm_tri(c, m, jb, jb, reinterpret_cast<const float*>(S + t0 + (int64_t)j0 * lda), lda,
                            reinterpret_cast<const float*>(XU), jb, reinterpret_cast<float*>(Y), ldy, 2)))
