@@ -500,7 +500,8 @@ def leg_adjoint(device, fd_coords=2, m=16):
         return compliance(mesh, X, u, t, inner), X, m_, n_, x
 
     try:
-        forward(X0, mu0, nu0)  # warm-up
+        Jw = forward(X0, mu0, nu0, grad=True)[0]  # warm-up of the forward and the backward path
+        Jw.backward()
         t0 = time.perf_counter()
         J, X, mu, nu, x = forward(X0, mu0, nu0, grad=True)
         t1 = time.perf_counter()
