@@ -767,13 +767,16 @@ def run_gpu(args, ws, rank, local):
     b = roofline["tensor"] if tensor_frac >= hbm_frac else roofline["hbm"]
     roofline.update({"bound": "tensor" if tensor_frac >= hbm_frac else "hbm", "achieved": b["achieved"],
                      "peak": b["peak"], "unit": b["unit"], "frac": b["frac"], "peak_source": b["peak_source"]})
+    # DRAM traffic: the algorithmic bytes x the DRAM/algorithmic ratio of this mode's ncu
+    # capture at 18,438 DOF (a full-size capture would hold 65 GB on the device; the
+    # traffic grows with m^2 like the algorithmic bytes)
     tf = os.path.join(HERE, "profiles", "trailing_gemm_traffic.json")
     if os.path.exists(tf):
         with open(tf) as f:
-            ratio = json.load(f).get("dram_bytes_over_algorithmic")
+            ratio = (json.load(f).get(args.precision) or {}).get("dram_bytes_over_algorithmic")
         if ratio:
             roofline["traffic"] = ratio * roofline["algorithmic_bytes_per_launch"]
-            roofline["traffic_source"] = "ncu dram__bytes ratio, profiles/trailing_gemm_traffic.json"
+            roofline["traffic_source"] = f"ncu dram__bytes ratio ({args.precision}), profiles/trailing_gemm_traffic.json"
 
     cpu = None
     parity = {"rel_err_vs_fp64": rel_err, "rel_err_vs_fp64_ir": rel_err_ir, "fp64_lu_vs_fp64_ir": fp64_lu_vs_ir,
