@@ -85,27 +85,15 @@ __device__ __forceinline__ void regular_pair(const AsmArgs& P, int e, const doub
 #pragma unroll
       for (int ld = 0; ld < 3; ++ld) {
         if (__ldg(P.kode + 3 * e + ld) == 0) {
-          // read-modify-write of the element's 3 x NC block: all loads first, so the
-          // update costs one memory round trip instead of one per entry
+          // the element's 3 x NC block added into A by reductions at L2 (no load on the
+          // SM's critical path); the batches' CTA barrier orders the additions into an
+          // entry, so the sums are deterministic
           const double mu = P.mat.mu;
-          constexpr int G1 = (NC + 2) / 3;
 #pragma unroll
-          for (int k0 = 0; k0 < NC; k0 += G1) {
-            double old[G1][3];
+          for (int k = 0; k < NC; ++k) {
+            double* col = P.A + (3 * (int64_t)kc[k] + ld) * P.lda + row;
 #pragma unroll
-            for (int kk = 0; kk < G1; ++kk)
-              if (k0 + kk < NC) {
-                const double* col = P.A + (3 * (int64_t)kc[k0 + kk] + ld) * P.lda + row;
-#pragma unroll
-                for (int jj = 0; jj < 3; ++jj) old[kk][jj] = col[jj];
-              }
-#pragma unroll
-            for (int kk = 0; kk < G1; ++kk)
-              if (k0 + kk < NC) {
-                double* col = P.A + (3 * (int64_t)kc[k0 + kk] + ld) * P.lda + row;
-#pragma unroll
-                for (int jj = 0; jj < 3; ++jj) col[jj] = old[kk][jj] - g[k0 + kk][sym_idx(jj, ld)] * mu;
-              }
+            for (int jj = 0; jj < 3; ++jj) atomicAdd(col + jj, -(g[k][sym_idx(jj, ld)] * mu));
           }
         } else {
 #pragma unroll
@@ -182,59 +170,31 @@ __device__ __forceinline__ void regular_pair(const AsmArgs& P, int e, const doub
             for (int jj = 0; jj < 3; ++jj) fi[jj] = fma(-h[k][jj + 3 * ld], b, fi[jj]);
           }
         } else {
-          // the same batched read-modify-write, in thirds of the element's nodes to
-          // bound the registers held next to the 9 x NC accumulators
-          constexpr int H1 = (NC + 2) / 3;
+          // the same reductions into A for the unknown columns; the prescribed ones go
+          // to FI
 #pragma unroll
-          for (int k0 = 0; k0 < NC; k0 += H1) {
-            double old[H1][3];
-            bool uk[H1];
+          for (int k = 0; k < NC; ++k) {
+            const int64_t dof = 3 * (int64_t)kc[k] + ld;
+            if (__ldg(P.uknown + dof) == 0) {
+              double* col = P.A + dof * P.lda + row;
 #pragma unroll
-            for (int kk = 0; kk < H1; ++kk) {
-              const int k = k0 + kk;
-              if (k < NC) {
-                const int64_t dof = 3 * (int64_t)kc[k] + ld;
-                uk[kk] = __ldg(P.uknown + dof) != 0;
-                if (!uk[kk]) {
-                  const double* col = P.A + dof * P.lda + row;
+              for (int jj = 0; jj < 3; ++jj) atomicAdd(col + jj, h[k][jj + 3 * ld]);
+            } else {
+              const double v = __ldg(P.vp + dof);
 #pragma unroll
-                  for (int jj = 0; jj < 3; ++jj) old[kk][jj] = col[jj];
-                }
-              }
-            }
-#pragma unroll
-            for (int kk = 0; kk < H1; ++kk) {
-              const int k = k0 + kk;
-              if (k < NC) {
-                const int64_t dof = 3 * (int64_t)kc[k] + ld;
-                if (!uk[kk]) {
-                  double* col = P.A + dof * P.lda + row;
-#pragma unroll
-                  for (int jj = 0; jj < 3; ++jj) col[jj] = old[kk][jj] + h[k][jj + 3 * ld];
-                } else {
-                  const double v = __ldg(P.vp + dof);
-#pragma unroll
-                  for (int jj = 0; jj < 3; ++jj) fi[jj] = fma(-h[k][jj + 3 * ld], v, fi[jj]);
-                }
-              }
+              for (int jj = 0; jj < 3; ++jj) fi[jj] = fma(-h[k][jj + 3 * ld], v, fi[jj]);
             }
           }
         }
       }
     } else {
 #pragma unroll
-      for (int k = 0; k < NC; ++k) {
-        double old[3][3];
-#pragma unroll
-        for (int ii = 0; ii < 3; ++ii)
-#pragma unroll
-          for (int jj = 0; jj < 3; ++jj) old[ii][jj] = P.A[(3 * (int64_t)kc[k] + ii) * P.lda + row + jj];
+      for (int k = 0; k < NC; ++k)
 #pragma unroll
         for (int ii = 0; ii < 3; ++ii)
 #pragma unroll
           for (int jj = 0; jj < 3; ++jj)
-            P.A[(3 * (int64_t)kc[k] + ii) * P.lda + row + jj] = old[ii][jj] + h[k][jj + 3 * ii];
-      }
+            atomicAdd(P.A + (3 * (int64_t)kc[k] + ii) * P.lda + row + jj, h[k][jj + 3 * ii]);
     }
   }
   if (MODE == kModeA)

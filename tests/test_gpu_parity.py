@@ -93,6 +93,18 @@ def test_ghmat8_entrywise(which, cube2, cube8_mesh, gpu_cube2, gpu_cube8):
     assert np.abs(F - Fr).max() <= 1e-12 * np.abs(Fr).max()
 
 
+def test_assembly_is_bitwise_reproducible(gpu_cube8):
+    """The element blocks are added into A and H by reductions at L2; the CTA barrier
+    between element batches orders the additions into an entry, so two assemblies
+    agree bit for bit."""
+    A1, F1 = gpu_cube8.ghmat8(return_system=True)
+    A2, F2 = gpu_cube8.ghmat8(return_system=True)
+    assert np.array_equal(A1, A2) and np.array_equal(F1, F2)
+    H1, G1 = gpu_cube8.hg()
+    H2, G2 = gpu_cube8.hg()
+    assert np.array_equal(H1, H2) and np.array_equal(G1, G2)
+
+
 @pytest.mark.parametrize("precision", ["fp64", "fp32-ir"])
 def test_solution_vs_oracle_cube8(precision, cube8_mesh):
     from bem3d_elastostatic_b200.api import Quadesth
