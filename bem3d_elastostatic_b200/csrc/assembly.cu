@@ -134,15 +134,16 @@ __device__ __forceinline__ void regular_pair(const AsmArgs& P, int e, const doub
       const R a[3] = {r0 * ri, r1 * ri, r2 * ri};
       const R rdn = a[0] * n[0] + a[1] * n[1] + a[2] * n[2];
       const R c5r2 = rc5 * ri * ri;
-      R t[9];
-#pragma unroll
-      for (int ii = 0; ii < 3; ++ii)
-#pragma unroll
-        for (int jj = 0; jj < 3; ++jj) {
-          const R d = (ii == jj) ? rc6 : R(0);
-          t[jj + 3 * ii] =
-              c5r2 * (rdn * (d + R(3) * a[ii] * a[jj]) + rc6 * (n[jj] * a[ii] - n[ii] * a[jj]));
-        }
+      // T*(ii, jj) = c5/r^2 (rdn (c6 delta + 3 a_ii a_jj) + c6 (n_jj a_ii - n_ii a_jj)):
+      // the symmetric part from the 6 products a_ii a_jj, the antisymmetric part from 3
+      const R k1 = R(3) * c5r2 * rdn, k2 = c5r2 * rc6, k3 = k2 * rdn;
+      const R s00 = k1 * (a[0] * a[0]) + k3, s11 = k1 * (a[1] * a[1]) + k3, s22 = k1 * (a[2] * a[2]) + k3;
+      const R s01 = k1 * (a[0] * a[1]), s12 = k1 * (a[1] * a[2]), s20 = k1 * (a[2] * a[0]);
+      const R b01 = k2 * (n[1] * a[0] - n[0] * a[1]);  // antisymmetric (ii, jj) = (0, 1)
+      const R b12 = k2 * (n[2] * a[1] - n[1] * a[2]);
+      const R b20 = k2 * (n[0] * a[2] - n[2] * a[0]);
+      // t[jj + 3 ii]
+      const R t[9] = {s00, s01 + b01, s20 - b20, s01 - b01, s11, s12 + b12, s20 + b20, s12 - b12, s22};
       const double* W = T + kTabGeo + 9 * q;
 #pragma unroll
       for (int k = 0; k < NC; ++k) {
