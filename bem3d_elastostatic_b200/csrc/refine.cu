@@ -33,43 +33,67 @@ __device__ __forceinline__ double pow2_scale(double mx) {
   return exp2(-floor(log2(mx)));
 }
 
-// one thread per row, eight columns per step (eight loads in flight per thread)
-__global__ void row_scale_kernel(const double* __restrict__ A, int64_t lda, int n, double* __restrict__ rs) {
+// Row maxima of |A| by column chunks: a thread per row and a CTA column range of
+// kRowChunk columns, 16 loads in flight per thread; the chunks' maxima meet in rmax
+// (the bits of a non-negative double order like the double).  NaNs are skipped by fmax.
+constexpr int kRowChunk = 1024;
+__global__ void row_max_kernel(const double* __restrict__ A, int64_t lda, int n, unsigned long long* rmax) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const int j0 = blockIdx.y * kRowChunk, j1 = min(n, j0 + kRowChunk);
   double mx = 0.0;
-  int j = 0;
-  for (; j + 8 <= n; j += 8) {
+  int j = j0;
+  for (; j + 16 <= j1; j += 16) {
+    double v[16];
+#pragma unroll
+    for (int u = 0; u < 16; ++u) v[u] = fabs(A[i + (int64_t)(j + u) * lda]);
+#pragma unroll
+    for (int u = 0; u < 16; ++u) mx = fmax(mx, v[u]);
+  }
+  for (; j < j1; ++j) mx = fmax(mx, fabs(A[i + (int64_t)j * lda]));
+  atomicMax(rmax + i, (unsigned long long)__double_as_longlong(mx));
+}
+
+__global__ void row_scale_kernel(int n, const unsigned long long* __restrict__ rmax, double* __restrict__ rs) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) rs[i] = pow2_scale(__longlong_as_double((long long)rmax[i]));
+}
+
+// Column scales of the row-scaled matrix and the scaled FP32 copy in one pass per
+// column: a CTA reads column j (eight loads in flight per thread), reduces its maximum,
+// then converts the column again from L2 (148 columns in flight are ~90 MB); the FP32
+// copy's padding rows are zero.
+constexpr int kColThreads = 256;
+__global__ void __launch_bounds__(kColThreads) col_scale_convert_kernel(const double* __restrict__ A, int64_t lda,
+                                                                        int n, const double* __restrict__ rs,
+                                                                        double* __restrict__ cs, float* A32) {
+  const int64_t j = blockIdx.x;
+  const double* a = A + j * lda;
+  __shared__ double red[kColThreads / 32];
+  __shared__ double s_c;
+  double mx = 0.0;
+  int i = threadIdx.x;
+  for (; i + 7 * kColThreads < n; i += 8 * kColThreads) {
     double v[8];
 #pragma unroll
-    for (int u = 0; u < 8; ++u) v[u] = fabs(A[i + (int64_t)(j + u) * lda]);
+    for (int u = 0; u < 8; ++u) v[u] = fabs(a[i + u * kColThreads] * rs[i + u * kColThreads]);
 #pragma unroll
     for (int u = 0; u < 8; ++u) mx = fmax(mx, v[u]);
   }
-  for (; j < n; ++j) mx = fmax(mx, fabs(A[i + (int64_t)j * lda]));
-  rs[i] = pow2_scale(mx);
-}
-
-// one warp per column of the row-scaled matrix
-__global__ void col_scale_kernel(const double* __restrict__ A, int64_t lda, int n, const double* __restrict__ rs,
-                                 double* __restrict__ cs) {
-  const int64_t j = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (j >= n) return;
-  double mx = 0.0;
-  for (int i = lane; i < n; i += 32) mx = fmax(mx, fabs(A[i + j * lda] * rs[i]));
+  for (; i < n; i += kColThreads) mx = fmax(mx, fabs(a[i] * rs[i]));
   for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
-  if (lane == 0) cs[j] = pow2_scale(mx);
-}
-
-__global__ void to_fp32_scaled_kernel(const double* A, int64_t lda, int n, const double* rs, const double* cs,
-                                      float* A32) {
-  const int64_t total = (int64_t)lda * n;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t j = e / lda;
-    const int i = (int)(e - j * lda);
-    A32[e] = i < n ? (float)(A[e] * rs[i] * cs[j]) : 0.f;
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = red[0];
+    for (int w = 1; w < kColThreads / 32; ++w) m = fmax(m, red[w]);
+    s_c = pow2_scale(m);
+    cs[j] = s_c;
   }
+  __syncthreads();
+  const double c = s_c;
+  float* o = A32 + j * lda;
+  for (int64_t r = threadIdx.x; r < lda; r += kColThreads) o[r] = r < n ? (float)(a[r] * rs[r] * c) : 0.f;
 }
 
 __global__ void mul_kernel(int n, const double* s, double* x) {
@@ -215,13 +239,16 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
   if (scaled) {
     BEM_CUDA(c, c->rowscale.alloc(n));
     BEM_CUDA(c, c->colscale.alloc(n));
-    row_scale_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(c->A.p, lda, n, c->rowscale.p);
+    // the column scales' buffer holds the row maxima until the column pass
+    unsigned long long* rmax = reinterpret_cast<unsigned long long*>(c->colscale.p);
+    BEM_CUDA(c, cudaMemsetAsync(rmax, 0, (size_t)n * sizeof(unsigned long long), c->stream));
+    row_max_kernel<<<dim3((n + 255) / 256, (n + kRowChunk - 1) / kRowChunk), 256, 0, c->stream>>>(c->A.p, lda, n,
+                                                                                                  rmax);
     BEM_LAUNCH_CHECK(c);
-    col_scale_kernel<<<(unsigned)(((int64_t)n * 32 + 255) / 256), 256, 0, c->stream>>>(c->A.p, lda, n, c->rowscale.p,
-                                                                                      c->colscale.p);
+    row_scale_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(n, rmax, c->rowscale.p);
     BEM_LAUNCH_CHECK(c);
-    to_fp32_scaled_kernel<<<c->sm_count * 8, 256, 0, c->stream>>>(c->A.p, lda, n, c->rowscale.p, c->colscale.p,
-                                                                 c->A32.p);
+    col_scale_convert_kernel<<<n, kColThreads, 0, c->stream>>>(c->A.p, lda, n, c->rowscale.p, c->colscale.p,
+                                                               c->A32.p);
   } else if (dbl) {
     BEM_CUDA(c, cudaMemcpyAsync(c->A64f.p, c->A.p, (size_t)lda * n * sizeof(double), cudaMemcpyDeviceToDevice,
                                 c->stream));
