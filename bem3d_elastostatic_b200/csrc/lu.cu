@@ -1226,11 +1226,7 @@ int gemm(bem_ctx* c, int M, int N, int K, const T* A, int64_t lda, const T* B, i
     if (tc && c->f64_gemm == 1)
       return gemm_dmma(c, M, N, K, (const double*)A, lda, (const double*)B, ldb, (double*)C, ldc, mode);
   } else {
-    // tcgen05 once the product fills every SM with a 128 x 256 tile; smaller ones (the
-    // triangle-inverse assembly's) take one mma.sync launch instead of a launch plus two
-    // operand splits
-    const int64_t tiles = (int64_t)((M + 127) / 128) * ((N + 255) / 256);
-    if (uses_umma(c) && umma_supported(K) && M >= 128 && N >= 256 && tiles >= c->sm_count && umma_c_ok(C, ldc))
+    if (uses_umma(c) && umma_supported(K) && M >= 128 && N >= 256 && umma_c_ok(C, ldc))
       return gemm_umma_bf16(c, M, N, K, (const float*)A, lda, (const float*)B, ldb, (float*)C, ldc, 3, mode == 1,
                             0);
     if (tc && (c->f32_gemm >= 1 && c->f32_gemm <= 4))
