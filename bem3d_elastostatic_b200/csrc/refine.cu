@@ -60,40 +60,44 @@ __global__ void row_scale_kernel(int n, const unsigned long long* __restrict__ r
 }
 
 // Column scales of the row-scaled matrix and the scaled FP32 copy in one pass per
-// column: a CTA reads column j (eight loads in flight per thread), reduces its maximum,
-// then converts the column again from L2 (148 columns in flight are ~90 MB); the FP32
-// copy's padding rows are zero.
-constexpr int kColThreads = 256;
+// column: a CTA reads column j (16 loads in flight per thread), reduces its maximum,
+// then converts the column again while it is still in L2.  The grid is sized so that
+// the columns in flight fill half the L2 (kColL2 bytes), and each CTA walks its columns
+// in turn.  The FP32 copy's padding rows are zero.
+constexpr int kColThreads = 1024;
+constexpr size_t kColL2 = 64ull << 20;
 __global__ void __launch_bounds__(kColThreads) col_scale_convert_kernel(const double* __restrict__ A, int64_t lda,
                                                                         int n, const double* __restrict__ rs,
                                                                         double* __restrict__ cs, float* A32) {
-  const int64_t j = blockIdx.x;
-  const double* a = A + j * lda;
   __shared__ double red[kColThreads / 32];
   __shared__ double s_c;
-  double mx = 0.0;
-  int i = threadIdx.x;
-  for (; i + 7 * kColThreads < n; i += 8 * kColThreads) {
-    double v[8];
+  for (int64_t j = blockIdx.x; j < n; j += gridDim.x) {
+    const double* a = A + j * lda;
+    double mx = 0.0;
+    int i = threadIdx.x;
+    for (; i + 15 * kColThreads < n; i += 16 * kColThreads) {
+      double v[16];
 #pragma unroll
-    for (int u = 0; u < 8; ++u) v[u] = fabs(a[i + u * kColThreads] * rs[i + u * kColThreads]);
+      for (int u = 0; u < 16; ++u) v[u] = fabs(a[i + u * kColThreads] * rs[i + u * kColThreads]);
 #pragma unroll
-    for (int u = 0; u < 8; ++u) mx = fmax(mx, v[u]);
+      for (int u = 0; u < 16; ++u) mx = fmax(mx, v[u]);
+    }
+    for (; i < n; i += kColThreads) mx = fmax(mx, fabs(a[i] * rs[i]));
+    for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double m = red[0];
+      for (int w = 1; w < kColThreads / 32; ++w) m = fmax(m, red[w]);
+      s_c = pow2_scale(m);
+      cs[j] = s_c;
+    }
+    __syncthreads();
+    const double c = s_c;
+    float* o = A32 + j * lda;
+    for (int64_t r = threadIdx.x; r < lda; r += kColThreads) o[r] = r < n ? (float)(a[r] * rs[r] * c) : 0.f;
+    __syncthreads();  // red and s_c are reused by the next column
   }
-  for (; i < n; i += kColThreads) mx = fmax(mx, fabs(a[i] * rs[i]));
-  for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double m = red[0];
-    for (int w = 1; w < kColThreads / 32; ++w) m = fmax(m, red[w]);
-    s_c = pow2_scale(m);
-    cs[j] = s_c;
-  }
-  __syncthreads();
-  const double c = s_c;
-  float* o = A32 + j * lda;
-  for (int64_t r = threadIdx.x; r < lda; r += kColThreads) o[r] = r < n ? (float)(a[r] * rs[r] * c) : 0.f;
 }
 
 __global__ void mul_kernel(int n, const double* s, double* x) {
@@ -247,8 +251,11 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
     BEM_LAUNCH_CHECK(c);
     row_scale_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(n, rmax, c->rowscale.p);
     BEM_LAUNCH_CHECK(c);
-    col_scale_convert_kernel<<<n, kColThreads, 0, c->stream>>>(c->A.p, lda, n, c->rowscale.p, c->colscale.p,
-                                                               c->A32.p);
+    const int64_t col_ctas =
+        std::max<int64_t>(1, std::min<int64_t>({(int64_t)n, (int64_t)(kColL2 / ((size_t)lda * sizeof(double))),
+                                                (int64_t)2 * c->sm_count}));
+    col_scale_convert_kernel<<<(unsigned)col_ctas, kColThreads, 0, c->stream>>>(c->A.p, lda, n, c->rowscale.p,
+                                                                                c->colscale.p, c->A32.p);
   } else if (dbl) {
     BEM_CUDA(c, cudaMemcpyAsync(c->A64f.p, c->A.p, (size_t)lda * n * sizeof(double), cudaMemcpyDeviceToDevice,
                                 c->stream));
