@@ -21,6 +21,7 @@ struct AsmArgs {
   const double* y;
   const double* z;
   const double* tab;
+  const double* rec;  // mode A: per-element boundary records (assembly.cu, kRecD doubles each)
   Material mat;
   double* A;  // mode A: (3n, 3n); mode HG: H
   int64_t lda;

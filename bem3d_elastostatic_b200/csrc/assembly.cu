@@ -38,13 +38,52 @@ __device__ __forceinline__ int sym_idx(int a, int b) {
   return s == 1 ? 3 : (s == 3 ? 4 : 5);
 }
 
+// The boundary record of an element for mode A (the column swap's inputs, staged in
+// shared memory with the element's quadrature table so that the element's epilogue
+// reads warp-uniform values from shared memory instead of global memory):
+//   doubles [k + 9 ld]       bc(k, ld) of the element (its prescribed displacement or
+//                            traction value, io_mod layout bc(3k + ld + 27 e))
+//   doubles [27 + k + 9 ld]  vp of the element node's dof 3 kc[k] + ld
+//   ints    kRecInt + 0      bit ld: kode(ld, e) != 0; bit 3 + k + 9 ld: uknown(dof) != 0
+//   ints    kRecInt + 1      the element's node count; + 2..10 its nodes (0-based)
+constexpr int kRecD = 60;              // doubles per record (480 B)
+constexpr int kRecInt = 2 * 54;        // int offset of the flags
+__global__ void elem_record_kernel(AsmArgs P, double* rec) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= P.ne) return;
+  double* R = rec + (int64_t)e * kRecD;
+  int* I = reinterpret_cast<int*>(R) + kRecInt;
+  const int ncone = P.nconec[e];
+  unsigned bits = 0;
+  for (int ld = 0; ld < 3; ++ld) {
+    if (P.kode[3 * e + ld] != 0) bits |= 1u << ld;
+    for (int k = 0; k < 9; ++k) {
+      double b = 0.0, v = 0.0;
+      if (k < ncone) {
+        const int64_t dof = 3 * (int64_t)(P.kconec[k + 9 * e] - 1) + ld;
+        b = P.bc[3 * k + ld + 27 * e];
+        v = P.vp[dof];
+        if (P.uknown[dof] != 0) bits |= 1u << (3 + k + 9 * ld);
+      }
+      R[k + 9 * ld] = b;
+      R[27 + k + 9 * ld] = v;
+    }
+  }
+  I[0] = (int)bits;
+  I[1] = ncone;
+  for (int k = 0; k < 9; ++k) I[2 + k] = (k < ncone) ? P.kconec[k + 9 * e] - 1 : 0;
+  I[11] = 0;
+}
+
 // fi_acc (3) and d1_acc (9) are this lane's running sums over its elements, kept in
 // shared memory so the 9 x NC accumulators below have the register file to themselves.
 // T: the element's packed quadrature table, staged in shared memory by the caller.
 template <int NC, int MODE, typename R>
-__device__ __forceinline__ void regular_pair(const AsmArgs& P, int e, const double* T, const int* kc, double xi0,
-                                             double xi1, double xi2, int64_t row,
+__device__ __forceinline__ void regular_pair(const AsmArgs& P, int e, const double* T, const double* Rec,
+                                             const int* kc, double xi0, double xi1, double xi2, int64_t row,
                                              double* fi_acc, double* d1) {
+  // mode A: the element's boundary record Rec (shared memory)
+  const unsigned rbits = (MODE == kModeA) ? (unsigned)reinterpret_cast<const int*>(Rec)[kRecInt] : 0u;
   double fi[3] = {0.0, 0.0, 0.0};
   constexpr int NG = (NC == 9) ? 36 : 16;
   const double c3 = P.mat.c3, c4 = P.mat.c4, c5 = P.mat.c5, c6 = P.mat.c6;
@@ -84,7 +123,7 @@ __device__ __forceinline__ void regular_pair(const AsmArgs& P, int e, const doub
     if (MODE == kModeA) {
 #pragma unroll
       for (int ld = 0; ld < 3; ++ld) {
-        if (__ldg(P.kode + 3 * e + ld) == 0) {
+        if (((rbits >> ld) & 1u) == 0) {
           // the element's 3 x NC block added into A by reductions at L2 (no load on the
           // SM's critical path); the batches' CTA barrier orders the additions into an
           // entry, so the sums are deterministic
@@ -98,7 +137,7 @@ __device__ __forceinline__ void regular_pair(const AsmArgs& P, int e, const doub
         } else {
 #pragma unroll
           for (int k = 0; k < NC; ++k) {
-            const double b = __ldg(P.bc + 3 * k + ld + 27 * e);
+            const double b = Rec[k + 9 * ld];
 #pragma unroll
             for (int jj = 0; jj < 3; ++jj) fi[jj] = fma(g[k][sym_idx(jj, ld)], b, fi[jj]);
           }
@@ -163,10 +202,10 @@ __device__ __forceinline__ void regular_pair(const AsmArgs& P, int e, const doub
     if (MODE == kModeA) {
 #pragma unroll
       for (int ld = 0; ld < 3; ++ld) {
-        if (__ldg(P.kode + 3 * e + ld) == 0) {
+        if (((rbits >> ld) & 1u) == 0) {
 #pragma unroll
           for (int k = 0; k < NC; ++k) {
-            const double b = __ldg(P.bc + 3 * k + ld + 27 * e);
+            const double b = Rec[k + 9 * ld];
 #pragma unroll
             for (int jj = 0; jj < 3; ++jj) fi[jj] = fma(-h[k][jj + 3 * ld], b, fi[jj]);
           }
@@ -176,12 +215,12 @@ __device__ __forceinline__ void regular_pair(const AsmArgs& P, int e, const doub
 #pragma unroll
           for (int k = 0; k < NC; ++k) {
             const int64_t dof = 3 * (int64_t)kc[k] + ld;
-            if (__ldg(P.uknown + dof) == 0) {
+            if (((rbits >> (3 + k + 9 * ld)) & 1u) == 0) {
               double* col = P.A + dof * P.lda + row;
 #pragma unroll
               for (int jj = 0; jj < 3; ++jj) atomicAdd(col + jj, h[k][jj + 3 * ld]);
             } else {
-              const double v = __ldg(P.vp + dof);
+              const double v = Rec[27 + k + 9 * ld];
 #pragma unroll
               for (int jj = 0; jj < 3; ++jj) fi[jj] = fma(-h[k][jj + 3 * ld], v, fi[jj]);
             }
@@ -214,12 +253,13 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
 
 // Dynamic shared memory of the regular tile: two buffers of one quadrature table per
 // warp (the batch being integrated and the next one, copied in meanwhile).
-constexpr int kTabSmem = 2 * kBatch * kTabStride * (int)sizeof(double);
+constexpr int kTabSmem = 2 * kBatch * (kTabStride + kRecD) * (int)sizeof(double);
 
 template <int MODE, int PREC>
 __device__ __forceinline__ void regular_tile(const AsmArgs& P, int tile) {
   __shared__ double s_red[kBatch][32][12];
-  extern __shared__ __align__(16) double s_tab[];  // [2][kBatch][kTabStride]
+  extern __shared__ __align__(16) double s_tab[];  // [2][kBatch][kTabStride], then [2][kBatch][kRecD]
+  double* s_rec = s_tab + 2 * kBatch * kTabStride;
   const int w = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   // each warp copies its own next element's table (16-byte cp.async, 270 per table)
@@ -231,6 +271,11 @@ __device__ __forceinline__ void regular_tile(const AsmArgs& P, int tile) {
         const char* src = reinterpret_cast<const char*>(P.tab + (int64_t)e * kTabStride);
         char* dst = reinterpret_cast<char*>(s_tab + ((b & 1) * kBatch + w) * kTabStride);
         for (int i = lane; i < kTabStride * 8 / 16; i += 32) cp_async16(dst + 16 * i, src + 16 * i);
+        if (MODE == kModeA) {  // and its boundary record
+          const char* rs = reinterpret_cast<const char*>(P.rec + (int64_t)e * kRecD);
+          char* rd = reinterpret_cast<char*>(s_rec + ((b & 1) * kBatch + w) * kRecD);
+          if (lane < kRecD * 8 / 16) cp_async16(rd + 16 * lane, rs + 16 * lane);
+        }
       }
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
@@ -252,13 +297,15 @@ __device__ __forceinline__ void regular_tile(const AsmArgs& P, int tile) {
     asm volatile("cp.async.wait_group 1;" ::: "memory");  // this batch's table is in
     __syncwarp();
     const double* T = s_tab + ((b & 1) * kBatch + w) * kTabStride;
+    const double* R = s_rec + ((b & 1) * kBatch + w) * kRecD;
     if (e >= 0) {
-      const int ncone = __ldg(P.nconec + e);
+      const int* RI = reinterpret_cast<const int*>(R) + kRecInt;
+      const int ncone = (MODE == kModeA) ? RI[1] : __ldg(P.nconec + e);
       int kc[9];
       bool sing = false;
 #pragma unroll
       for (int m = 0; m < 9; ++m) {
-        kc[m] = (m < ncone) ? __ldg(P.kconec + m + 9 * e) - 1 : 0;
+        kc[m] = (MODE == kModeA) ? RI[2 + m] : ((m < ncone) ? __ldg(P.kconec + m + 9 * e) - 1 : 0);
         sing |= (m < ncone) && (kc[m] == in);
       }
       bool far32 = false;
@@ -283,14 +330,14 @@ __device__ __forceinline__ void regular_tile(const AsmArgs& P, int tile) {
       if (active && !sing) {
         if (ncone == 9) {
           if (far32)
-            regular_pair<9, MODE, float>(P, e, T, kc, xi0, xi1, xi2, row, fi, d1);
+            regular_pair<9, MODE, float>(P, e, T, R, kc, xi0, xi1, xi2, row, fi, d1);
           else
-            regular_pair<9, MODE, double>(P, e, T, kc, xi0, xi1, xi2, row, fi, d1);
+            regular_pair<9, MODE, double>(P, e, T, R, kc, xi0, xi1, xi2, row, fi, d1);
         } else {
           if (far32)
-            regular_pair<6, MODE, float>(P, e, T, kc, xi0, xi1, xi2, row, fi, d1);
+            regular_pair<6, MODE, float>(P, e, T, R, kc, xi0, xi1, xi2, row, fi, d1);
           else
-            regular_pair<6, MODE, double>(P, e, T, kc, xi0, xi1, xi2, row, fi, d1);
+            regular_pair<6, MODE, double>(P, e, T, R, kc, xi0, xi1, xi2, row, fi, d1);
         }
       }
     }
@@ -640,6 +687,10 @@ int launch_ghmat8(bem_ctx* c, int precision) {
   P.A = c->A.p;
   P.lda = lda;
   P.FI = c->FI.p;
+  BEM_CUDA(c, c->erec.alloc((size_t)c->ne * kRecD));
+  elem_record_kernel<<<(c->ne + 127) / 128, 128, 0, c->stream>>>(P, c->erec.p);
+  BEM_LAUNCH_CHECK(c);
+  P.rec = c->erec.p;
   const int tiles = (c->n + 31) / 32;
   static DeviceOnce attr;  // the tables' double buffer is above the 48 KB default
   if (attr.pending()) {

@@ -160,6 +160,7 @@ struct bem_ctx {
 
   // geometry (reference layout) and the packed assembly table
   bem::DBuf<double> eta1, eta2, eta3, xja, xg1, xg2, xg3, ff, tab;
+  bem::DBuf<double> erec;  // per-element boundary records of the assembly (mode A)
   bool have_geometry = false;
 
   // system
