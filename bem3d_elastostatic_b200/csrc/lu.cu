@@ -587,27 +587,24 @@ __device__ __forceinline__ bool coop_barrier(unsigned* barrier, unsigned target,
 }
 
 // The diagonal block [j0, t0)^2 of a window-pivoted FP32 panel in one cooperative
-// launch: the 32-wide sub-panels in turn, two grid barriers each:
+// launch: the 32-wide sub-panels in turn, each in three phases separated by grid
+// barriers (two per sub-panel) instead of kernel boundaries:
+//   A  every CTA's warp 0 stages and factors the 32 x 32 window (redundantly; the
+//      interchanges composed into a gather on the way); CTA 0 records the pivots and
+//      the first exact zero pivot;
 //   B  the sub-panel's vectors, one thread each, spread over the CTAs in contiguous
 //      runs: every column c in [r0 + 32, t0) eliminated with the window's steps
 //      (window_panel_kernel's column operations, with each multiplier formed by the
 //      pivot's reciprocal), every row of the block outside the window gathered
 //      through the interchanges and, below the window, solved with the window's
 //      unit-lower triangle (trsm_small_kernel's operations);
-//   C  warps 0-7: the rank-32 update of the block's trailing part,
-//      S(q, q) -= S(q, w) S(w, q) with q = [r0 + 32, t0) and w the window, in 64 x 64
-//      tiles (FP32 FMA), except the next window's 32 x 32 block; CTA 0 stores the
-//      factored window.  Warp 8 meanwhile forms the next window itself (its old
-//      values minus the same update, summed in the same order) and factors it
-//      (window_lu_warp_f32, the interchanges composed into a gather), so the window LU
-//      overlaps the tile updates instead of following them.  Every CTA does this
-//      redundantly and identically; CTA 0 records the pivots and the first exact zero
-//      pivot.  The window state is double-buffered between sub-panels.
+//   C  the rank-32 update of the block's trailing part, S(q, q) -= S(q, w) S(w, q)
+//      with q = [r0 + 32, t0) and w the window, in 64 x 64 tiles (FP32 FMA), and
+//      CTA 0 stores the factored window (every CTA has read it by now).
 // Every read of S goes through L2 (__ldcg): the other CTAs' writes of the previous
 // phase are ordered by the barrier, never by this SM's L1.  The rows and columns
 // outside the block follow per panel (permute_panel_kernel, the blocked TRSMs).
-constexpr int kCoopThreads = 288;  // 8 tile warps and the window warp
-constexpr int kCoopTileThreads = 256;
+constexpr int kCoopThreads = 256;
 constexpr int kCoopTile = 64;
 constexpr int kCoopMaxCtas = 160;  // one CTA per SM (148 on a B200)
 __global__ void __launch_bounds__(kCoopThreads, 1)
@@ -615,47 +612,38 @@ __global__ void __launch_bounds__(kCoopThreads, 1)
                       int* status, unsigned long long wait_ns) {
   constexpr int W = kPanelW;
   constexpr int TP = kCoopTile + 4;  // strip pitch: 16-byte rows, 4-way store conflicts at most
-  constexpr int LUW = kCoopTileThreads / 32;  // the window warp
-  __shared__ float D[2][W][W + 1];  // D[c][j] = S(r0 + j, r0 + c), factored
-  __shared__ float rdg[2][W];       // reciprocal pivots (0 for an exact zero pivot)
-  __shared__ int s_p[2][W], s_g[2][W];
-  __shared__ float Lw[W][W + 1];    // Lw[k][j] = S(q0 + j, r0 + k): the next window's L block
+  __shared__ float D[W][W + 1];     // D[c][j] = S(r0 + j, r0 + c)
+  __shared__ float rdg[W];          // reciprocal pivots (0 for an exact zero pivot)
+  __shared__ int s_p[W], s_g[W];
   __shared__ __align__(16) float Ls[W][TP];  // Ls[k][r] = S(q0 + tr + r, r0 + k)
   __shared__ __align__(16) float Us[W][TP];  // Us[k][c] = S(r0 + k, q0 + tc + c)
   __shared__ int s_abort;
-  const int G = gridDim.x, g = blockIdx.x, tid = threadIdx.x, lane = tid & 31, wp = tid >> 5;
-  // the window warp: factor D[buf] (the window at r0), its reciprocal pivots, and on
-  // CTA 0 the pivots and the first exact zero pivot
-  auto factor_window = [&](int buf, int r0) {
-    window_lu_warp_f32(D[buf], s_p[buf], s_g[buf], lane);
-    rdg[buf][lane] = (D[buf][lane][lane] != 0.f) ? __frcp_rn(D[buf][lane][lane]) : 0.f;
-    if (g == 0) {
-      piv[r0 + lane] = r0 + s_p[buf][lane];
-      if (lane == 0) {
-        for (int t = 0; t < W; ++t)
-          if (D[buf][t][t] == 0.f) {
-            if (status[1] == 0) status[1] = r0 + t + 1;
-            break;
-          }
+  const int G = gridDim.x, g = blockIdx.x, tid = threadIdx.x, lane = tid & 31;
+  unsigned target = bar_base;
+  for (int r0 = j0; r0 < t0; r0 += W) {
+    const int q0 = r0 + W, m = t0 - q0;
+    // A: the window
+    if (tid < W) {
+      float wv[W];  // every load in flight before the first store
+#pragma unroll
+      for (int cc = 0; cc < W; ++cc) wv[cc] = __ldcg(S + r0 + lane + (int64_t)(r0 + cc) * lda);
+#pragma unroll
+      for (int cc = 0; cc < W; ++cc) D[cc][lane] = wv[cc];
+      __syncwarp();
+      window_lu_warp_f32(D, s_p, s_g, lane);
+      rdg[lane] = (D[lane][lane] != 0.f) ? __frcp_rn(D[lane][lane]) : 0.f;
+      if (g == 0) {
+        piv[r0 + lane] = r0 + s_p[lane];
+        if (lane == 0) {
+          for (int t = 0; t < W; ++t)
+            if (D[t][t] == 0.f) {
+              if (status[1] == 0) status[1] = r0 + t + 1;
+              break;
+            }
+        }
       }
     }
-    __syncwarp();
-  };
-  if (wp == LUW) {  // the first window, as it stands
-    float wv[W];  // every load in flight before the first store
-#pragma unroll
-    for (int cc = 0; cc < W; ++cc) wv[cc] = __ldcg(S + j0 + lane + (int64_t)(j0 + cc) * lda);
-#pragma unroll
-    for (int cc = 0; cc < W; ++cc) D[0][cc][lane] = wv[cc];
-    __syncwarp();
-    factor_window(0, j0);
-  }
-  __syncthreads();
-  unsigned target = bar_base;
-  int cur = 0;
-  for (int r0 = j0; r0 < t0; r0 += W, cur ^= 1) {
-    const int q0 = r0 + W, m = t0 - q0;
-    const float(*Dc)[W + 1] = D[cur];
+    __syncthreads();
     // B: columns [q0, t0), then rows [j0, r0) and [q0, t0)
     {
       const int nabove = r0 - j0;
@@ -678,12 +666,12 @@ __global__ void __launch_bounds__(kCoopThreads, 1)
           // and a fused multiply-add each, not a division
 #pragma unroll
           for (int t = 0; t < W; ++t) {
-            const float rp = rdg[cur][t];
+            const float rp = rdg[t];
             if (rp != 0.f) {
               const float l = x[t] * rp;
               x[t] = l;
 #pragma unroll
-              for (int j = t + 1; j < W; ++j) x[j] -= l * Dc[t][j];
+              for (int j = t + 1; j < W; ++j) x[j] -= l * D[t][j];
             }
           }
 #pragma unroll
@@ -694,13 +682,13 @@ __global__ void __launch_bounds__(kCoopThreads, 1)
           const int r = i < nabove ? j0 + i : q0 + (i - nabove);
           float y[W];
 #pragma unroll
-          for (int b = 0; b < W; ++b) y[b] = __ldcg(S + r + (int64_t)(r0 + s_g[cur][b]) * lda);
+          for (int b = 0; b < W; ++b) y[b] = __ldcg(S + r + (int64_t)(r0 + s_g[b]) * lda);
           if (r >= q0) {
 #pragma unroll
             for (int b = 0; b < W; ++b) {
               float a = y[b];
 #pragma unroll
-              for (int k = 0; k < b; ++k) a -= y[k] * Dc[b][k];  // U(k, b) = S(r0 + k, r0 + b)
+              for (int k = 0; k < b; ++k) a -= y[k] * D[b][k];  // U(k, b) = S(r0 + k, r0 + b)
               y[b] = a;
             }
           }
@@ -711,95 +699,70 @@ __global__ void __launch_bounds__(kCoopThreads, 1)
     }
     target += (unsigned)G;
     if (!coop_barrier(barrier, target, status, wait_ns, &s_abort)) return;
-    // C
-    if (wp == LUW) {
-      if (m > 0) {
-        // the next window: its old values minus this sub-panel's update of it
-        float wv[W], uv[W];
-#pragma unroll
-        for (int k = 0; k < W; ++k) Lw[k][lane] = __ldcg(S + q0 + lane + (int64_t)(r0 + k) * lda);
-#pragma unroll
-        for (int j = 0; j < W; ++j) wv[j] = __ldcg(S + q0 + j + (int64_t)(q0 + lane) * lda);
-#pragma unroll
-        for (int k = 0; k < W; ++k) uv[k] = __ldcg(S + r0 + k + (int64_t)(q0 + lane) * lda);
-        __syncwarp();
-        float(*Dn)[W + 1] = D[cur ^ 1];
-#pragma unroll
-        for (int j = 0; j < W; ++j) {
-          float acc = 0.f;
-#pragma unroll
-          for (int k = 0; k < W; ++k) acc = fmaf(Lw[k][j], uv[k], acc);
-          Dn[lane][j] = wv[j] - acc;
-        }
-        __syncwarp();
-        factor_window(cur ^ 1, q0);
+    // C: the trailing tiles; CTA 0 stores the window
+    if (g == 0)
+      for (int i = tid; i < W * W; i += blockDim.x) {
+        const int j = i % W, cc = i / W;
+        S[r0 + j + (int64_t)(r0 + cc) * lda] = D[cc][j];
       }
-    } else {
-      if (g == 0)
-        for (int i = tid; i < W * W; i += kCoopTileThreads) {
-          const int j = i % W, cc = i / W;
-          S[r0 + j + (int64_t)(r0 + cc) * lda] = Dc[cc][j];
-        }
-      const int nt = (m + kCoopTile - 1) / kCoopTile;
-      for (int tau = g; tau < nt * nt; tau += G) {
-        const int tr = (tau % nt) * kCoopTile, tc = (tau / nt) * kCoopTile;
-        const int ri = (tid % 16) * 4, ci = (tid / 16) * 4;
-        // every load of the tile in flight before the first use: the strips, then C
-        constexpr int NS = W * kCoopTile / kCoopTileThreads;
-        float lv[NS], uv[NS];
+    const int nt = (m + kCoopTile - 1) / kCoopTile;
+    for (int tau = g; tau < nt * nt; tau += G) {
+      const int tr = (tau % nt) * kCoopTile, tc = (tau / nt) * kCoopTile;
+      const int ri = (tid % 16) * 4, ci = (tid / 16) * 4;
+      // every load of the tile in flight before the first use: the strips, then C
+      constexpr int NS = W * kCoopTile / kCoopThreads;
+      float lv[NS], uv[NS];
 #pragma unroll
-        for (int u = 0; u < NS; ++u) {
-          const int i = tid + u * kCoopTileThreads;
-          const int rr = i % kCoopTile, k = i / kCoopTile;
-          lv[u] = (tr + rr < m) ? __ldcg(S + q0 + tr + rr + (int64_t)(r0 + k) * lda) : 0.f;
-        }
+      for (int u = 0; u < NS; ++u) {
+        const int i = tid + u * kCoopThreads;
+        const int rr = i % kCoopTile, k = i / kCoopTile;
+        lv[u] = (tr + rr < m) ? __ldcg(S + q0 + tr + rr + (int64_t)(r0 + k) * lda) : 0.f;
+      }
 #pragma unroll
-        for (int u = 0; u < NS; ++u) {
-          const int i = tid + u * kCoopTileThreads;
-          const int k = i % W, cc = i / W;
-          uv[u] = (tc + cc < m) ? __ldcg(S + r0 + k + (int64_t)(q0 + tc + cc) * lda) : 0.f;
-        }
-        float4 cv[4];
+      for (int u = 0; u < NS; ++u) {
+        const int i = tid + u * kCoopThreads;
+        const int k = i % W, cc = i / W;
+        uv[u] = (tc + cc < m) ? __ldcg(S + r0 + k + (int64_t)(q0 + tc + cc) * lda) : 0.f;
+      }
+      float4 cv[4];
 #pragma unroll
-        for (int v = 0; v < 4; ++v)
-          cv[v] = (tr + ri < m && tc + ci + v < m)
-                      ? __ldcg(reinterpret_cast<const float4*>(S + q0 + tr + ri + (int64_t)(q0 + tc + ci + v) * lda))
-                      : make_float4(0.f, 0.f, 0.f, 0.f);
+      for (int v = 0; v < 4; ++v)
+        cv[v] = (tr + ri < m && tc + ci + v < m)
+                    ? __ldcg(reinterpret_cast<const float4*>(S + q0 + tr + ri + (int64_t)(q0 + tc + ci + v) * lda))
+                    : make_float4(0.f, 0.f, 0.f, 0.f);
 #pragma unroll
-        for (int u = 0; u < NS; ++u) {
-          const int i = tid + u * kCoopTileThreads;
-          Ls[i / kCoopTile][i % kCoopTile] = lv[u];
-          Us[i % W][i / W] = uv[u];
-        }
-        asm volatile("bar.sync 1, %0;" ::"n"(kCoopTileThreads) : "memory");
-        float acc[4][4] = {};
+      for (int u = 0; u < NS; ++u) {
+        const int i = tid + u * kCoopThreads;
+        Ls[i / kCoopTile][i % kCoopTile] = lv[u];
+        Us[i % W][i / W] = uv[u];
+      }
+      __syncthreads();
+      float acc[4][4] = {};
 #pragma unroll 8
-        for (int k = 0; k < W; ++k) {
-          const float4 a = *reinterpret_cast<const float4*>(&Ls[k][ri]);
-          const float4 b = *reinterpret_cast<const float4*>(&Us[k][ci]);
-          const float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
+      for (int k = 0; k < W; ++k) {
+        const float4 a = *reinterpret_cast<const float4*>(&Ls[k][ri]);
+        const float4 b = *reinterpret_cast<const float4*>(&Us[k][ci]);
+        const float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
 #pragma unroll
-          for (int u = 0; u < 4; ++u)
+        for (int u = 0; u < 4; ++u)
 #pragma unroll
-            for (int v = 0; v < 4; ++v) acc[u][v] = fmaf(av[u], bv[v], acc[u][v]);
-        }
-        // m is a multiple of 32: a 4-row group lies wholly inside or outside the block;
-        // the next window's block [q0, q0 + 32)^2 is the window warp's
-        if (tr + ri < m) {
+          for (int v = 0; v < 4; ++v) acc[u][v] = fmaf(av[u], bv[v], acc[u][v]);
+      }
+      // m is a multiple of 32: a 4-row group lies wholly inside or outside the block
+      if (tr + ri < m) {
 #pragma unroll
-          for (int v = 0; v < 4; ++v) {
-            if (tc + ci + v < m && !(tr + ri < W && tc + ci + v < W)) {
-              float4 o = cv[v];
-              o.x -= acc[0][v];
-              o.y -= acc[1][v];
-              o.z -= acc[2][v];
-              o.w -= acc[3][v];
-              *reinterpret_cast<float4*>(S + q0 + tr + ri + (int64_t)(q0 + tc + ci + v) * lda) = o;
-            }
+        for (int v = 0; v < 4; ++v) {
+          if (tc + ci + v < m) {
+            float4 o = cv[v];
+            o.x -= acc[0][v];
+            o.y -= acc[1][v];
+            o.z -= acc[2][v];
+            o.w -= acc[3][v];
+            *reinterpret_cast<float4*>(S + q0 + tr + ri + (int64_t)(q0 + tc + ci + v) * lda) = o;
           }
         }
-        asm volatile("bar.sync 1, %0;" ::"n"(kCoopTileThreads) : "memory");
       }
+      __syncthreads();
     }
     target += (unsigned)G;
     if (!coop_barrier(barrier, target, status, wait_ns, &s_abort)) return;
