@@ -59,7 +59,9 @@ def test_adjoint_matches_finite_differences():
         q.load_mesh()
         q.precompute_element_geometry()
         q.ghmat8()
-        x = torch.as_tensor(q.solve_linear_system("fp64"))
+        # the objective from the refined FP64 solve (FP64 rounding of the stored system):
+        # the central difference then carries ~1e-10 of rounding, not the LU's ~1e-13 / h
+        x = torch.as_tensor(q.solve_linear_system("fp64-ir", tol=1e-15, max_iter=20))
         u, t = reorganize(mesh, x, torch.tensor(mesh.mu, dtype=torch.float64))
         return float(compliance(mesh, torch.as_tensor(Xv), u, t, inner))
 
@@ -71,7 +73,9 @@ def test_adjoint_matches_finite_differences():
             Xp[node, d] += h
             Xm[node, d] -= h
             fd = (J_at(X=Xp) - J_at(X=Xm)) / (2 * h)
-            assert abs(fd - gX[node, d]) <= 1e-6 * np.abs(gX).max(), (node, d, fd, gX[node, d])
+            # per entry at 1e-6 (entries below 1e-3 of the largest at 1e-6 of the largest)
+            assert abs(fd - gX[node, d]) <= 1e-6 * max(abs(gX[node, d]), 1e-3 * np.abs(gX).max()), (
+                node, d, fd, gX[node, d])
     fd_nu = (J_at(nu=nu0 + h) - J_at(nu=nu0 - h)) / (2 * h)
     assert abs(fd_nu - gnu) <= 1e-6 * abs(gnu)
     fd_mu = (J_at(mu=mu0 + h) - J_at(mu=mu0 - h)) / (2 * h)
