@@ -35,7 +35,7 @@ constexpr int UM = 128;                 // tile rows (UMMA M)
 constexpr int UN = 256;                 // tile columns (UMMA N)
 constexpr int UK = 64;                  // K chunk per TMA box (128 bytes of BF16)
 constexpr int kMaxK = 1024;             // largest panel width
-constexpr int kRasterW = 8;             // column tiles per raster group
+constexpr int kRasterW = 16;            // column tiles per raster group
 constexpr int A_TILE = UM * UK * 2;     // 16 KB
 constexpr int B_TILE = UN * UK * 2;     // 32 KB
 // Shared memory: a ring of K chunks, then the barriers, then the epilogue's staging
