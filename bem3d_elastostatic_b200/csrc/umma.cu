@@ -1,23 +1,26 @@
-// Trailing update of the FP32 LU on the 5th-generation tensor cores (tcgen05).
+// Tensor-core products of the FP32 LU on the 5th-generation tensor cores (tcgen05):
 //
-//   C (m x n, FP32, column-major, ldc) -= A (m x K) * B (K x n),  K = the panel width
+//   C (m x n, FP32, column-major, ldc) -= A (m x K) * B (K x n)   (the trailing update)
+//   C = A * B                                                     (the block TRSMs)
 //
-// FP32 operands are split once per call into BF16 hi + lo parts (split_a_kernel /
+// FP32 operands are split once per call into BF16 hi (+ lo) parts (split_a_kernel /
 // split_b_kernel), stored K-major so the Tensor Memory Accelerator can bring 64-wide
 // K chunks into 128-byte-swizzled shared memory.  One thread issues, per K chunk and
-// per 16-wide K step, the three products hi*hi + hi*lo + lo*hi as tcgen05.mma
-// (kind::f16, BF16 inputs, FP32 accumulation in tensor memory, M = 128, N = 256); a
-// tcgen05.commit signals an mbarrier when they are done, and eight warps drain the
-// 128 x 256 accumulator with tcgen05.ld (one TMEM lane = one row of C): they stage
-// -acc for 128 x 32 boxes in shared memory and add each box into C with a bulk tensor
-// reduction (cp.reduce.async.bulk.tensor .add.f32), so the L2 performs the
-// read-modify-write of C and the SM never waits on a load of C.  Every element of C
-// receives exactly one addition per call, C + (-acc), the same IEEE operation as
-// C - acc: the result is deterministic.
+// per 16-wide K step, one product hi*hi or the three products hi*hi + hi*lo + lo*hi as
+// tcgen05.mma (kind::f16, BF16 inputs, FP32 accumulation in tensor memory, M = 128,
+// N = 256); a tcgen05.commit signals an mbarrier when they are done, and eight warps
+// drain the 128 x 256 accumulator with tcgen05.ld (one TMEM lane = one row of C): they
+// stage 128 x 32 boxes in shared memory and either add each box into C with a bulk
+// tensor reduction (cp.reduce.async.bulk.tensor .add.f32, staging -acc), so the L2
+// performs the read-modify-write of C and the SM never waits on a load of C, or store
+// it (cp.async.bulk.tensor).  Every element of C receives exactly one addition per call,
+// C + (-acc), the same IEEE operation as C - acc: the result is deterministic.  With a
+// triangular operand a tile runs only the K chunks that meet its nonzero part.
 //
-// Every mbarrier wait is bounded (the context's wait limit, 2 s by default): on timeout the kernel records an error word, the
-// other roles stop at their next wait, the producer waits (bounded) for its own copies
-// and the MMA warp for its own MMAs, and the tensor memory is freed.
+// Every mbarrier wait is bounded (the context's wait limit, 2 s by default): on timeout
+// the kernel records an error word, the other roles stop at their next wait, the
+// producer waits (bounded) for its own copies and the MMA warp for its own MMAs, and the
+// tensor memory is freed.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cudaTypedefs.h>
