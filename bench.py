@@ -53,6 +53,7 @@ process per GPU under torchrun) and value = max-over-ranks step time / N.
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -502,13 +503,22 @@ def leg_adjoint(device, fd_coords=2, m=16):
     try:
         Jw = forward(X0, mu0, nu0, grad=True)[0]  # warm-up of the forward and the backward path
         Jw.backward()
+        gc.collect()
         t0 = time.perf_counter()
         J, X, mu, nu, x = forward(X0, mu0, nu0, grad=True)
         t1 = time.perf_counter()
-        J.backward()
-        t2 = time.perf_counter()
+        J.backward(retain_graph=True)
         g = X.grad.numpy().copy()
         gnu = float(nu.grad)
+        # the backward pass (transposed solve, backward assembly, torch's part) is short
+        # next to host noise: the median of three passes over the same graph
+        tb = []
+        for _ in range(3):
+            X.grad, mu.grad, nu.grad = None, None, None
+            gc.collect()
+            tb0 = time.perf_counter()
+            J.backward(retain_graph=True)
+            tb.append(time.perf_counter() - tb0)
         r = np.linalg.norm(X0, axis=1)
         ur = (x.detach().numpy().reshape(-1, 3) * X0).sum(1) / r
         exact = lame_sphere_displacement(r, 1.0, 2.0, 1.0, 2 * mu0 * (1 + nu0), nu0)
@@ -526,7 +536,8 @@ def leg_adjoint(device, fd_coords=2, m=16):
                 errs.append(abs(fd - g[i, d]) / max(abs(fd), 1e-300))
             fdn = (float(forward(X0, mu0, nu0 + h)[0]) - float(forward(X0, mu0, nu0 - h)[0])) / (2 * h)
         return {"workload": f"hollow sphere a=1 b=2, m={m}: {mesh.ne} quad9, {mesh.ndof} DOF",
-                "forward_s_wall": t1 - t0, "backward_s_wall": t2 - t1,
+                "forward_s_wall": t1 - t0, "backward_s_wall": float(np.median(tb)),
+                "backward_s_wall_passes": tb,
                 "lame_ur_max_rel_err": float(np.abs(ur - exact).max() / np.abs(exact).max()),
                 "fd_coordinates": fd_coords, "fd_rel_err_max": float(max(errs)) if errs else None,
                 "fd_nu_rel_err": abs(fdn - gnu) / abs(fdn)}
