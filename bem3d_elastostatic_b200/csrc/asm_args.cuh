@@ -28,6 +28,13 @@ struct AsmArgs {
   double* FI;  // mode A only
   double* G;   // mode HG only
   int64_t ldg;
+  // mode A, last wave split (assembly.cu): tiles >= tail0 run as nparts pieces, each
+  // over its share of the element batches; pieces >= 1 add into scratch that
+  // tail_merge_*_kernel then adds into A and FI.  nparts <= 1: no split.
+  int tail0, nparts, scr_cols;
+  const int* slot;  // [(nparts - 1) * n]: scratch column slot of a node in piece p, or -1
+  double* scr;      // [piece item][3 * scr_cols][96]: the pieces' A column segments
+  double* fd;       // [piece item][32][12]: the pieces' FI and diagonal-block partial sums
 };
 
 // Batched H/G assembly of many systems (assembly.cu): d_args[i] describes system i

@@ -21,6 +21,7 @@
 // The column swap (:125-218) uses a per-(node, component) lookup built on the host
 // from the same node->element adjacency the reference scans (uknown / vp).
 #include <algorithm>
+#include <cstdlib>
 
 #include "asm_args.cuh"
 #include "common.cuh"
@@ -78,10 +79,12 @@ __global__ void elem_record_kernel(AsmArgs P, double* rec) {
 // fi_acc (3) and d1_acc (9) are this lane's running sums over its elements, kept in
 // shared memory so the 9 x NC accumulators below have the register file to themselves.
 // T: the element's packed quadrature table, staged in shared memory by the caller.
+// Mode A adds column kc[k] (3 DOFs) of the element's block at Ab + dof * ald + row: A
+// itself, or a piece's scratch, whose columns are the piece's node slots.
 template <int NC, int MODE, typename R>
 __device__ __forceinline__ void regular_pair(const AsmArgs& P, int e, const double* T, const double* Rec,
-                                             const int* kc, double xi0, double xi1, double xi2, int64_t row,
-                                             double* fi_acc, double* d1) {
+                                             const int* kc, double xi0, double xi1, double xi2, double* Ab,
+                                             int64_t ald, int64_t row, double* fi_acc, double* d1) {
   // mode A: the element's boundary record Rec (shared memory)
   const unsigned rbits = (MODE == kModeA) ? (unsigned)reinterpret_cast<const int*>(Rec)[kRecInt] : 0u;
   double fi[3] = {0.0, 0.0, 0.0};
@@ -130,7 +133,7 @@ __device__ __forceinline__ void regular_pair(const AsmArgs& P, int e, const doub
           const double mu = P.mat.mu;
 #pragma unroll
           for (int k = 0; k < NC; ++k) {
-            double* col = P.A + (3 * (int64_t)kc[k] + ld) * P.lda + row;
+            double* col = Ab + (3 * (int64_t)kc[k] + ld) * ald + row;
 #pragma unroll
             for (int jj = 0; jj < 3; ++jj) atomicAdd(col + jj, -(g[k][sym_idx(jj, ld)] * mu));
           }
@@ -216,7 +219,7 @@ __device__ __forceinline__ void regular_pair(const AsmArgs& P, int e, const doub
           for (int k = 0; k < NC; ++k) {
             const int64_t dof = 3 * (int64_t)kc[k] + ld;
             if (((rbits >> (3 + k + 9 * ld)) & 1u) == 0) {
-              double* col = P.A + dof * P.lda + row;
+              double* col = Ab + dof * ald + row;
 #pragma unroll
               for (int jj = 0; jj < 3; ++jj) atomicAdd(col + jj, h[k][jj + 3 * ld]);
             } else {
@@ -255,8 +258,10 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
 // warp (the batch being integrated and the next one, copied in meanwhile).
 constexpr int kTabSmem = 2 * kBatch * (kTabStride + kRecD) * (int)sizeof(double);
 
+// Tile `tile` (32 collocation nodes) against the element batches [b0, b1); piece
+// `part` >= 1 of a split tile adds into its scratch instead of A and FI.
 template <int MODE, int PREC>
-__device__ __forceinline__ void regular_tile(const AsmArgs& P, int tile) {
+__device__ __forceinline__ void regular_tile(const AsmArgs& P, int tile, int part, int b0, int b1) {
   __shared__ double s_red[kBatch][32][12];
   extern __shared__ __align__(16) double s_tab[];  // [2][kBatch][kTabStride], then [2][kBatch][kRecD]
   double* s_rec = s_tab + 2 * kBatch * kTabStride;
@@ -265,7 +270,7 @@ __device__ __forceinline__ void regular_tile(const AsmArgs& P, int tile) {
   // each warp copies its own next element's table (16-byte cp.async, 270 per table)
   // while it integrates the current one: the table loads leave the dependent chain
   auto prefetch = [&](int b) {
-    if (b < P.nbatches) {
+    if (b < b1) {
       const int e = __ldg(P.batches + kBatch * b + w);
       if (e >= 0) {
         const char* src = reinterpret_cast<const char*>(P.tab + (int64_t)e * kTabStride);
@@ -285,13 +290,19 @@ __device__ __forceinline__ void regular_tile(const AsmArgs& P, int tile) {
   const int in = P.in0 + (active ? local : 0);
   const double xi0 = P.x[in], xi1 = P.y[in], xi2 = P.z[in];
   const int64_t row = 3 * (int64_t)local;
+  // where the element blocks go: A's rows of this tile, or the piece's scratch item
+  // (96 rows, the piece's node slots as columns)
+  const int64_t item = part > 0 ? (int64_t)(tile - P.tail0) * (P.nparts - 1) + (part - 1) : 0;
+  double* Ab = part > 0 ? P.scr + item * (3 * (int64_t)P.scr_cols) * 96 : P.A;
+  const int64_t ald = part > 0 ? 96 : P.lda;
+  const int64_t arow = part > 0 ? 3 * (int64_t)lane : row;
   double* fi = &s_red[w][lane][0];  // running FI sums of this lane
   double* d1 = &s_red[w][lane][3];  // running rigid-body sums d1
 #pragma unroll
   for (int p = 0; p < 12; ++p) s_red[w][lane][p] = 0.0;
 
-  prefetch(0);
-  for (int b = 0; b < P.nbatches; ++b) {
+  prefetch(b0);
+  for (int b = b0; b < b1; ++b) {
     const int e = __ldg(P.batches + kBatch * b + w);
     prefetch(b + 1);
     asm volatile("cp.async.wait_group 1;" ::: "memory");  // this batch's table is in
@@ -327,17 +338,20 @@ __device__ __forceinline__ void regular_tile(const AsmArgs& P, int tile) {
         const double dx = xi0 - cx, dy = xi1 - cy, dz = xi2 - cz;
         far32 = dx * dx + dy * dy + dz * dz > 12.25 * r2;
       }
+      if (part > 0)  // a piece's columns are its node slots
+#pragma unroll
+        for (int m = 0; m < 9; ++m) kc[m] = (m < ncone) ? __ldg(P.slot + (int64_t)(part - 1) * P.n + kc[m]) : 0;
       if (active && !sing) {
         if (ncone == 9) {
           if (far32)
-            regular_pair<9, MODE, float>(P, e, T, R, kc, xi0, xi1, xi2, row, fi, d1);
+            regular_pair<9, MODE, float>(P, e, T, R, kc, xi0, xi1, xi2, Ab, ald, arow, fi, d1);
           else
-            regular_pair<9, MODE, double>(P, e, T, R, kc, xi0, xi1, xi2, row, fi, d1);
+            regular_pair<9, MODE, double>(P, e, T, R, kc, xi0, xi1, xi2, Ab, ald, arow, fi, d1);
         } else {
           if (far32)
-            regular_pair<6, MODE, float>(P, e, T, R, kc, xi0, xi1, xi2, row, fi, d1);
+            regular_pair<6, MODE, float>(P, e, T, R, kc, xi0, xi1, xi2, Ab, ald, arow, fi, d1);
           else
-            regular_pair<6, MODE, double>(P, e, T, R, kc, xi0, xi1, xi2, row, fi, d1);
+            regular_pair<6, MODE, double>(P, e, T, R, kc, xi0, xi1, xi2, Ab, ald, arow, fi, d1);
         }
       }
     }
@@ -353,7 +367,11 @@ __device__ __forceinline__ void regular_tile(const AsmArgs& P, int tile) {
       for (int p = 0; p < 3; ++p) F[p] += s_red[ww][lane][p];
       for (int p = 0; p < 9; ++p) D[p] += s_red[ww][lane][3 + p];
     }
-    if (MODE == kModeA) {
+    if (part > 0) {  // the piece's partial sums, added by tail_merge_fd_kernel
+      double* o = P.fd + (item * 32 + lane) * 12;
+      for (int p = 0; p < 3; ++p) o[p] = F[p];
+      for (int p = 0; p < 9; ++p) o[3 + p] = D[p];
+    } else if (MODE == kModeA) {
       // diagonal block from the non-singular elements (assembly_mod.f90:192-218)
       for (int ld = 0; ld < 3; ++ld) {
         const int64_t dof = 3 * (int64_t)in + ld;
@@ -375,9 +393,84 @@ __device__ __forceinline__ void regular_tile(const AsmArgs& P, int tile) {
   }
 }
 
+// One CTA per 32-node tile.  With a split last wave (mode A, P.nparts > 1) the CTAs
+// from tail0 on are the pieces of the last tiles, nparts per tile, piece p over the
+// batches [nbatches p / nparts, nbatches (p + 1) / nparts): the last wave ends after
+// about 1 / nparts of a tile's time instead of a whole tile's.
 template <int MODE, int PREC>
 __global__ void __launch_bounds__(256, 1) ghmat_regular_kernel(AsmArgs P) {
-  regular_tile<MODE, PREC>(P, blockIdx.x);
+  if (P.nparts > 1 && (int)blockIdx.x >= P.tail0) {
+    const int i = blockIdx.x - P.tail0, part = i % P.nparts;
+    const int b0 = (int)((int64_t)P.nbatches * part / P.nparts);
+    const int b1 = (int)((int64_t)P.nbatches * (part + 1) / P.nparts);
+    regular_tile<MODE, PREC>(P, P.tail0 + i / P.nparts, part, b0, b1);
+  } else {
+    regular_tile<MODE, PREC>(P, blockIdx.x, 0, 0, P.nbatches);
+  }
+}
+
+// The pieces' A column segments into A: segment (tail tile t, node j, DOF ld) of 96
+// rows, one warp each; the pieces' contributions are summed in piece order and added
+// once, so the result is deterministic.
+__global__ void tail_merge_cols_kernel(AsmArgs P, int ntail) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nseg = (int64_t)ntail * P.n * 3;
+  const int64_t wstride = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t sg = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; sg < nseg; sg += wstride) {
+    const int ld = (int)(sg % 3);
+    const int64_t q = sg / 3;
+    const int j = (int)(q % P.n), t = (int)(q / P.n);
+    const int tile = P.tail0 + t;
+    const int rows = 3 * min(32, P.nrows_nodes - 32 * tile);
+    double acc[3] = {0.0, 0.0, 0.0};
+    bool any = false;
+    for (int p = 1; p < P.nparts; ++p) {
+      const int sl = __ldg(P.slot + (int64_t)(p - 1) * P.n + j);
+      if (sl >= 0) {
+        any = true;
+        const int64_t item = (int64_t)t * (P.nparts - 1) + (p - 1);
+        const double* src = P.scr + (item * 3 * P.scr_cols + 3 * (int64_t)sl + ld) * 96;
+#pragma unroll
+        for (int u = 0; u < 3; ++u) acc[u] += src[lane + 32 * u];
+      }
+    }
+    if (any) {
+      double* dst = P.A + (3 * (int64_t)j + ld) * P.lda + 96 * (int64_t)tile;
+#pragma unroll
+      for (int u = 0; u < 3; ++u)
+        if (lane + 32 * u < rows) dst[lane + 32 * u] += acc[u];
+    }
+  }
+}
+
+// The pieces' FI and diagonal-block partial sums (assembly_mod.f90:192-218), one
+// thread per node of the tail tiles, after tail_merge_cols_kernel.
+__global__ void tail_merge_fd_kernel(AsmArgs P, int ntail) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 32 * ntail) return;
+  const int t = i >> 5, lane = i & 31;
+  const int local = 32 * (P.tail0 + t) + lane;
+  if (local >= P.nrows_nodes) return;
+  const int in = P.in0 + local;
+  const int64_t row = 3 * (int64_t)local;
+  double F[3] = {0.0, 0.0, 0.0}, D[9];
+  for (int p = 0; p < 9; ++p) D[p] = 0.0;
+  for (int p = 1; p < P.nparts; ++p) {
+    const double* o = P.fd + (((int64_t)t * (P.nparts - 1) + (p - 1)) * 32 + lane) * 12;
+    for (int r = 0; r < 3; ++r) F[r] += o[r];
+    for (int r = 0; r < 9; ++r) D[r] += o[3 + r];
+  }
+  for (int ld = 0; ld < 3; ++ld) {
+    const int64_t dof = 3 * (int64_t)in + ld;
+    if (P.uknown[dof] == 0) {
+      double* col = P.A + dof * P.lda + row;
+      for (int r = 0; r < 3; ++r) col[r] += D[r + 3 * ld];
+    } else {
+      const double v = P.vp[dof];
+      for (int r = 0; r < 3; ++r) F[r] -= D[r + 3 * ld] * v;
+    }
+  }
+  for (int r = 0; r < 3; ++r) P.FI[row + r] += F[r];
 }
 
 // ---------------------------------------------------------------------------------
@@ -666,6 +759,88 @@ static int upload_singular_constants(bem_ctx* c) {
   return BEM_OK;
 }
 
+// The last wave of the regular kernel: the tiles beyond the last full wave (rem of
+// them) run as pieces over shares of the batch list, as many pieces per tile as fill
+// the SMs (at most kMaxPieces), so that the kernel ends about (1 - 1 / pieces) of a
+// tile's time earlier.  Pieces >= 1 need a scratch item each: 96 rows by the piece's
+// node slots (the nodes of its elements), at most kTailScratch bytes in all.  Sets
+// P's split fields (nparts = 1: no split) and returns the number of split tiles.
+constexpr int kMaxPieces = 8;
+constexpr size_t kTailScratch = size_t(4) << 30;
+
+static int plan_tail(bem_ctx* c, AsmArgs& P, int tiles, int& rc) {
+  rc = BEM_OK;
+  P.nparts = 1;
+  P.tail0 = tiles;
+  const char* env = std::getenv("BEM_ASM_SPLIT");
+  if (env && std::atoi(env) == 0) return 0;
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ghmat_regular_kernel<kModeA, 0>, 256, kTabSmem) !=
+          cudaSuccess ||
+      occ < 1) {
+    cudaGetLastError();
+    return 0;
+  }
+  const int wave = c->sm_count * occ;
+  const int rem = tiles % wave;
+  if (rem == 0) return 0;
+  int pp = std::min(std::min(kMaxPieces, wave / rem), c->nbatches);
+  for (; pp >= 2; --pp) {
+    if (c->tail_parts != pp) {  // node slots of pieces 1 .. pp-1 (cached per mesh)
+      std::vector<int> slot((size_t)(pp - 1) * c->n, -1);
+      int cols = 0;
+      for (int p = 1; p < pp; ++p) {
+        const int b0 = (int)((int64_t)c->nbatches * p / pp), b1 = (int)((int64_t)c->nbatches * (p + 1) / pp);
+        int* sl = slot.data() + (size_t)(p - 1) * c->n;
+        std::vector<int> nodes;
+        for (size_t i = (size_t)b0 * kBatch; i < (size_t)b1 * kBatch; ++i) {
+          const int e = c->h_batches[i];
+          if (e < 0) continue;
+          for (int m = 0; m < c->h_nconec[e]; ++m) nodes.push_back(c->h_kconec[m + 9 * (size_t)e] - 1);
+        }
+        std::sort(nodes.begin(), nodes.end());
+        nodes.erase(std::unique(nodes.begin(), nodes.end()), nodes.end());
+        for (size_t k = 0; k < nodes.size(); ++k) sl[nodes[k]] = (int)k;
+        cols = std::max(cols, (int)nodes.size());
+      }
+      const size_t bytes = (size_t)rem * (pp - 1) * ((size_t)3 * cols * 96 + 32 * 12) * sizeof(double);
+      if (bytes > kTailScratch) continue;
+      c->tail_parts = 0;
+      if (c->tail_slot.alloc(slot.size()) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+      }
+      if (cudaMemcpy(c->tail_slot.p, slot.data(), slot.size() * sizeof(int), cudaMemcpyHostToDevice) !=
+          cudaSuccess) {
+        rc = bem_fail(c, BEM_ERR_CUDA, "uploading the assembly's piece slots");
+        return 0;
+      }
+      c->tail_parts = pp;
+      c->tail_cols = cols;
+    }
+    const size_t nscr = (size_t)rem * (pp - 1) * 3 * c->tail_cols * 96, nfd = (size_t)rem * (pp - 1) * 32 * 12;
+    if ((c->tail_scr.count < nscr && c->tail_scr.alloc(nscr) != cudaSuccess) ||
+        (c->tail_fd.count < nfd && c->tail_fd.alloc(nfd) != cudaSuccess)) {
+      cudaGetLastError();  // no room: no split
+      c->tail_scr.release();
+      c->tail_fd.release();
+      return 0;
+    }
+    if (cudaMemsetAsync(c->tail_scr.p, 0, nscr * sizeof(double), c->stream) != cudaSuccess) {
+      rc = bem_fail(c, BEM_ERR_CUDA, "clearing the assembly's piece scratch");
+      return 0;
+    }
+    P.nparts = pp;
+    P.tail0 = tiles - rem;
+    P.scr_cols = c->tail_cols;
+    P.slot = c->tail_slot.p;
+    P.scr = c->tail_scr.p;
+    P.fd = c->tail_fd.p;
+    return rem;
+  }
+  return 0;
+}
+
 int launch_ghmat8(bem_ctx* c, int precision) {
   if (!c->have_geometry || !c->have_bc || !c->have_material)
     return bem_fail(c, BEM_ERR_STATE, "ghmat8 needs mesh, material, bc and geometry");
@@ -700,11 +875,22 @@ int launch_ghmat8(bem_ctx* c, int precision) {
                                      kTabSmem));
     attr.mark();
   }
+  const int ntail = plan_tail(c, P, tiles, rc);
+  if (rc) return rc;
+  const int grid = P.nparts > 1 ? P.tail0 + ntail * P.nparts : tiles;
   if (precision == BEM_ASM_FP32_FAR)
-    ghmat_regular_kernel<kModeA, 1><<<tiles, 256, kTabSmem, c->stream>>>(P);
+    ghmat_regular_kernel<kModeA, 1><<<grid, 256, kTabSmem, c->stream>>>(P);
   else
-    ghmat_regular_kernel<kModeA, 0><<<tiles, 256, kTabSmem, c->stream>>>(P);
+    ghmat_regular_kernel<kModeA, 0><<<grid, 256, kTabSmem, c->stream>>>(P);
   BEM_LAUNCH_CHECK(c);
+  if (P.nparts > 1) {
+    const int64_t segs = (int64_t)ntail * c->n * 3;
+    const int blocks = (int)std::min<int64_t>((segs + 7) / 8, 8 * (int64_t)c->sm_count);
+    tail_merge_cols_kernel<<<blocks, 256, 0, c->stream>>>(P, ntail);
+    BEM_LAUNCH_CHECK(c);
+    tail_merge_fd_kernel<<<(32 * ntail + 127) / 128, 128, 0, c->stream>>>(P, ntail);
+    BEM_LAUNCH_CHECK(c);
+  }
   ghmat_singular_kernel<kModeA><<<(c->n + 3) / 4, 128, 0, c->stream>>>(P);
   BEM_LAUNCH_CHECK(c);
   if (c->npins > 0) {
@@ -769,7 +955,7 @@ __global__ void __launch_bounds__(256, 1)
     const int2 w = tiles[it];
     if (threadIdx.x == 0) sP = args[w.x];
     __syncthreads();
-    regular_tile<kModeHG, 0>(sP, w.y);
+    regular_tile<kModeHG, 0>(sP, w.y, 0, 0, sP.nbatches);
     __syncthreads();
   }
 }

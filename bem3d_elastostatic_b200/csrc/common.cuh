@@ -161,6 +161,12 @@ struct bem_ctx {
   // geometry (reference layout) and the packed assembly table
   bem::DBuf<double> eta1, eta2, eta3, xja, xg1, xg2, xg3, ff, tab;
   bem::DBuf<double> erec;  // per-element boundary records of the assembly (mode A)
+  // split last wave of the assembly: host copy of the batch list, the pieces' node
+  // slots (built for tail_parts pieces, 0 = not built) and their scratch
+  std::vector<int> h_batches;
+  int tail_parts = 0, tail_cols = 0;
+  bem::DBuf<int> tail_slot;
+  bem::DBuf<double> tail_scr, tail_fd;
   bool have_geometry = false;
 
   // system

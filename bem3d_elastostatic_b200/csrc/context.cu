@@ -229,6 +229,8 @@ int bem_set_mesh(bem_ctx* c, int n, int ne, const double* x, const double* y, co
   std::vector<int> sched;
   build_batches(n, ne, c->h_nconec, c->h_kconec, sched, c->nbatches);
   if ((rc = upload(c, c->batches, sched.data(), sched.size()))) return rc;
+  c->h_batches = sched;
+  c->tail_parts = 0;
   BEM_CUDA(c, cudaStreamSynchronize(c->stream));
   c->have_mesh = true;
   c->have_bc = false;

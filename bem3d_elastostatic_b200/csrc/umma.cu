@@ -26,7 +26,10 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 
 #include "lu.cuh"
 
@@ -291,10 +294,12 @@ __global__ void __launch_bounds__(kThreads, 1)
     int ab = 0;
     unsigned aphase = 0;
     bool pending = false;
-    for (int t = blockIdx.x; t < total && !*abort_flag; t += gridDim.x) {
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {  // leaves only through the barrier below
       int m0, n0;
       coords(t, m0, n0);
-      // the four warps of a half leave together (they meet at named barriers below)
+      // the four warps of a half leave together: an abort ends every warp's wait, and
+      // the barrier's AND makes the decision the same for all four (a warp that left
+      // on its own would leave the others waiting at the named barriers)
       const int ok = mbar_wait(smem_u32(&tfull[ab]), aphase, abort_flag, wait_ns) ? 1 : 0;
       int all_ok;
       asm volatile(
@@ -372,6 +377,363 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
 }
 
+// ---- CTA pairs (cta_group::2) for the one-product trailing update ------------------
+// A pair of CTAs (a cluster of two) computes a 256 x 256 tile of C with
+// tcgen05.mma.cta_group::2 (M = 256, N = 256), issued by one thread of the pair's
+// first CTA.  Each CTA stages its own 128 rows of A and its own 128 columns of B per K
+// chunk, 32 KB instead of the single CTA's 48 KB for the same 128 x 256 share of C, so
+// each SM's operand stream falls by a third; the tensor cores read the partner's half
+// of B from its shared memory.  Each CTA holds its 128 rows of the accumulator in its
+// own tensor memory and drains them with its own eight epilogue warps, as above.
+//   * Both CTAs' copies complete on the first CTA's `full` barrier (a .cta_group::2
+//     copy may signal the partner's barrier); the first CTA arms it with the pair's
+//     bytes and its MMA thread waits on it alone.
+//   * The MMA commits arrive on both CTAs' `empty` and `tfull` barriers (multicast
+//     commit), so each producer and each epilogue waits on its own shared memory.
+//   * Both epilogues release an accumulator on the first CTA's `tempty` barrier, one
+//     arrival per warp (16).
+// Every wait is bounded as in umma_update_kernel; a CTA also gives up a wait when the
+// error word is set (after the first millisecond of a wait), so that a failure in one
+// CTA of the pair ends the other's waits too.
+constexpr int PK = 128;  // rows of A and columns of B staged per CTA of a pair
+constexpr int kPairStages = 6;  // ring stages of the pair kernel
+constexpr int kPairNstg = 1;    // staging boxes per epilogue half
+
+template <int STAGES, int NSTG>
+struct PairCfg {
+  static constexpr int stage = A_TILE + PK * UK * 2;  // 32 KB
+  static constexpr int ring = STAGES * stage;
+  static constexpr int box = 32 * UM * 4;
+  static constexpr int bar_bytes = 256;  // barriers, then the TMEM address and the abort flag
+  static constexpr int smem = ring + 1024 + bar_bytes + 2 * NSTG * box;
+  static_assert(smem <= 227 * 1024, "shared memory");
+  static_assert((2 * STAGES + 5) * 8 <= 192, "barrier block");
+};
+
+__device__ __forceinline__ unsigned cluster_ctarank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+
+// shared::cluster address of the first CTA's copy of this CTA's shared location a
+__device__ __forceinline__ unsigned map_first(unsigned a) {
+  unsigned r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(0));
+  return r;
+}
+
+__device__ __forceinline__ void cluster_sync() {
+  asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+  asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// bounded wait with cluster-scope acquire (arrivals from the partner CTA); gives up
+// early when this CTA aborted or, after 1 ms, when the error word is set
+__device__ __forceinline__ bool mbar_wait_pair(unsigned bar, unsigned parity, volatile int* abort_flag,
+                                               const volatile int* err, unsigned long long wait_ns) {
+  const unsigned long long t0 = globaltimer();
+  while (true) {
+    unsigned done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (abort_flag && *abort_flag) return false;
+    const unsigned long long dt = globaltimer() - t0;
+    if (dt > wait_ns || (dt > 1000000ull && *err != 0)) return false;
+  }
+}
+
+template <int STAGES, int NSTG>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
+    umma_pair_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB,
+                     const __grid_constant__ CUtensorMap tC, int M, int N, int K, int* err,
+                     unsigned long long wait_ns) {
+  using C_ = PairCfg<STAGES, NSTG>;
+  constexpr int STAGE = C_::stage, kRing = C_::ring;
+  extern __shared__ __align__(16) unsigned char umma_smem[];
+  const unsigned raw = smem_u32(umma_smem);
+  const unsigned base = (raw + 1023u) & ~1023u;  // 1024-byte aligned operand tiles
+  unsigned char* gbase = umma_smem + (base - raw);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(gbase + kRing);
+  uint64_t* full = bars;                    // [STAGES] copies -> MMA (the first CTA's are used)
+  uint64_t* empty = bars + STAGES;          // [STAGES] MMA -> this CTA's producer
+  uint64_t* tfull = bars + 2 * STAGES;      // [2] MMA -> this CTA's epilogue
+  uint64_t* tempty = bars + 2 * STAGES + 2; // [2] both epilogues -> MMA (the first CTA's)
+  uint64_t* drain = bars + 2 * STAGES + 4;  // MMA completion before teardown
+  unsigned* tmem_slot = reinterpret_cast<unsigned*>(gbase + kRing + 192);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(gbase + kRing + 200);
+  const volatile int* gerr = err;
+
+  const unsigned rank = cluster_ctarank();
+  const bool first = rank == 0;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int pair = (int)(blockIdx.x >> 1), npairs = (int)(gridDim.x >> 1);
+  const int tiles_m = (M + 2 * UM - 1) / (2 * UM), tiles_n = (N + UN - 1) / UN, total = tiles_m * tiles_n;
+  const int nchunk = K / UK;
+  // the grouped tile order of umma_update_kernel, with 256-row tiles
+  auto coords = [&](int t, int& m0, int& n0) {
+    const int g = t / (kRasterW * tiles_m), r = t - g * kRasterW * tiles_m;
+    const int nb0 = g * kRasterW, wg = min(kRasterW, tiles_n - nb0);
+    m0 = (r / wg) * (2 * UM);
+    n0 = (nb0 + r % wg) * UN;
+  };
+
+  if (threadIdx.x == 0) {
+    *abort_flag = 0;
+    for (int s = 0; s < STAGES; ++s) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&full[s])), "r"(1) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&empty[s])), "r"(1) : "memory");
+    }
+    for (int b = 0; b < 2; ++b) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&tfull[b])), "r"(1) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&tempty[b])), "r"(2 * kEpiThreads / 32)
+                   : "memory");
+    }
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(drain)), "r"(1) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if (warp == 1) {  // one warp of each CTA of the pair allocates, collectively
+    asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  cluster_sync();  // both CTAs' barriers are initialised before any copy or arrival
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const unsigned tmem = *tmem_slot;
+
+  auto fail = [&]() {
+    *abort_flag = 1;
+    atomicCAS(err, 0, BEM_ERR_TIMEOUT);
+  };
+
+  if (warp == 0) {
+    if (lane == 0) {
+      int stage = 0;
+      unsigned phase = 0;
+      int last[STAGES];
+#pragma unroll
+      for (int s = 0; s < STAGES; ++s) last[s] = -1;
+      const unsigned full_first = map_first(smem_u32(&full[0]));
+      for (int t = pair; t < total && !*abort_flag; t += npairs) {
+        int m0, n0;
+        coords(t, m0, n0);
+        // this CTA's rows of A and columns of B; a half wholly outside the matrix loads
+        // the first half again (its products fall outside C and are not stored)
+        const int ar = (m0 + PK * (int)rank < M) ? m0 + PK * (int)rank : m0;
+        const int br = (n0 + PK * (int)rank < N) ? n0 + PK * (int)rank : n0;
+        bool ok = true;
+        for (int c = 0; c < nchunk; ++c) {
+          if (!mbar_wait_pair(smem_u32(&empty[stage]), phase ^ 1u, abort_flag, gerr, wait_ns)) {
+            ok = false;
+            break;
+          }
+          const unsigned st = base + stage * STAGE;
+          const unsigned bar = full_first + 8u * (unsigned)stage;
+          if (first)  // the pair's bytes: both CTAs' copies complete on this barrier
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(&full[stage])),
+                         "r"(2 * STAGE)
+                         : "memory");
+          asm volatile(
+              "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], "
+              "[%1, {%2, %3}], [%4];" ::"r"(st),
+              "l"(reinterpret_cast<uint64_t>(&tA)), "r"(c * UK), "r"(ar), "r"(bar)
+              : "memory");
+          asm volatile(
+              "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], "
+              "[%1, {%2, %3}], [%4];" ::"r"(st + A_TILE),
+              "l"(reinterpret_cast<uint64_t>(&tB)), "r"(c * UK), "r"(br), "r"(bar)
+              : "memory");
+          last[stage] = (int)phase;
+          if (++stage == STAGES) {
+            stage = 0;
+            phase ^= 1u;
+          }
+        }
+        if (!ok) {
+          fail();
+          break;
+        }
+      }
+      // the first CTA's barrier counts the pair's copies: the phases it armed complete
+      // once both CTAs' copies have landed
+      if (first)
+        for (int s = 0; s < STAGES; ++s)
+          if (last[s] >= 0) mbar_wait(smem_u32(&full[s]), (unsigned)last[s], nullptr, wait_ns);
+    }
+  } else if (warp == 1) {
+    if (lane == 0 && first) {
+      // F32 accumulate, BF16 A and B, both K-major, N = 256, M = 256 (the pair)
+      const unsigned idesc =
+          (1u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(UN >> 3) << 17) | ((unsigned)((2 * UM) >> 4) << 24);
+      const unsigned short both = 3;  // the pair's CTAs
+      int stage = 0, ab = 0;
+      unsigned phase = 0, aphase = 0;
+      for (int t = pair; t < total && !*abort_flag; t += npairs) {
+        if (!mbar_wait_pair(smem_u32(&tempty[ab]), aphase ^ 1u, abort_flag, gerr, wait_ns)) {
+          fail();
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const unsigned d = tmem + (unsigned)(ab * UN);
+        bool ok = true;
+        for (int c = 0; c < nchunk; ++c) {
+          if (!mbar_wait_pair(smem_u32(&full[stage]), phase, abort_flag, gerr, wait_ns)) {
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const unsigned st = base + stage * STAGE;
+#pragma unroll
+          for (int kk = 0; kk < UK / 16; ++kk) {
+            const unsigned off = kk * 32;  // 16 BF16 = 32 bytes along K inside the swizzle atom
+            const uint64_t a = sw128_desc(st + off), b = sw128_desc(st + A_TILE + off);
+            const int acc = (c | kk) != 0;
+            asm volatile(
+                "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+                "l"(a), "l"(b), "r"(idesc), "r"(acc)
+                : "memory");
+          }
+          // frees the stage in both CTAs once these MMAs are done
+          asm volatile(
+              "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+                  smem_u32(&empty[stage])),
+              "h"(both)
+              : "memory");
+          if (++stage == STAGES) {
+            stage = 0;
+            phase ^= 1u;
+          }
+        }
+        if (!ok) {
+          fail();
+          break;
+        }
+        // the accumulator is ready for both epilogues
+        asm volatile(
+            "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+                smem_u32(&tfull[ab])),
+            "h"(both)
+            : "memory");
+        if (++ab == 2) {
+          ab = 0;
+          aphase ^= 1u;
+        }
+      }
+      asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(drain))
+                   : "memory");
+      mbar_wait(smem_u32(drain), 0, nullptr, wait_ns);
+    }
+    __syncwarp();
+  } else {
+    // 8 epilogue warps, as in umma_update_kernel, on this CTA's 128 rows of the tile
+    const int lq = warp & 3;
+    const int half = (warp - 2) >> 2;  // 0 or 1
+    float* stg0 = reinterpret_cast<float*>(gbase + kRing + C_::bar_bytes) + half * NSTG * (32 * UM);
+    int bx = 0;
+    const bool leader = (lq == 0 && lane == 0);
+    const unsigned tempty_first = map_first(smem_u32(&tempty[0]));
+    int ab = 0;
+    unsigned aphase = 0;
+    bool pending = false;
+    for (int t = pair; t < total; t += npairs) {  // leaves only through the barrier below
+      int m0, n0;
+      coords(t, m0, n0);
+      const int rm0 = m0 + PK * (int)rank;  // this CTA's rows
+      const int ok = mbar_wait_pair(smem_u32(&tfull[ab]), aphase, abort_flag, gerr, wait_ns) ? 1 : 0;
+      int all_ok;
+      asm volatile(
+          "{\n\t.reg .pred p, q;\n\tsetp.ne.b32 p, %1, 0;\n\t"
+          "bar.red.and.pred q, %2, 128, p;\n\tselp.b32 %0, 1, 0, q;\n\t}\n"
+          : "=r"(all_ok)
+          : "r"(ok), "r"(1 + half)
+          : "memory");
+      if (!all_ok) {
+        fail();
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      if (rm0 < M) {
+#pragma unroll 1
+        for (int q = 0; q < UN / 64; ++q) {
+          const int j0 = half * (UN / 2) + 32 * q;
+          if (n0 + j0 >= N) break;  // boxes wholly right of C (uniform over the half)
+          unsigned r[32];
+          const unsigned taddr = tmem + ((unsigned)(lq * 32) << 16) + (unsigned)(ab * UN + j0);
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+              "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+              : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+                "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+                "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+              : "r"(taddr)
+              : "memory");
+          float* stg = stg0 + (bx % NSTG) * (32 * UM);
+          const unsigned stg_s = smem_u32(stg);
+          ++bx;
+          if (leader && pending) asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(NSTG - 1) : "memory");
+          asm volatile("bar.sync %0, 128;" ::"r"(1 + half) : "memory");
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          const int rr = lq * 32 + lane;
+#pragma unroll
+          for (int j = 0; j < 32; ++j) stg[j * UM + rr] = -__uint_as_float(r[j]);
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          asm volatile("bar.sync %0, 128;" ::"r"(1 + half) : "memory");
+          if (leader) {
+            asm volatile(
+                "cp.reduce.async.bulk.tensor.2d.global.shared::cta.add.tile.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
+                    reinterpret_cast<uint64_t>(&tC)),
+                "r"(rm0), "r"(n0 + j0), "r"(stg_s)
+                : "memory");
+            asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+            pending = true;
+          }
+        }
+      }
+      // this warp's reads of the accumulator are done: one arrival on the first CTA's
+      // barrier
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0)
+        asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(tempty_first +
+                                                                                           8u * (unsigned)ab)
+                     : "memory");
+      if (++ab == 2) {
+        ab = 0;
+        aphase ^= 1u;
+      }
+    }
+    if (leader && pending) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  // the first CTA's MMAs (which read this CTA's shared memory and write its tensor
+  // memory) are complete, and no copy of either CTA signals the other's barriers
+  cluster_sync();
+  if (*gerr != 0) {
+    // after a failure a copy that the partner issued may still be in flight to this
+    // CTA's shared memory: give it time to land before the memory goes away
+    const unsigned long long t0 = globaltimer();
+    while (globaltimer() - t0 < 100000ull) __nanosleep(1000);
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+  }
+}
+
 // A (m x K, FP32, column-major lda) -> hi/lo BF16 [m][K] (K contiguous); lo nullable
 __global__ void split_a_kernel(int m, int K, const float* __restrict__ A, int64_t lda, __nv_bfloat16* hi,
                                __nv_bfloat16* lo) {
@@ -420,6 +782,50 @@ bool make_map(CUtensorMap* map, const void* ptr, int rows, int K, int box_rows) 
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// one product: four ring stages (48 KB each); three products: two (96 KB each); CTA
+// pairs: six (32 KB each); one staging box per epilogue half (two measured no faster)
+using K1 = Cfg<1, 4, 1>;
+using K3 = Cfg<3, 2, 1>;
+using KP = PairCfg<kPairStages, kPairNstg>;
+std::atomic<int> g_pair_clusters[64];  // co-resident CTA pairs per device (-1: none)
+
+// Kernel attributes (per device), and how many CTA pairs the device holds at once;
+// called before a factorisation is captured into a graph.
+int umma_setup(bem_ctx* c) {
+  static DeviceOnce attr;  // the kernel attribute is per device
+  if (attr.pending()) {
+    int pc = -1;
+    if (cudaFuncSetAttribute(umma_pair_kernel<kPairStages, kPairNstg>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             KP::smem) == cudaSuccess) {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(2 * (unsigned)c->sm_count);
+      cfg.blockDim = dim3(kThreads);
+      cfg.dynamicSmemBytes = KP::smem;
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeClusterDimension;
+      at[0].val.clusterDim.x = 2;
+      at[0].val.clusterDim.y = 1;
+      at[0].val.clusterDim.z = 1;
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+      int n = 0;
+      if (cudaOccupancyMaxActiveClusters(&n, umma_pair_kernel<kPairStages, kPairNstg>, &cfg) == cudaSuccess && n > 0) pc = n;
+    }
+    cudaGetLastError();  // a device without room for the pair kernel keeps the single-CTA kernel
+    g_pair_clusters[current_device()].store(pc);
+    if (std::getenv("BEM_LU_PROFILE"))
+      std::fprintf(stderr, "umma: %d CTA pairs resident per launch (-1: single CTAs)\n", pc);
+    BEM_CUDA(c, cudaFuncSetAttribute(umma_update_kernel<1, 4, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     K1::smem));
+    BEM_CUDA(c, cudaFuncSetAttribute(umma_update_kernel<3, 2, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     K3::smem));
+    BEM_CUDA(c, cudaFuncSetAttribute(umma_update_kernel<3, 2, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     K3::smem));
+    attr.mark();
+  }
+  return BEM_OK;
+}
+
 }  // namespace
 
 bool umma_supported(int K) { return K > 0 && K <= kMaxK && K % UK == 0; }
@@ -427,6 +833,7 @@ bool umma_supported(int K) { return K > 0 && K <= kMaxK && K % UK == 0; }
 // Grows the BF16 operand buffer to what an M x N x K update needs (before a captured
 // factorisation, whose first trailing update is its largest).
 int umma_reserve(bem_ctx* c, int M, int N, int K) {
+  if (int rc = umma_setup(c)) return rc;
   const size_t need = 2 * ((size_t)M * K + (size_t)N * K) * sizeof(__nv_bfloat16) + 256;
   if (c->umma_buf.count < need) {
     c->umma_buf.release();
@@ -454,20 +861,7 @@ int gemm_umma_bf16(bem_ctx* c, int M, int N, int K, const float* A, int64_t lda,
       return bem_fail(c, BEM_ERR_CUDA, "cuTensorMapEncodeTiled not available");
     g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
   }
-  // one product: four ring stages (48 KB each); three products: two (96 KB each); one
-  // staging box per epilogue half (two measured no faster)
-  using K1 = Cfg<1, 4, 1>;
-  using K3 = Cfg<3, 2, 1>;
-  static DeviceOnce attr;  // the kernel attribute is per device
-  if (attr.pending()) {
-    BEM_CUDA(c, cudaFuncSetAttribute(umma_update_kernel<1, 4, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     K1::smem));
-    BEM_CUDA(c, cudaFuncSetAttribute(umma_update_kernel<3, 2, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     K3::smem));
-    BEM_CUDA(c, cudaFuncSetAttribute(umma_update_kernel<3, 2, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     K3::smem));
-    attr.mark();
-  }
+  if (int rc = umma_setup(c)) return rc;
   const size_t na = (size_t)M * K, nb_ = (size_t)N * K;
   const size_t need = 2 * (na + nb_) * sizeof(__nv_bfloat16) + 256;
   if (c->umma_buf.count < need) {
@@ -505,6 +899,22 @@ int gemm_umma_bf16(bem_ctx* c, int M, int N, int K, const float* A, int64_t lda,
                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
       return bem_fail(c, BEM_ERR_CUDA, "umma: tensor map encoding of C failed");
+  }
+  // the one-product update on CTA pairs (BEM_UMMA_PAIR=0: single CTAs)
+  const int pairs = g_pair_clusters[current_device()].load();
+  static const bool pair_env = [] {
+    const char* e = std::getenv("BEM_UMMA_PAIR");
+    return !(e && std::atoi(e) == 0);
+  }();
+  if (nprod == 1 && !store && kmode == 0 && pairs > 0 && pair_env) {
+    CUtensorMap mBp;
+    if (!make_map(&mBp, bh, N, K, PK)) return bem_fail(c, BEM_ERR_CUDA, "umma: tensor map encoding failed");
+    const int64_t ptiles = (int64_t)((M + 2 * UM - 1) / (2 * UM)) * ((N + UN - 1) / UN);
+    const int pgrid = 2 * (int)std::min<int64_t>(ptiles, pairs);
+    umma_pair_kernel<kPairStages, kPairNstg><<<pgrid, kThreads, KP::smem, c->stream>>>(mAh, mBp, mC, M, N, K, c->umma_err.p,
+                                                                              c->wait_ns);
+    BEM_LAUNCH_CHECK(c);
+    return BEM_OK;
   }
   const int grid = (int)std::min<int64_t>(tiles, c->sm_count);
   if (store)
