@@ -423,6 +423,15 @@ __device__ __forceinline__ unsigned map_first(unsigned a) {
   return r;
 }
 
+// arrives on the barrier at shared offset bar in both CTAs of the pair once the MMAs
+// this thread issued are done
+__device__ __forceinline__ void umma_commit_pair(unsigned bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(bar),
+      "h"((unsigned short)3)
+      : "memory");
+}
+
 __device__ __forceinline__ void cluster_sync() {
   asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
   asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
@@ -575,7 +584,6 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
       // F32 accumulate, BF16 A and B, both K-major, N = 256, M = 256 (the pair)
       const unsigned idesc =
           (1u << 4) | (1u << 7) | (1u << 10) | ((unsigned)(UN >> 3) << 17) | ((unsigned)((2 * UM) >> 4) << 24);
-      const unsigned short both = 3;  // the pair's CTAs
       int stage = 0, ab = 0;
       unsigned phase = 0, aphase = 0;
       for (int t = pair; t < total && !*abort_flag; t += npairs) {
@@ -604,12 +612,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
                 "l"(a), "l"(b), "r"(idesc), "r"(acc)
                 : "memory");
           }
-          // frees the stage in both CTAs once these MMAs are done
-          asm volatile(
-              "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
-                  smem_u32(&empty[stage])),
-              "h"(both)
-              : "memory");
+          umma_commit_pair(smem_u32(&empty[stage]));  // frees the stage in both CTAs
           if (++stage == STAGES) {
             stage = 0;
             phase ^= 1u;
@@ -619,12 +622,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
           fail();
           break;
         }
-        // the accumulator is ready for both epilogues
-        asm volatile(
-            "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
-                smem_u32(&tfull[ab])),
-            "h"(both)
-            : "memory");
+        umma_commit_pair(smem_u32(&tfull[ab]));  // the accumulator is ready for both epilogues
         if (++ab == 2) {
           ab = 0;
           aphase ^= 1u;
@@ -795,8 +793,8 @@ int umma_setup(bem_ctx* c) {
   static DeviceOnce attr;  // the kernel attribute is per device
   if (attr.pending()) {
     int pc = -1;
-    if (cudaFuncSetAttribute(umma_pair_kernel<kPairStages, kPairNstg>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             KP::smem) == cudaSuccess) {
+    auto* pair_fn = umma_pair_kernel<kPairStages, kPairNstg>;
+    if (cudaFuncSetAttribute(pair_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, KP::smem) == cudaSuccess) {
       cudaLaunchConfig_t cfg = {};
       cfg.gridDim = dim3(2 * (unsigned)c->sm_count);
       cfg.blockDim = dim3(kThreads);
@@ -809,7 +807,7 @@ int umma_setup(bem_ctx* c) {
       cfg.attrs = at;
       cfg.numAttrs = 1;
       int n = 0;
-      if (cudaOccupancyMaxActiveClusters(&n, umma_pair_kernel<kPairStages, kPairNstg>, &cfg) == cudaSuccess && n > 0) pc = n;
+      if (cudaOccupancyMaxActiveClusters(&n, pair_fn, &cfg) == cudaSuccess && n > 0) pc = n;
     }
     cudaGetLastError();  // a device without room for the pair kernel keeps the single-CTA kernel
     g_pair_clusters[current_device()].store(pc);
@@ -911,8 +909,8 @@ int gemm_umma_bf16(bem_ctx* c, int M, int N, int K, const float* A, int64_t lda,
     if (!make_map(&mBp, bh, N, K, PK)) return bem_fail(c, BEM_ERR_CUDA, "umma: tensor map encoding failed");
     const int64_t ptiles = (int64_t)((M + 2 * UM - 1) / (2 * UM)) * ((N + UN - 1) / UN);
     const int pgrid = 2 * (int)std::min<int64_t>(ptiles, pairs);
-    umma_pair_kernel<kPairStages, kPairNstg><<<pgrid, kThreads, KP::smem, c->stream>>>(mAh, mBp, mC, M, N, K, c->umma_err.p,
-                                                                              c->wait_ns);
+    umma_pair_kernel<kPairStages, kPairNstg><<<pgrid, kThreads, KP::smem, c->stream>>>(mAh, mBp, mC, M, N, K,
+                                                                                      c->umma_err.p, c->wait_ns);
     BEM_LAUNCH_CHECK(c);
     return BEM_OK;
   }

@@ -762,8 +762,9 @@ def run_gpu(args, ws, rank, local):
     roofline = {
         "kernel": ("umma_update_kernel + its BF16 split kernels (LU trailing update: C -= A B, "
                    "tcgen05 BF16x3 into TMEM, TMA-reduce epilogue)" if args.precision == "fp32-ir" else
-                   "umma_update_kernel, one BF16 product (LU trailing update: C -= A B, tcgen05 into TMEM, "
-                   "four-stage TMA ring, TMA-reduce epilogue)"),
+                   "umma_pair_kernel, one BF16 product (LU trailing update: C -= A B, 256 x 256 tiles on "
+                   "CTA pairs, tcgen05.mma.cta_group::2 into TMEM, six-stage TMA ring per CTA, "
+                   "TMA-reduce epilogue)"),
         "traffic": None,
         "algorithmic_bytes_per_launch": prof["lu_trailing_bytes"] / n_launch,
         "algorithmic_fp32_flops_per_launch": prof["lu_trailing_flops"] / n_launch,
