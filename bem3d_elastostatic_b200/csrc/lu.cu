@@ -1245,6 +1245,12 @@ static int trailing_gemm(bem_ctx* c, int M, int N, int K, const float* A, int64_
   return gemm<float>(c, M, N, K, A, lda, B, ldb, C, ldc, 0);
 }
 
+// Whether gemm_tri runs on tcgen05, whose kernel reads only the BF16 copies of its
+// operands that the split kernels made before it: C may then be one of the operands.
+static bool gemm_tri_in_place(const bem_ctx* c, int M, int N, int K, const float* C, int64_t ldc) {
+  return uses_umma(c) && umma_supported(K) && M >= 128 && N >= 256 && umma_c_ok(C, ldc);
+}
+
 // C = A B with a triangular factor (kmode 1: A lower, kmode 2: B upper): on tcgen05 each
 // tile skips the K chunks of the factor's zero part.
 static int gemm_tri(bem_ctx* c, int M, int N, int K, const float* A, int64_t lda, const float* B, int64_t ldb,
@@ -1632,21 +1638,36 @@ static int lu_factor_enqueue(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int
               (rc = gemm<T>(c, bb, b0, bb, Wb, kInvBlock, Tl, kInvBlock, XL + b0, jb, 0)))
             return rc;
         }
-        if ((rc = gemm_tri(c, jb, m, jb, reinterpret_cast<const float*>(XL), jb,
-                           reinterpret_cast<const float*>(S + j0 + (int64_t)t0 * lda), lda, reinterpret_cast<float*>(Y),
-                           jb, 1)))
-          return rc;
-        BEM_CUDA(c, cudaMemcpy2DAsync(S + j0 + (int64_t)t0 * lda, lda * sizeof(T), Y, jb * sizeof(T), jb * sizeof(T), m,
-                                      cudaMemcpyDeviceToDevice, c->stream));
+        float* L21 = reinterpret_cast<float*>(S + j0 + (int64_t)t0 * lda);
+        if (gemm_tri_in_place(c, jb, m, jb, L21, lda)) {  // written over its own operand
+          if ((rc = gemm_tri(c, jb, m, jb, reinterpret_cast<const float*>(XL), jb, L21, lda, L21, lda, 1)))
+            return rc;
+        } else {
+          if ((rc = gemm_tri(c, jb, m, jb, reinterpret_cast<const float*>(XL), jb, L21, lda,
+                             reinterpret_cast<float*>(Y), jb, 1)))
+            return rc;
+          BEM_CUDA(c, cudaMemcpy2DAsync(L21, lda * sizeof(T), Y, jb * sizeof(T), jb * sizeof(T), m,
+                                        cudaMemcpyDeviceToDevice, c->stream));
+        }
         prof.end(c->stream);
       }
       prof.begin(3, c->stream);
+      // the block row's solution Y = X U^{-1}: in a buffer (ldy), copied into S below, or
+      // on tcgen05 written over X in S itself
+      const T* Yr = Y;
+      int64_t ldyr = ldy;
       if (blocked) {
         if (c->aux_stream) BEM_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_join, 0));
         // TRSM of the block row in one product, Y = X U^{-1}
-        if ((rc = gemm_tri(c, m, jb, jb, reinterpret_cast<const float*>(S + t0 + (int64_t)j0 * lda), lda,
-                           reinterpret_cast<const float*>(XU), jb, reinterpret_cast<float*>(Y), ldy, 2)))
+        float* X = reinterpret_cast<float*>(S + t0 + (int64_t)j0 * lda);
+        const bool in_place = gemm_tri_in_place(c, m, jb, jb, X, lda);
+        if ((rc = gemm_tri(c, m, jb, jb, X, lda, reinterpret_cast<const float*>(XU), jb,
+                           in_place ? X : reinterpret_cast<float*>(Y), in_place ? lda : ldy, 2)))
           return rc;
+        if (in_place) {
+          Yr = S + t0 + (int64_t)j0 * lda;
+          ldyr = lda;
+        }
       } else {
       // TRSM of the block row, Y = X U^{-1} with U the unit upper triangle of the panel's
       // diagonal block, in 128-wide column blocks: X_b -= Y_{<b} U_{<b,b}, Y_b = X_b inv(U_bb)
@@ -1667,16 +1688,17 @@ static int lu_factor_enqueue(bem_ctx* c, T* S, int64_t lda, int n, int* piv, int
         if ((rc = gemm<T>(c, m, bb, bb, Xb, lda, V, kInvBlock, Y + (int64_t)b0 * ldy, ldy, 1))) return rc;
       }
       }
-      BEM_CUDA(c, cudaMemcpy2DAsync(S + t0 + (int64_t)j0 * lda, lda * sizeof(T), Y, ldy * sizeof(T), m * sizeof(T),
-                                    jb, cudaMemcpyDeviceToDevice, c->stream));
+      if (Yr == Y)
+        BEM_CUDA(c, cudaMemcpy2DAsync(S + t0 + (int64_t)j0 * lda, lda * sizeof(T), Y, ldy * sizeof(T), m * sizeof(T),
+                                      jb, cudaMemcpyDeviceToDevice, c->stream));
       prof.end(c->stream);
       prof.begin(4, c->stream);
       if constexpr (sizeof(T) == 4) {
-        if ((rc = trailing_gemm(c, m, m, jb, Y, ldy, S + j0 + (int64_t)t0 * lda, lda, S + t0 + (int64_t)t0 * lda,
+        if ((rc = trailing_gemm(c, m, m, jb, Yr, ldyr, S + j0 + (int64_t)t0 * lda, lda, S + t0 + (int64_t)t0 * lda,
                                 lda)))
           return rc;
-      } else if ((rc = gemm<T>(c, m, m, jb, Y, ldy, S + j0 + (int64_t)t0 * lda, lda, S + t0 + (int64_t)t0 * lda, lda,
-                               0))) {
+      } else if ((rc = gemm<T>(c, m, m, jb, Yr, ldyr, S + j0 + (int64_t)t0 * lda, lda, S + t0 + (int64_t)t0 * lda,
+                               lda, 0))) {
         return rc;
       }
       prof.end(c->stream, 2.0 * m * (double)m * jb, (2.0 * m * (double)m + 2.0 * m * (double)jb) * sizeof(T));
