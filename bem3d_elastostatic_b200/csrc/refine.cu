@@ -1,6 +1,7 @@
 // Mixed-precision solve (FP32 factors + FP64 iterative refinement against the FP64
 // A) and reorganize_solution (io_mod.f90:148-183).
 #include <cmath>
+#include <limits>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -402,9 +403,18 @@ int solve_mixed(bem_ctx* c, int precision, double rel_tol, int max_iter, bem_sol
     };
     const double inner_tol = 1e-6;
     for (restarts = 0; restarts < max_iter; ++restarts) {
-      if ((rc = residual_fp64(c, c->A.p, lda, n, c->X.p, c->FI.p, r.p, norms, anorm < 0, ext))) return rc;
-      if (anorm < 0) anorm = norms[3];
-      berr = norms[0] / (anorm * norms[1] + norms[2]);
+      if (restarts == 0) {
+        // x = 0: the residual is b itself (r holds a copy) and the backward error
+        // |r| / (|A| |x| + |b|) is 1, or undefined for b = 0, without a pass over A;
+        // the matrix norm comes with the next residual
+        double bn = 0.0;
+        if ((rc = norm2(r.p, &bn))) return rc;
+        berr = bn > 0.0 ? 1.0 : std::numeric_limits<double>::quiet_NaN();
+      } else {
+        if ((rc = residual_fp64(c, c->A.p, lda, n, c->X.p, c->FI.p, r.p, norms, anorm < 0, ext))) return rc;
+        if (anorm < 0) anorm = norms[3];
+        berr = norms[0] / (anorm * norms[1] + norms[2]);
+      }
       if (!(berr == berr) || berr <= rel_tol) break;
       if (berr > 0.5 * prev && restarts > 3) break;  // stagnation
       prev = berr;
