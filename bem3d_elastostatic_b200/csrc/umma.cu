@@ -377,14 +377,18 @@ __global__ void __launch_bounds__(kThreads, 1)
   }
 }
 
-// ---- CTA pairs (cta_group::2) for the one-product trailing update ------------------
+// ---- CTA pairs (cta_group::2) -----------------------------------------------------
 // A pair of CTAs (a cluster of two) computes a 256 x 256 tile of C with
 // tcgen05.mma.cta_group::2 (M = 256, N = 256), issued by one thread of the pair's
 // first CTA.  Each CTA stages its own 128 rows of A and its own 128 columns of B per K
-// chunk, 32 KB instead of the single CTA's 48 KB for the same 128 x 256 share of C, so
-// each SM's operand stream falls by a third; the tensor cores read the partner's half
-// of B from its shared memory.  Each CTA holds its 128 rows of the accumulator in its
-// own tensor memory and drains them with its own eight epilogue warps, as above.
+// chunk (hi, or hi and lo for three products): 32 KB instead of the single CTA's 48 KB
+// for the same 128 x 256 share of C with one product, 64 KB instead of 96 KB with
+// three, so each SM's operand stream falls by a third; the tensor cores read the
+// partner's half of B from its shared memory.  Each CTA holds its 128 rows of the
+// accumulator in its own tensor memory and drains them with its own eight epilogue
+// warps, as above (reductions into C, or stores with STORE).  With a triangular
+// operand (kmode) a tile runs the K chunks that meet the nonzero part of its 256 rows
+// or columns.
 //   * Both CTAs' copies complete on the first CTA's `full` barrier (a .cta_group::2
 //     copy may signal the partner's barrier); the first CTA arms it with the pair's
 //     bytes and its MMA thread waits on it alone.
@@ -396,16 +400,15 @@ __global__ void __launch_bounds__(kThreads, 1)
 // error word is set (after the first millisecond of a wait), so that a failure in one
 // CTA of the pair ends the other's waits too.
 constexpr int PK = 128;  // rows of A and columns of B staged per CTA of a pair
-constexpr int kPairStages = 6;  // ring stages of the pair kernel
-constexpr int kPairNstg = 1;    // staging boxes per epilogue half
+constexpr int B_HALF = PK * UK * 2;  // 16 KB
 
-template <int STAGES, int NSTG>
+template <int NPROD, int STAGES>
 struct PairCfg {
-  static constexpr int stage = A_TILE + PK * UK * 2;  // 32 KB
+  static constexpr int stage = NPROD == 3 ? 2 * A_TILE + 2 * B_HALF : A_TILE + B_HALF;  // 64 or 32 KB
   static constexpr int ring = STAGES * stage;
   static constexpr int box = 32 * UM * 4;
   static constexpr int bar_bytes = 256;  // barriers, then the TMEM address and the abort flag
-  static constexpr int smem = ring + 1024 + bar_bytes + 2 * NSTG * box;
+  static constexpr int smem = ring + 1024 + bar_bytes + 2 * box;  // one staging box per epilogue half
   static_assert(smem <= 227 * 1024, "shared memory");
   static_assert((2 * STAGES + 5) * 8 <= 192, "barrier block");
 };
@@ -458,12 +461,14 @@ __device__ __forceinline__ bool mbar_wait_pair(unsigned bar, unsigned parity, vo
   }
 }
 
-template <int STAGES, int NSTG>
+template <int NPROD, int STAGES, bool STORE>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
-    umma_pair_kernel(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB,
-                     const __grid_constant__ CUtensorMap tC, int M, int N, int K, int* err,
+    umma_pair_kernel(const __grid_constant__ CUtensorMap tAh, const __grid_constant__ CUtensorMap tAl,
+                     const __grid_constant__ CUtensorMap tBh, const __grid_constant__ CUtensorMap tBl,
+                     const __grid_constant__ CUtensorMap tC, int M, int N, int K, int kmode, int* err,
                      unsigned long long wait_ns) {
-  using C_ = PairCfg<STAGES, NSTG>;
+  constexpr int NSTG = 1;
+  using C_ = PairCfg<NPROD, STAGES>;
   constexpr int STAGE = C_::stage, kRing = C_::ring;
   extern __shared__ __align__(16) unsigned char umma_smem[];
   const unsigned raw = smem_u32(umma_smem);
@@ -484,13 +489,17 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int pair = (int)(blockIdx.x >> 1), npairs = (int)(gridDim.x >> 1);
   const int tiles_m = (M + 2 * UM - 1) / (2 * UM), tiles_n = (N + UN - 1) / UN, total = tiles_m * tiles_n;
-  const int nchunk = K / UK;
   // the grouped tile order of umma_update_kernel, with 256-row tiles
   auto coords = [&](int t, int& m0, int& n0) {
     const int g = t / (kRasterW * tiles_m), r = t - g * kRasterW * tiles_m;
     const int nb0 = g * kRasterW, wg = min(kRasterW, tiles_n - nb0);
     m0 = (r / wg) * (2 * UM);
     n0 = (nb0 + r % wg) * UN;
+  };
+  // K chunks of the pair's tile (kmode 1: A lower triangular, 2: B upper triangular)
+  auto chunks = [&](int m0, int n0) {
+    const int ke = kmode == 1 ? min(K, m0 + 2 * UM) : (kmode == 2 ? min(K, n0 + UN) : K);
+    return (ke + UK - 1) / UK;
   };
 
   if (threadIdx.x == 0) {
@@ -540,6 +549,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
         // the first half again (its products fall outside C and are not stored)
         const int ar = (m0 + PK * (int)rank < M) ? m0 + PK * (int)rank : m0;
         const int br = (n0 + PK * (int)rank < N) ? n0 + PK * (int)rank : n0;
+        const int nchunk = chunks(m0, n0);
         bool ok = true;
         for (int c = 0; c < nchunk; ++c) {
           if (!mbar_wait_pair(smem_u32(&empty[stage]), phase ^ 1u, abort_flag, gerr, wait_ns)) {
@@ -552,16 +562,19 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
             asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(&full[stage])),
                          "r"(2 * STAGE)
                          : "memory");
-          asm volatile(
-              "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], "
-              "[%1, {%2, %3}], [%4];" ::"r"(st),
-              "l"(reinterpret_cast<uint64_t>(&tA)), "r"(c * UK), "r"(ar), "r"(bar)
-              : "memory");
-          asm volatile(
-              "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], "
-              "[%1, {%2, %3}], [%4];" ::"r"(st + A_TILE),
-              "l"(reinterpret_cast<uint64_t>(&tB)), "r"(c * UK), "r"(br), "r"(bar)
-              : "memory");
+          // stage layout: three products [A hi | A lo | B hi | B lo], one [A hi | B hi]
+          const CUtensorMap* maps[4] = {&tAh, &tAl, &tBh, &tBl};
+          const int row[4] = {ar, ar, br, br};
+          const unsigned dst[4] = {st, st + A_TILE, NPROD == 3 ? st + 2 * A_TILE : st + A_TILE,
+                                   st + 2 * A_TILE + B_HALF};
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            if (NPROD == 3 || q == 0 || q == 2)
+              asm volatile(
+                  "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], "
+                  "[%1, {%2, %3}], [%4];" ::"r"(dst[q]),
+                  "l"(reinterpret_cast<uint64_t>(maps[q])), "r"(c * UK), "r"(row[q]), "r"(bar)
+                  : "memory");
           last[stage] = (int)phase;
           if (++stage == STAGES) {
             stage = 0;
@@ -593,6 +606,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const unsigned d = tmem + (unsigned)(ab * UN);
+        int tm0, tn0;
+        coords(t, tm0, tn0);
+        const int nchunk = chunks(tm0, tn0);
         bool ok = true;
         for (int c = 0; c < nchunk; ++c) {
           if (!mbar_wait_pair(smem_u32(&full[stage]), phase, abort_flag, gerr, wait_ns)) {
@@ -601,16 +617,23 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
           }
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
           const unsigned st = base + stage * STAGE;
+          const unsigned ah = st, al = st + A_TILE, bh = NPROD == 3 ? st + 2 * A_TILE : st + A_TILE,
+                         bl = st + 2 * A_TILE + B_HALF;
 #pragma unroll
           for (int kk = 0; kk < UK / 16; ++kk) {
             const unsigned off = kk * 32;  // 16 BF16 = 32 bytes along K inside the swizzle atom
-            const uint64_t a = sw128_desc(st + off), b = sw128_desc(st + A_TILE + off);
-            const int acc = (c | kk) != 0;
-            asm volatile(
-                "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-                "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
-                "l"(a), "l"(b), "r"(idesc), "r"(acc)
-                : "memory");
+            const uint64_t a_h = sw128_desc(ah + off), a_l = sw128_desc(al + off);
+            const uint64_t b_h = sw128_desc(bh + off), b_l = sw128_desc(bl + off);
+            const uint64_t pa[3] = {a_h, a_h, a_l}, pb[3] = {b_h, b_l, b_h};
+#pragma unroll
+            for (int q = 0; q < NPROD; ++q) {
+              const int acc = (c | kk | q) != 0;
+              asm volatile(
+                  "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                  "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+                  "l"(pa[q]), "l"(pb[q]), "r"(idesc), "r"(acc)
+                  : "memory");
+            }
           }
           umma_commit_pair(smem_u32(&empty[stage]));  // frees the stage in both CTAs
           if (++stage == STAGES) {
@@ -686,15 +709,21 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
           asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
           const int rr = lq * 32 + lane;
 #pragma unroll
-          for (int j = 0; j < 32; ++j) stg[j * UM + rr] = -__uint_as_float(r[j]);
+          for (int j = 0; j < 32; ++j) stg[j * UM + rr] = STORE ? __uint_as_float(r[j]) : -__uint_as_float(r[j]);
           asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
           asm volatile("bar.sync %0, 128;" ::"r"(1 + half) : "memory");
           if (leader) {
-            asm volatile(
-                "cp.reduce.async.bulk.tensor.2d.global.shared::cta.add.tile.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
-                    reinterpret_cast<uint64_t>(&tC)),
-                "r"(rm0), "r"(n0 + j0), "r"(stg_s)
-                : "memory");
+            if (STORE)
+              asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
+                               reinterpret_cast<uint64_t>(&tC)),
+                           "r"(rm0), "r"(n0 + j0), "r"(stg_s)
+                           : "memory");
+            else
+              asm volatile(
+                  "cp.reduce.async.bulk.tensor.2d.global.shared::cta.add.tile.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
+                      reinterpret_cast<uint64_t>(&tC)),
+                  "r"(rm0), "r"(n0 + j0), "r"(stg_s)
+                  : "memory");
             asm volatile("cp.async.bulk.commit_group;" ::: "memory");
             pending = true;
           }
@@ -784,32 +813,42 @@ bool make_map(CUtensorMap* map, const void* ptr, int rows, int K, int box_rows) 
 // pairs: six (32 KB each); one staging box per epilogue half (two measured no faster)
 using K1 = Cfg<1, 4, 1>;
 using K3 = Cfg<3, 2, 1>;
-using KP = PairCfg<kPairStages, kPairNstg>;
+// CTA pairs: six 32 KB stages for one product, three 64 KB stages for three (the ring
+// depth measured best: five or four stages of one product were slower)
+using KP1 = PairCfg<1, 6>;
+using KP3 = PairCfg<3, 3>;
 std::atomic<int> g_pair_clusters[64];  // co-resident CTA pairs per device (-1: none)
+
+// the most clusters of two of `fn` (smem bytes each) the device holds at once, or -1
+template <typename F>
+int pair_capacity(bem_ctx* c, F* fn, int smem) {
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) return -1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(2 * (unsigned)c->sm_count);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = smem;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = 2;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, fn, &cfg) != cudaSuccess || n <= 0) return -1;
+  return n;
+}
 
 // Kernel attributes (per device), and how many CTA pairs the device holds at once;
 // called before a factorisation is captured into a graph.
 int umma_setup(bem_ctx* c) {
   static DeviceOnce attr;  // the kernel attribute is per device
   if (attr.pending()) {
-    int pc = -1;
-    auto* pair_fn = umma_pair_kernel<kPairStages, kPairNstg>;
-    if (cudaFuncSetAttribute(pair_fn, cudaFuncAttributeMaxDynamicSharedMemorySize, KP::smem) == cudaSuccess) {
-      cudaLaunchConfig_t cfg = {};
-      cfg.gridDim = dim3(2 * (unsigned)c->sm_count);
-      cfg.blockDim = dim3(kThreads);
-      cfg.dynamicSmemBytes = KP::smem;
-      cudaLaunchAttribute at[1];
-      at[0].id = cudaLaunchAttributeClusterDimension;
-      at[0].val.clusterDim.x = 2;
-      at[0].val.clusterDim.y = 1;
-      at[0].val.clusterDim.z = 1;
-      cfg.attrs = at;
-      cfg.numAttrs = 1;
-      int n = 0;
-      if (cudaOccupancyMaxActiveClusters(&n, pair_fn, &cfg) == cudaSuccess && n > 0) pc = n;
-    }
-    cudaGetLastError();  // a device without room for the pair kernel keeps the single-CTA kernel
+    int pc = pair_capacity(c, umma_pair_kernel<1, 6, false>, KP1::smem);
+    const int p3 = pair_capacity(c, umma_pair_kernel<3, 3, false>, KP3::smem);
+    const int p3s = pair_capacity(c, umma_pair_kernel<3, 3, true>, KP3::smem);
+    pc = std::min(pc, std::min(p3, p3s));
+    cudaGetLastError();  // a device without room for the pair kernels keeps the single-CTA kernel
     g_pair_clusters[current_device()].store(pc);
     if (std::getenv("BEM_LU_PROFILE"))
       std::fprintf(stderr, "umma: %d CTA pairs resident per launch (-1: single CTAs)\n", pc);
@@ -898,19 +937,27 @@ int gemm_umma_bf16(bem_ctx* c, int M, int N, int K, const float* A, int64_t lda,
                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
       return bem_fail(c, BEM_ERR_CUDA, "umma: tensor map encoding of C failed");
   }
-  // the one-product update on CTA pairs (BEM_UMMA_PAIR=0: single CTAs)
+  // CTA pairs for tiles of more than 128 rows (BEM_UMMA_PAIR=0: single CTAs)
   const int pairs = g_pair_clusters[current_device()].load();
   static const bool pair_env = [] {
     const char* e = std::getenv("BEM_UMMA_PAIR");
     return !(e && std::atoi(e) == 0);
   }();
-  if (nprod == 1 && !store && kmode == 0 && pairs > 0 && pair_env) {
-    CUtensorMap mBp;
-    if (!make_map(&mBp, bh, N, K, PK)) return bem_fail(c, BEM_ERR_CUDA, "umma: tensor map encoding failed");
+  if (M > UM && pairs > 0 && pair_env) {
+    CUtensorMap mBph, mBpl;  // B halves of 128 columns per CTA
+    if (!make_map(&mBph, bh, N, K, PK) || !make_map(&mBpl, bl, N, K, PK))
+      return bem_fail(c, BEM_ERR_CUDA, "umma: tensor map encoding failed");
     const int64_t ptiles = (int64_t)((M + 2 * UM - 1) / (2 * UM)) * ((N + UN - 1) / UN);
     const int pgrid = 2 * (int)std::min<int64_t>(ptiles, pairs);
-    umma_pair_kernel<kPairStages, kPairNstg><<<pgrid, kThreads, KP::smem, c->stream>>>(mAh, mBp, mC, M, N, K,
-                                                                                      c->umma_err.p, c->wait_ns);
+    if (store)
+      umma_pair_kernel<3, 3, true><<<pgrid, kThreads, KP3::smem, c->stream>>>(mAh, mAl, mBph, mBpl, mC, M, N, K,
+                                                                              kmode, c->umma_err.p, c->wait_ns);
+    else if (nprod == 3)
+      umma_pair_kernel<3, 3, false><<<pgrid, kThreads, KP3::smem, c->stream>>>(mAh, mAl, mBph, mBpl, mC, M, N, K,
+                                                                               kmode, c->umma_err.p, c->wait_ns);
+    else
+      umma_pair_kernel<1, 6, false><<<pgrid, kThreads, KP1::smem, c->stream>>>(mAh, mAl, mBph, mBpl, mC, M, N, K,
+                                                                               kmode, c->umma_err.p, c->wait_ns);
     BEM_LAUNCH_CHECK(c);
     return BEM_OK;
   }
