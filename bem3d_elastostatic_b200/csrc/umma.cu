@@ -809,8 +809,8 @@ bool make_map(CUtensorMap* map, const void* ptr, int rows, int K, int box_rows) 
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// one product: four ring stages (48 KB each); three products: two (96 KB each); CTA
-// pairs: six (32 KB each); one staging box per epilogue half (two measured no faster)
+// single CTAs: four ring stages of 48 KB for one product, two of 96 KB for three; one
+// staging box per epilogue half (two measured no faster)
 using K1 = Cfg<1, 4, 1>;
 using K3 = Cfg<3, 2, 1>;
 // CTA pairs: six 32 KB stages for one product, three 64 KB stages for three (the ring
