@@ -1255,8 +1255,7 @@ static bool gemm_tri_in_place(const bem_ctx* c, int M, int N, int K, const float
 // tile skips the K chunks of the factor's zero part.
 static int gemm_tri(bem_ctx* c, int M, int N, int K, const float* A, int64_t lda, const float* B, int64_t ldb,
                     float* C, int64_t ldc, int kmode) {
-  if (uses_umma(c) && umma_supported(K) && M >= 128 && N >= 256 && umma_c_ok(C, ldc))
-    return gemm_umma_bf16(c, M, N, K, A, lda, B, ldb, C, ldc, 3, true, kmode);
+  if (gemm_tri_in_place(c, M, N, K, C, ldc)) return gemm_umma_bf16(c, M, N, K, A, lda, B, ldb, C, ldc, 3, true, kmode);
   return gemm<float>(c, M, N, K, A, lda, B, ldb, C, ldc, 1);
 }
 
